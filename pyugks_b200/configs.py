@@ -1,0 +1,174 @@
+"""Case descriptions: the problems the solver runs, as plain data.
+
+A *case* is a dict holding everything a pyUGKS job file would set for the
+time-step path (``ugks_data.py:146-235`` defaults, ``Block2D`` /
+``connect_blocks_2D`` / ``*BC`` objects of ``geom/``): physics constants, the
+velocity quadrature, and per block its vertex grid, four boundary conditions
+and fill.  All values are non-dimensional (reference density, temperature and
+length of 1; velocities in units of the most probable speed sqrt(2RT_ref),
+``ugks_data.py:362``).
+
+``cavity`` and ``channel`` build the workloads this package is measured on:
+
+* ``cavity(32, 24, ...)``: lid-driven cavity, 32x32 cells, 24x24 velocities on
+  [-4,4]^2 (rounded by the Newton rule to 25x25 = 625), vanLeer, Kn 0.075,
+  CFL 0.8, diffuse walls at T=1 with the lid at U=0.15;
+* ``cavity_multiblock(...)``: the same cavity as 2x2 blocks of 64x64 cells,
+  33x33 velocities on [-5,5]^2, WENO5, Kn 0.01, density 1 + 0.01 N(0,1)
+  smoothed by three 3x3 box passes (seed 0);
+* ``batched_cavities(64, seed=1)``: 64 independent cavities with drawn sizes
+  and parameters;
+* ``channel(...)``: 256x64 pressure-driven channel in 4 blocks with an
+  adsorbing lower wall.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import defs as D
+
+
+def uniform_grid(ni, nj, x0=0.0, x1=1.0, y0=0.0, y1=1.0):
+    """Vertex coordinates (ni+1, nj+1) of a uniform Cartesian block; the
+    reference's StructuredGrid layout (``geom/geom_grid.py:61-69``)."""
+    i = np.arange(ni + 1, dtype=np.float64)[:, None]
+    j = np.arange(nj + 1, dtype=np.float64)[None, :]
+    x = x0 + (x1 - x0) * (i / ni) + 0.0 * j
+    y = y0 + (y1 - y0) * (j / nj) + 0.0 * i
+    return np.ascontiguousarray(x), np.ascontiguousarray(y)
+
+
+def diffuse(T=1.0, U=0.0, V=0.0, D_=1.0):
+    """``DiffuseBC`` (``geom/geom_bc_defs.py:316-353``); U, V are global x/y."""
+    return dict(type=D.DIFFUSE, D=D_, T=T, U=U, V=V)
+
+
+def adjacent(other_block, other_face, orientation=1, flip=D.NO_FLIP):
+    """``AdjacentBC`` (``geom/geom_bc_defs.py:198-217``)."""
+    return dict(type=D.ADJACENT, other_block=other_block, other_face=other_face,
+                orientation=orientation, flip=flip, transform=D.TRANSFORM, flip_normal=0)
+
+
+def inflow(D_=1.0, T=1.0):
+    """``InflowBC`` (``geom/geom_bc_defs.py:416-429``)."""
+    return dict(type=D.INFLOW, D=D_, T=T, U=0.0, V=0.0)
+
+
+def reflect():
+    return dict(type=D.REFLECT)
+
+
+def adsorbing(T=1.0, gamma_f=0.5, k_des=0.01, adsorb=0.5, S_T=1.0, reflect_type="D",
+              cover_initial=0.0, beta_n=0.0, beta_t=0.0):
+    """``AdsorbingBC`` (``geom/geom_bc_defs.py:355-414``) with the extra
+    first-order desorption rate ``k_des`` (per unit time; 0 restores the
+    reference's Langmuir-driven desorption, which needs ``adsorb``).  With
+    reference values of 1, ``alpha_p = 1/S_T`` and ``gamma_f = S_T k_f``
+    (``ugks_data.py:516-518``)."""
+    return dict(type=D.ADSORBING, D=1.0, T=T, U=0.0, V=0.0, gamma_f=gamma_f, alpha_p=1.0 / S_T,
+                S_T=S_T, beta_n=beta_n, beta_t=beta_t, adsorb=adsorb, dynamic=1,
+                reflect_type=reflect_type, cover_initial=cover_initial, k_des=k_des)
+
+
+def base_case(flux_method, Kn, m, vlim, CFL=0.8):
+    return dict(flux_method=flux_method, CFL=CFL, Pr=2.0 / 3.0, gamma=5.0 / 3.0, omega=0.81,
+                Kn_eff=Kn, relax_type=2, delta_dt=1.0,
+                quad=dict(type="Newton", u_num=m, v_num=m, u_min=-vlim, u_max=vlim,
+                          v_min=-vlim, v_max=vlim),
+                blocks=[])
+
+
+def cavity(n=32, m=24, vlim=4.0, flux_method="vanLeer", Kn=0.075, lid=0.15, T_wall=1.0,
+           CFL=0.8, rho=1.0, nj=None):
+    """Single-block lid-driven cavity on the unit square."""
+    nj = n if nj is None else nj
+    case = base_case(flux_method, Kn, m, vlim, CFL)
+    x, y = uniform_grid(n, nj)
+    case["blocks"].append(dict(
+        ni=n, nj=nj, x=x, y=y,
+        bc=[diffuse(T_wall, U=lid), diffuse(T_wall), diffuse(T_wall), diffuse(T_wall)],
+        fill=dict(D=rho, U=0.0, V=0.0, T=1.0, qx=0.0, qy=0.0)))
+    return case
+
+
+def smoothed_density(n, seed=0, amp=0.01, passes=3):
+    """1 + amp*N(0,1) per cell, smoothed by box-filter passes with edge
+    replication; index [i, j] with i along x."""
+    rho = 1.0 + amp * np.random.default_rng(seed).standard_normal((n, n))
+    for _ in range(passes):
+        p = np.pad(rho, 1, mode="edge")
+        rho = sum(p[1 + a:1 + a + n, 1 + b:1 + b + n] for a in (-1, 0, 1) for b in (-1, 0, 1)) / 9.0
+    return rho
+
+
+def cavity_multiblock(nb=2, n=64, m=32, vlim=5.0, flux_method="WENO5", Kn=0.01, lid=0.15,
+                      seed=0, CFL=0.8):
+    """The cavity split into nb x nb blocks of n x n cells (block id = bi*nb + bj,
+    bi along x), connected across every internal face."""
+    case = base_case(flux_method, Kn, m, vlim, CFL)
+    N = nb * n
+    rho = smoothed_density(N, seed)
+    for bi in range(nb):
+        for bj in range(nb):
+            x, y = uniform_grid(n, n, bi / nb, (bi + 1) / nb, bj / nb, (bj + 1) / nb)
+            bid = lambda a, b: a * nb + b
+            bc = [None] * 4
+            bc[D.NORTH] = adjacent(bid(bi, bj + 1), D.SOUTH) if bj + 1 < nb else diffuse(1.0, U=lid)
+            bc[D.SOUTH] = adjacent(bid(bi, bj - 1), D.NORTH) if bj > 0 else diffuse(1.0)
+            bc[D.EAST] = adjacent(bid(bi + 1, bj), D.WEST) if bi + 1 < nb else diffuse(1.0)
+            bc[D.WEST] = adjacent(bid(bi - 1, bj), D.EAST) if bi > 0 else diffuse(1.0)
+            case["blocks"].append(dict(
+                ni=n, nj=n, x=x, y=y, bc=bc,
+                fill=dict(D=np.ascontiguousarray(rho[bi * n:(bi + 1) * n, bj * n:(bj + 1) * n]),
+                          U=0.0, V=0.0, T=1.0, qx=0.0, qy=0.0)))
+    return case
+
+
+def channel(nblocks=4, n=64, m=32, vlim=5.0, flux_method="WENO5", Kn=0.05, rho_in=1.2,
+            rho_out=1.0, length=4.0, height=1.0, gamma_f=0.5, k_des=0.01, CFL=0.8, nj=None):
+    """Pressure-driven channel: nblocks blocks of n x nj cells along x,
+    equilibrium inlet/outlet ghosts, diffuse upper wall, adsorbing lower wall."""
+    nj = n if nj is None else nj
+    case = base_case(flux_method, Kn, m, vlim, CFL)
+    for b in range(nblocks):
+        x, y = uniform_grid(n, nj, length * b / nblocks, length * (b + 1) / nblocks, 0.0, height)
+        bc = [None] * 4
+        bc[D.NORTH] = diffuse(1.0)
+        bc[D.SOUTH] = adsorbing(1.0, gamma_f=gamma_f, k_des=k_des)
+        bc[D.WEST] = adjacent(b - 1, D.EAST) if b > 0 else inflow(rho_in, 1.0)
+        bc[D.EAST] = adjacent(b + 1, D.WEST) if b + 1 < nblocks else inflow(rho_out, 1.0)
+        # linear initial density between inlet and outlet
+        xc = 0.5 * (x[1:, :-1] + x[:-1, :-1])
+        rho = rho_in + (rho_out - rho_in) * xc / length
+        case["blocks"].append(dict(ni=n, nj=nj, x=x, y=y, bc=bc,
+                                   fill=dict(D=np.ascontiguousarray(rho), U=0.0, V=0.0, T=1.0,
+                                             qx=0.0, qy=0.0)))
+    return case
+
+
+CAVITY_SIZES = (24, 32, 48, 64, 96, 128)
+CAVITY_VGRIDS = (16, 24, 32, 48)
+
+
+def batched_cavities(count=64, seed=1):
+    """Independent cavity solves with drawn sizes and parameters: n from
+    {24..128}, velocity grid m from {16..48} on [-5,5]^2, Kn log-uniform on
+    [0.005, 1], lid U(0.05, 0.3), wall T U(0.8, 1.2), vanLeer or WENO5."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        n = int(rng.choice(CAVITY_SIZES))
+        m = int(rng.choice(CAVITY_VGRIDS))
+        Kn = float(10 ** rng.uniform(np.log10(0.005), 0.0))
+        lid = float(rng.uniform(0.05, 0.3))
+        Tw = float(rng.uniform(0.8, 1.2))
+        scheme = "WENO5" if rng.random() < 0.5 else "vanLeer"
+        out.append(cavity(n=n, m=m, vlim=5.0, flux_method=scheme, Kn=Kn, lid=lid, T_wall=Tw))
+    return out
+
+
+def workload_size(case) -> int:
+    """Interior cell-velocity points per step: sum over blocks of ni*nj*Nv."""
+    q = case["quad"]
+    nv = (int(q["u_num"] / 4) * 4 + 1) * (int(q["v_num"] / 4) * 4 + 1)
+    return sum(b["ni"] * b["nj"] for b in case["blocks"]) * nv
