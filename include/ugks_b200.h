@@ -1,0 +1,300 @@
+/* ugks_b200.h -- C ABI of libugks_b200.so, the B200 (sm_100a) UGKS time step.
+ *
+ * Two layers, both plain pointers and sizes:
+ *
+ *  1. Drop-in kernels.  One entry point per pyUGKS OpenCL kernel on the
+ *     time-step path, with the reference kernel's name, argument order and
+ *     meaning.  A pyUGKS-style driver that called
+ *         self.prg.<name>(queue, global_size, local_size, *args)
+ *     calls ugks_<name>(desc, g0, g1, *args, stream) instead: `desc` replaces
+ *     the per-block #define header that ugks_CL.py:20-400 generated, (g0, g1)
+ *     is the reference NDRange (work-group size is irrelevant here), every
+ *     buffer is a device pointer in the reference layout (source/clKernel.c:4-26):
+ *         f-like     [(i*Nj + j)*Nv + v] x (h, b)         (double2)
+ *         macro      [i*nj + j] x (rho, U, V, 1/T)        (double4, no ghosts)
+ *         per face   [(i*Nj + j)*2 + face]                (face 0 = SOUTH, 1 = WEST)
+ *     Each returns 0 on success or a negative cudaError_t on a launch error.
+ *     Nothing is synchronised; work is queued on `stream` (a cudaStream_t,
+ *     NULL = legacy default stream).
+ *
+ *  2. Fused step.  ugks_step_* run a whole UGKS step (both face directions,
+ *     walls, cell update, dt control, ghost exchange) for every block of every
+ *     solve listed in a device-resident block table, with no host
+ *     synchronisation, so that a caller can capture steps in a CUDA graph.
+ *
+ * The library never allocates, frees or keeps device memory: every buffer
+ * belongs to the caller and is borrowed for the duration of the call.
+ */
+#ifndef UGKS_B200_H
+#define UGKS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------
+ * Per-block constants: what the reference baked into each block's OpenCL
+ * header (ugks_CL.py:58-96, 102-156, 270-395).
+ * --------------------------------------------------------------------- */
+typedef struct ugks_block_desc {
+  int32_t ni, nj;        /* interior cells                                  */
+  int32_t Ni, Nj;        /* with ghosts: ni + 2*ghost, nj + 2*ghost         */
+  int32_t ghost;         /* 2 (vanLeer/minmod) or 3 (WENO5)                 */
+  int32_t Nv;            /* discrete velocities                             */
+  int32_t flux_method;   /* 0 vanLeer, 1 WENO5, 3 minmod                    */
+  int32_t relax_type;    /* relaxTime variant 0..3 (clFunctions.c:8-32)     */
+  double PI, Pr, umax, vmax, Kn_eff, gam, K, omega;
+  const double *quad;         /* device [Nv][2] global velocities          */
+  const double *weight;       /* device [Nv] quadrature weights            */
+  const int32_t *mirror_NS;   /* device [Nv] velocity permutations         */
+  const int32_t *mirror_EW;
+  const int32_t *mirror_D;
+  /* wall values of faces N, E, S, W (WALL_<f>_{D,U,V,T,P}; T holds 1/T) */
+  double wall_D[4], wall_U[4], wall_V[4], wall_T[4], wall_P[4];
+  /* adsorbing walls (BETA_N, BETA_T, GAMMA_F, ALPHA_P, ADSORB_<face>)      */
+  double beta_n[4], beta_t[4], gamma_f[4], alpha_p[4], adsorb[4];
+  /* first-order desorption rate (0 = the reference's Langmuir desorption) */
+  double k_des[4];
+  int32_t dynamic[4];          /* DYNAMIC_VARTHETA                         */
+  int32_t constant_adsorb[4];  /* CONSTANT_ADSORB_<face>                   */
+} ugks_block_desc;
+
+/* ------------------------------------------------------------------------
+ * 1. Drop-in kernels (reference: source/clUGKS.c, clKernel.c,
+ *    clGhostRoutines.c, clAdsorb.c).  Arguments follow the __kernel
+ *    signatures; double2/double4/double8 buffers are double* here.
+ * --------------------------------------------------------------------- */
+#define UGKS_STREAM void *stream
+
+/* clUGKS.c:110-199 */
+int ugks_iFace(const ugks_block_desc *d, size_t g0, size_t g1, const double *Fin, double *iface_f,
+               double *fsigma, const double *centre, const double *mid_side, const double *normal,
+               int face, UGKS_STREAM);
+/* clUGKS.c:209-271 */
+int ugks_getFaceCons(const ugks_block_desc *d, size_t g0, size_t g1, const double *iface_f,
+                     const double *normal, int face, double *primary, int offset_bottom,
+                     int offset_top, UGKS_STREAM);
+/* clUGKS.c:273-335 */
+int ugks_getAL(const ugks_block_desc *d, size_t g0, size_t g1, const double *Fin,
+               const double *normal, int face, double *gaL, int offset_bottom, int offset_top,
+               UGKS_STREAM);
+/* clUGKS.c:337-399 */
+int ugks_getAR(const ugks_block_desc *d, size_t g0, size_t g1, const double *Fin,
+               const double *normal, int face, double *gaR, int offset_bottom, int offset_top,
+               UGKS_STREAM);
+/* clUGKS.c:401-442 */
+int ugks_getPLR(const ugks_block_desc *d, size_t g0, size_t g1, const double *centre,
+                const double *mid_side, int face, double *primary, double *gaL, double *gaR,
+                int offset_bottom, int offset_top, UGKS_STREAM);
+/* clUGKS.c:446-518 */
+int ugks_initMacroFlux(const ugks_block_desc *d, size_t g0, size_t g1, double *flux_macro,
+                       int face, double dt, const double *primary, const double *gaL,
+                       const double *gaR, double *gaT, double *gMxi, int offset_bottom,
+                       int offset_top, UGKS_STREAM);
+/* clUGKS.c:522-585 */
+int ugks_calcFaceQ(const ugks_block_desc *d, size_t g0, size_t g1, const double *iface_f,
+                   const double *primary, const double *normal, double *faceQ, int face,
+                   int offset_bottom, int offset_top, UGKS_STREAM);
+/* clUGKS.c:587-681 */
+int ugks_macroFlux(const ugks_block_desc *d, size_t g0, size_t g1, const double *flux_f,
+                   const double *fsigma, double *flux_macro, const double *normal,
+                   const double *side_length, int face, double dt, const double *primary,
+                   const double *faceQ, int offset_bottom, int offset_top, UGKS_STREAM);
+/* clUGKS.c:683-772 */
+int ugks_distFlux(const ugks_block_desc *d, size_t g0, size_t g1, double *flux_f,
+                  const double *fsigma, const double *normal, const double *side_length, int face,
+                  double dt, const double *primary, const double *gaL, const double *gaR,
+                  const double *gaT, const double *gMxi, const double *faceQ, int offset_bottom,
+                  int offset_top, UGKS_STREAM);
+/* clUGKS.c:774-906 */
+int ugks_accommodatingWallDist(const ugks_block_desc *d, size_t g0, size_t g1,
+                               const double *normal, int face, const double *wall_prop,
+                               double *flux_f, double dt, UGKS_STREAM);
+/* clUGKS.c:910-1011 */
+int ugks_wallFlux(const ugks_block_desc *d, size_t g0, size_t g1, const double *normal,
+                  const double *side_length, int face, double *flux_f, double *flux_macro,
+                  double dt, UGKS_STREAM);
+/* clUGKS.c:1019-1147 */
+int ugks_wallMassEnergyFluxes(const ugks_block_desc *d, size_t g0, size_t g1,
+                              const double *normal, const double *side_length, const double *area,
+                              int face, const double *flux_f, double *wall_flux, double dt,
+                              UGKS_STREAM);
+/* clUGKS.c:1158-1187 */
+int ugks_updateMacro(const ugks_block_desc *d, size_t g0, size_t g1, const double *flux_macro_S,
+                     const double *flux_macro_W, const double *area, double *macro,
+                     double *residual, UGKS_STREAM);
+/* clUGKS.c:1189-1257; flag[0] becomes 1.0 if any new f is NaN */
+int ugks_UGKS_update(const ugks_block_desc *d, size_t g0, size_t g1, double *Fin,
+                     const double *flux_f_S, const double *flux_f_W, const double *area,
+                     const double *macro, const double *gQ, const double *residual, double dt,
+                     double *flag, UGKS_STREAM);
+/* clUGKS.c:1259-1277 */
+int ugks_getResidual(const ugks_block_desc *d, size_t g0, size_t g1, const double *macro,
+                     double *residual, UGKS_STREAM);
+/* clUGKS.c:1282-1337 */
+int ugks_edgeMassFlow(const ugks_block_desc *d, size_t g0, size_t g1, const double *macro,
+                      const double *normal, const double *side_length, double *mdot,
+                      int this_face, UGKS_STREAM);
+/* clKernel.c:480-543 */
+int ugks_calcQ(const ugks_block_desc *d, size_t g0, size_t g1, const double *Fin,
+               const double *macro, double *gQ, UGKS_STREAM);
+/* clKernel.c:414-478 */
+int ugks_calcMacro(const ugks_block_desc *d, size_t g0, size_t g1, const double *Fin,
+                   double *macro, UGKS_STREAM);
+/* clKernel.c:382-412 */
+int ugks_initFunctions(const ugks_block_desc *d, size_t g0, size_t g1, double *Fin,
+                       const double *macro, const double *gQ, UGKS_STREAM);
+/* clKernel.c:224-308 */
+int ugks_clFindDT(const ugks_block_desc *d, size_t g0, size_t g1, const double *xy,
+                  const double *area, const double *macro, double *time_step, double Kn,
+                  UGKS_STREAM);
+/* pyopencl.array.max of ugks_block.py:1426: out[0] = max(x[0..n)) */
+int ugks_array_max(const double *x, size_t n, double *out, UGKS_STREAM);
+/* clKernel.c:141-218 (constant wall values; para_def and t are unused there) */
+int ugks_paraBC(const ugks_block_desc *d, size_t g0, size_t g1, const double *para_def,
+                double *wall_prop, double t, UGKS_STREAM);
+/* clGhostRoutines.c:407-538; fB, xyB belong to the neighbour block */
+int ugks_edgeExchange(const ugks_block_desc *d, size_t g0, size_t g1, double *fA,
+                      const double *xyA, int this_face, const double *fB, const double *xyB,
+                      int NIB, int NJB, int that_face, int ori, int flip, UGKS_STREAM);
+/* clGhostRoutines.c:544-597 */
+int ugks_edgeExtrapolate(const ugks_block_desc *d, size_t g0, size_t g1, double *Fin,
+                         int this_face, UGKS_STREAM);
+/* clGhostRoutines.c:603-658 */
+int ugks_edgeConstant(const ugks_block_desc *d, size_t g0, size_t g1, double *Fin,
+                      int this_face, const double *wall_prop, UGKS_STREAM);
+/* clGhostRoutines.c:664-749 */
+int ugks_edgeInflow(const ugks_block_desc *d, size_t g0, size_t g1, double *Fin, int this_face,
+                    const double *normal, const double *macro, const double *gQ,
+                    const double *wall_prop, UGKS_STREAM);
+/* clGhostRoutines.c:755-839 */
+int ugks_edgeOutflow(const ugks_block_desc *d, size_t g0, size_t g1, double *Fin,
+                     int this_face, const double *normal, const double *macro, const double *gQ,
+                     const double *wall_prop, UGKS_STREAM);
+/* clGhostRoutines.c:845-905 */
+int ugks_edgeMirror(const ugks_block_desc *d, size_t g0, size_t g1, double *Fin, int this_face,
+                    UGKS_STREAM);
+/* clGhostRoutines.c:911-961 */
+int ugks_edgeBounceBack(const ugks_block_desc *d, size_t g0, size_t g1, double *Fin,
+                        int this_face, UGKS_STREAM);
+/* clGhostRoutines.c:967-1048 */
+int ugks_edgeConstGrad(const ugks_block_desc *d, size_t g0, size_t g1, double *Fin,
+                       int this_face, UGKS_STREAM);
+/* clAdsorb.c:253-482; flag[0] becomes 4.0 for a tabulated isotherm (not supported) */
+int ugks_adsorbingWall_P1(const ugks_block_desc *d, size_t g0, size_t g1, const double *normal,
+                          int face, const double *wall_prop, double *wall_cover,
+                          double *wall_dist, const double *flux_f, const double *macro,
+                          double dt, double *flag, UGKS_STREAM);
+/* clAdsorb.c:821-975 */
+int ugks_adsorbingWallD_P2(const ugks_block_desc *d, size_t g0, size_t g1, const double *normal,
+                           int face, const double *wall_prop, const double *wall_cover,
+                           const double *wall_dist, double *flux_f, const double *macro,
+                           double dt, UGKS_STREAM);
+
+/* ------------------------------------------------------------------------
+ * 2. Fused step.
+ *
+ * A solve is one pyUGKS simulation (UGKSim); it owns one or more blocks.
+ * The caller keeps, in device memory, an array of ugks_fused_block (one per
+ * block of every solve) and an array of ugks_solve_state (one per solve).
+ * f and the two face-flux arrays of a block are stored as FP64 (double2) by
+ * the *_fp64 entry points and as FP32 (float2) by the *_mixed ones; all
+ * moments, the conserved update, the relaxation and dt stay FP64.
+ * --------------------------------------------------------------------- */
+typedef struct ugks_fused_block {
+  ugks_block_desc d;           /* sizes, constants, tables, wall values    */
+  int32_t solve;               /* index of the owning ugks_solve_state     */
+  int32_t bc_type[4];          /* per face N,E,S,W: geom_bc_defs.py codes  */
+  int32_t bc_block[4];         /* ADJACENT: index (in this table) of the neighbour */
+  int32_t bc_face[4];          /* ADJACENT: neighbour face                 */
+  int32_t bc_ori[4];           /* ADJACENT: orientation flag               */
+  int32_t bc_flip[4];          /* ADJACENT: velocity permutation code      */
+  int32_t face_begin;          /* first face work item of this block       */
+  int32_t cell_begin;          /* first cell work item                     */
+  int32_t ghost_begin;         /* first ghost-cell work item               */
+  int32_t pad_;
+  void *f;                     /* [Ni][Nj][Nv] x (h, b), double or float    */
+  void *flux_S;                /* [Ni][Nj][Nv] x (h, b), SOUTH-face fluxes  */
+  void *flux_W;                /* WEST-face fluxes                          */
+  double *flux_macro_S;        /* [Ni][Nj] x 4                              */
+  double *flux_macro_W;
+  double *macro;               /* [ni][nj] x (rho, U, V, 1/T)               */
+  double *Q;                   /* [ni][nj] x 2 heat flux                    */
+  double *prim_old;            /* [ni][nj] x 4 (the reference's residual buffer) */
+  const double *area;          /* [Ni][Nj]                                  */
+  const double *centre;        /* [Ni][Nj] x 2                              */
+  const double *mid_side;      /* [Ni][Nj][2] x 2                           */
+  const double *normal;        /* [Ni][Nj][2] x 2                           */
+  const double *side_length;   /* [Ni][Nj][2]                               */
+  const double *xy;            /* [Ni+1][Nj+1] x 2                          */
+  double *wall_prop;           /* [max(ni,nj)][4] x 4                       */
+  double *wall_cover;          /* [max(ni,nj)][4] x 4                       */
+  double *wall_fluxes;         /* [max(ni,nj)][4] x 8                       */
+  double *wall_dist;           /* [max(ni,nj)][Nv] x 2                      */
+} ugks_fused_block;
+
+typedef struct ugks_solve_state {
+  double dt;                   /* current time step                         */
+  double time;                 /* simulated time                            */
+  double CFL;
+  double delta_dt;             /* dt growth limit (ugks_sim.py:306)         */
+  double max_dt;               /* CFL / max frequency of the last dt update */
+  unsigned long long max_freq; /* bits of the running max CFL frequency (atomicMax) */
+  int32_t retry;               /* 1 while this step's flux pass is redone   */
+  int32_t status;              /* 0 ok, 1 NaN in f, 4 isotherm, 6 bad block
+                                  connection (clError.c codes otherwise) */
+  int32_t steps;               /* completed steps                           */
+  int32_t retries;             /* flux passes redone so far                 */
+  int32_t active;              /* 0: skipped by every fused kernel          */
+  int32_t nblocks;             /* blocks of this solve                      */
+  double residual[4];          /* written by ugks_residual: mean over blocks
+                                  of sqrt(ni nj sum (dprim)^2) / sum |prim|
+                                  (ugks_block.py:1319-1327, ugks_sim.py:463-468) */
+} ugks_solve_state;
+
+/* Work sizes of a block table (computed on the host): number of face,
+   cell and ghost-cell work items.  Fills face_begin/cell_begin/ghost_begin
+   of the host copy `blocks` and returns the totals. */
+int ugks_fused_layout(ugks_fused_block *blocks, int nblocks, int32_t *n_faces,
+                      int32_t *n_cells, int32_t *n_ghost);
+
+/* Initial state (ugks_block.py:411-429, ugks_sim.py:88-92): f := fEQ(macro,
+   Q) on interior cells, macro := moments(f), Q := heat flux(f), wall_prop
+   from the wall values, ghosts filled, dt := CFL / max frequency. */
+int ugks_init_fp64(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_cells,
+                   int32_t n_ghost, ugks_solve_state *solves_dev, int nsolves, UGKS_STREAM);
+int ugks_init_mixed(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_cells,
+                    int32_t n_ghost, ugks_solve_state *solves_dev, int nsolves, UGKS_STREAM);
+
+/* One UGKSim.one_step (ugks_sim.py:407-501) of every active solve: flux
+   pass, dt check with the reference's single retry, cell update, new dt,
+   time advance, ghost update.  max_nv: largest Nv of the table (sizes the
+   face pass's shared memory, 32 bytes per velocity). */
+int ugks_step_fp64(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_faces,
+                   int32_t n_cells, int32_t n_ghost, int32_t max_nv, ugks_solve_state *solves_dev,
+                   int nsolves, UGKS_STREAM);
+int ugks_step_mixed(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_faces,
+                    int32_t n_cells, int32_t n_ghost, int32_t max_nv, ugks_solve_state *solves_dev,
+                    int nsolves, UGKS_STREAM);
+
+/* Residual of the last step (getResidual + the host reduction of
+   ugks_block.py:1303-1327, averaged over a solve's blocks as
+   ugks_sim.py:463-468 does) into ugks_solve_state.residual. */
+int ugks_residual(const ugks_fused_block *blocks_dev, int nblocks, ugks_solve_state *solves_dev,
+                  int nsolves, UGKS_STREAM);
+
+/* Library identification: returns a static version string. */
+const char *ugks_version(void);
+/* sizeof(ugks_block_desc), sizeof(ugks_fused_block), sizeof(ugks_solve_state),
+   offsetof(ugks_fused_block, f), offsetof(ugks_solve_state, residual),
+   offsetof(ugks_block_desc, wall_D): the first n into out; returns 6.  Lets a
+   binding check its struct layout against the library's. */
+int ugks_abi_sizes(int64_t *out, int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UGKS_B200_H */

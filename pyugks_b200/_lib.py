@@ -1,0 +1,127 @@
+"""ctypes binding of libugks_b200.so (include/ugks_b200.h).
+
+The library is the only compute path of this package: there is no CPU
+fallback.  ``lib()`` raises if the shared object is missing or was built
+against a different struct layout.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libugks_b200.so")
+
+i32, f64, vp = C.c_int32, C.c_double, C.c_void_p
+
+
+class BlockDesc(C.Structure):
+    """ugks_block_desc"""
+    _fields_ = [
+        ("ni", i32), ("nj", i32), ("Ni", i32), ("Nj", i32), ("ghost", i32), ("Nv", i32),
+        ("flux_method", i32), ("relax_type", i32),
+        ("PI", f64), ("Pr", f64), ("umax", f64), ("vmax", f64), ("Kn_eff", f64), ("gam", f64),
+        ("K", f64), ("omega", f64),
+        ("quad", vp), ("weight", vp), ("mirror_NS", vp), ("mirror_EW", vp), ("mirror_D", vp),
+        ("wall_D", f64 * 4), ("wall_U", f64 * 4), ("wall_V", f64 * 4), ("wall_T", f64 * 4),
+        ("wall_P", f64 * 4),
+        ("beta_n", f64 * 4), ("beta_t", f64 * 4), ("gamma_f", f64 * 4), ("alpha_p", f64 * 4),
+        ("adsorb", f64 * 4), ("k_des", f64 * 4),
+        ("dynamic", i32 * 4), ("constant_adsorb", i32 * 4),
+    ]
+
+
+class FusedBlock(C.Structure):
+    """ugks_fused_block"""
+    _fields_ = [
+        ("d", BlockDesc), ("solve", i32),
+        ("bc_type", i32 * 4), ("bc_block", i32 * 4), ("bc_face", i32 * 4), ("bc_ori", i32 * 4),
+        ("bc_flip", i32 * 4),
+        ("face_begin", i32), ("cell_begin", i32), ("ghost_begin", i32), ("pad_", i32),
+        ("f", vp), ("flux_S", vp), ("flux_W", vp), ("flux_macro_S", vp), ("flux_macro_W", vp),
+        ("macro", vp), ("Q", vp), ("prim_old", vp),
+        ("area", vp), ("centre", vp), ("mid_side", vp), ("normal", vp), ("side_length", vp),
+        ("xy", vp), ("wall_prop", vp), ("wall_cover", vp), ("wall_fluxes", vp), ("wall_dist", vp),
+    ]
+
+
+class SolveState(C.Structure):
+    """ugks_solve_state"""
+    _fields_ = [
+        ("dt", f64), ("time", f64), ("CFL", f64), ("delta_dt", f64), ("max_dt", f64),
+        ("max_freq", C.c_uint64),
+        ("retry", i32), ("status", i32), ("steps", i32), ("retries", i32), ("active", i32),
+        ("nblocks", i32),
+        ("residual", f64 * 4),
+    ]
+
+
+# argument kinds of the drop-in kernels in reference order (p pointer, i int,
+# d double); the C functions take (desc*, g0, g1, <args>, stream)
+KERNEL_SIGNATURES = {
+    "paraBC": "ppd", "clFindDT": "ppppd", "initFunctions": "ppp", "calcMacro": "pp",
+    "calcQ": "ppp", "iFace": "ppppppi", "getFaceCons": "ppipii", "getAL": "ppipii",
+    "getAR": "ppipii", "getPLR": "ppipppii", "initMacroFlux": "pidpppppii",
+    "calcFaceQ": "ppppiii", "macroFlux": "pppppidppii", "distFlux": "ppppidppppppii",
+    "accommodatingWallDist": "pippd", "wallFlux": "ppippd", "wallMassEnergyFluxes": "pppippd",
+    "updateMacro": "ppppp", "UGKS_update": "pppppppdp", "getResidual": "pp",
+    "edgeMassFlow": "ppppi", "edgeExchange": "ppippiiiii", "edgeExtrapolate": "pi",
+    "edgeConstant": "pip", "edgeInflow": "pipppp", "edgeOutflow": "pipppp",
+    "edgeMirror": "pi", "edgeBounceBack": "pi", "edgeConstGrad": "pi",
+    "adsorbingWall_P1": "pipppppdp", "adsorbingWallD_P2": "pipppppd",
+}
+_CT = {"p": vp, "i": C.c_int, "d": f64}
+
+_LIB = None
+
+
+class NativeLibraryMissing(RuntimeError):
+    pass
+
+
+def lib():
+    """The loaded library, with prototypes set.  Raises if it is absent."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise NativeLibraryMissing(
+            "libugks_b200.so is not built (run `python -m pyugks_b200.build`); "
+            "there is no CPU fallback")
+    L = C.CDLL(LIB_PATH)
+    for name, sig in KERNEL_SIGNATURES.items():
+        fn = getattr(L, "ugks_" + name)
+        fn.restype = C.c_int
+        fn.argtypes = [C.POINTER(BlockDesc), C.c_size_t, C.c_size_t] + [_CT[k] for k in sig] + [vp]
+    L.ugks_array_max.restype = C.c_int
+    L.ugks_array_max.argtypes = [vp, C.c_size_t, vp, vp]
+    L.ugks_fused_layout.restype = C.c_int
+    L.ugks_fused_layout.argtypes = [C.POINTER(FusedBlock), C.c_int, C.POINTER(i32), C.POINTER(i32),
+                                    C.POINTER(i32)]
+    for nm in ("ugks_init_fp64", "ugks_init_mixed"):
+        fn = getattr(L, nm)
+        fn.restype = C.c_int
+        fn.argtypes = [vp, C.c_int, i32, i32, vp, C.c_int, vp]
+    for nm in ("ugks_step_fp64", "ugks_step_mixed"):
+        fn = getattr(L, nm)
+        fn.restype = C.c_int
+        fn.argtypes = [vp, C.c_int, i32, i32, i32, i32, vp, C.c_int, vp]
+    L.ugks_residual.restype = C.c_int
+    L.ugks_residual.argtypes = [vp, C.c_int, vp, C.c_int, vp]
+    L.ugks_version.restype = C.c_char_p
+    L.ugks_abi_sizes.restype = C.c_int
+    L.ugks_abi_sizes.argtypes = [C.POINTER(C.c_int64), C.c_int]
+    sizes = (C.c_int64 * 6)()
+    L.ugks_abi_sizes(sizes, 6)
+    want = [C.sizeof(BlockDesc), C.sizeof(FusedBlock), C.sizeof(SolveState),
+            FusedBlock.f.offset, SolveState.residual.offset, BlockDesc.wall_D.offset]
+    if list(sizes) != want:
+        raise NativeLibraryMissing("struct layout mismatch with libugks_b200.so: %s vs %s"
+                                   % (list(sizes), want))
+    _LIB = L
+    return L
+
+
+def check(rc: int, what: str):
+    if rc != 0:
+        raise RuntimeError("%s failed: CUDA error %d" % (what, -rc))

@@ -1,0 +1,342 @@
+// ugks_device.cuh -- device physics of the UGKS time step (FP64 arithmetic).
+//
+// Each helper restates one function of the pyUGKS OpenCL sources
+// (file:line at each definition).  The header constants the reference baked
+// in with #define come from ugks_block_desc.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/ugks_b200.h"
+
+namespace ugks {
+
+constexpr int SOUTH = 0, WEST = 1;
+constexpr int GNORTH = 0, GEAST = 1, GSOUTH = 2, GWEST = 3;
+constexpr int NO_FLIP = 0, FLIP_NS = 1, FLIP_D = 2, FLIP_EW = 3;
+// boundary condition codes (geom/geom_bc_defs.py:27-37)
+constexpr int BC_ADJACENT = 0, BC_EXTRAPOLATE_OUT = 1, BC_CONSTANT = 2, BC_REFLECT = 3,
+              BC_DIFFUSE = 4, BC_PERIODIC = 5, BC_INFLOW = 6, BC_OUTFLOW = 7,
+              BC_ADSORBING = 8, BC_BOUNCE_BACK = 9;
+constexpr int MNUM = 7, MTUM = 5;
+
+struct V2 { double x, y; };
+// (rho, U, V, lambda) or conserved (rho, rho U, rho V, E)
+struct P4 { double s0, s1, s2, s3; };
+
+__device__ __forceinline__ V2 v2(double x, double y) { V2 r; r.x = x; r.y = y; return r; }
+__device__ __forceinline__ P4 p4(double a, double b, double c, double e) {
+  P4 r; r.s0 = a; r.s1 = b; r.s2 = c; r.s3 = e; return r;
+}
+__device__ __forceinline__ P4 add(P4 a, P4 b) {
+  return p4(a.s0 + b.s0, a.s1 + b.s1, a.s2 + b.s2, a.s3 + b.s3);
+}
+__device__ __forceinline__ P4 scale(double s, P4 a) { return p4(s * a.s0, s * a.s1, s * a.s2, s * a.s3); }
+
+__device__ __forceinline__ P4 ld4(const double *a, size_t k) {
+  const double2 *p = reinterpret_cast<const double2 *>(a + 4 * k);
+  double2 x = p[0], y = p[1];
+  return p4(x.x, x.y, y.x, y.y);
+}
+__device__ __forceinline__ void st4(double *a, size_t k, P4 v) {
+  double2 *p = reinterpret_cast<double2 *>(a + 4 * k);
+  p[0] = make_double2(v.s0, v.s1);
+  p[1] = make_double2(v.s2, v.s3);
+}
+__device__ __forceinline__ V2 ld2(const double *a, size_t k) {
+  double2 x = reinterpret_cast<const double2 *>(a)[k];
+  return v2(x.x, x.y);
+}
+__device__ __forceinline__ void st2(double *a, size_t k, V2 v) {
+  reinterpret_cast<double2 *>(a)[k] = make_double2(v.x, v.y);
+}
+
+// index helpers for the reference layouts (clKernel.c:4-26)
+__device__ __forceinline__ size_t fidx(const ugks_block_desc &d, long i, long j, long v) {
+  return ((size_t)i * d.Nj + (size_t)j) * d.Nv + (size_t)v;
+}
+__device__ __forceinline__ size_t gidx(const ugks_block_desc &d, long i, long j) {
+  return (size_t)i * d.Nj + (size_t)j;
+}
+__device__ __forceinline__ size_t faceidx(const ugks_block_desc &d, long i, long j, int f) {
+  return ((size_t)i * d.Nj + (size_t)j) * 2 + f;
+}
+__device__ __forceinline__ size_t midx(const ugks_block_desc &d, long i, long j) {
+  return (size_t)i * d.nj + (size_t)j;
+}
+
+// OpenCL sign(): +-1, keeps signed zero, 0 for NaN
+__device__ __forceinline__ double ocl_sign(double a) {
+  return a > 0.0 ? 1.0 : (a < 0.0 ? -1.0 : (a == 0.0 ? a : 0.0));
+}
+// upwind flag (sign(u)*rot + 1)/2 truncated to int: 1 for u*rot > 0 else 0
+__device__ __forceinline__ int upwind_flag(double u, int rot) {
+  return (int)((ocl_sign(u) * rot + 1) / 2);
+}
+
+// relaxTime (clFunctions.c:8-32)
+__device__ __forceinline__ double relax_time(const ugks_block_desc &d, P4 prim) {
+  double p = pow(prim.s3, 1.0 - d.omega);
+  switch (d.relax_type) {
+    case 0: return (d.Kn_eff / prim.s0) * 0.79788456080286541 * p;
+    case 1: return (5. / 8.) * (d.Kn_eff / prim.s0) * sqrt(d.PI) * p;
+    case 3: return (d.Kn_eff / prim.s0) * 2.2567583341910251 * p;
+    default: return (d.Kn_eff / prim.s0) * p;
+  }
+}
+
+// interfaceVelocity (clFunctions.c:191-209)
+__device__ __forceinline__ V2 face_velocity(const ugks_block_desc &d, int v, V2 n) {
+  double2 e = reinterpret_cast<const double2 *>(d.quad)[v];
+  return v2(e.x * n.x + e.y * n.y, e.x * (-n.y) + e.y * n.x);
+}
+__device__ __forceinline__ V2 quad_at(const ugks_block_desc &d, int v) {
+  double2 e = reinterpret_cast<const double2 *>(d.quad)[v];
+  return v2(e.x, e.y);
+}
+// toGlobal / toLocal (clFunctions.c:215-250)
+__device__ __forceinline__ V2 to_global(V2 in, V2 n) {
+  return v2(n.x * in.x + (-n.y) * in.y, n.y * in.x + n.x * in.y);
+}
+__device__ __forceinline__ V2 to_local(V2 in, V2 n) {
+  return v2(in.x * n.x + in.y * n.y, in.x * (-n.y) + in.y * n.x);
+}
+
+// fM (clFunctions.c:49-58): weighted Maxwellian (h, b)
+__device__ __forceinline__ V2 maxwellian(const ugks_block_desc &d, P4 prim, V2 uv, int v) {
+  double cx = uv.x - prim.s1, cy = uv.y - prim.s2;
+  double h = prim.s0 * (prim.s3 / d.PI) * exp(-prim.s3 * (cx * cx + cy * cy));
+  double b = (h * d.K) / (2.0 * prim.s3);
+  double w = d.weight[v];
+  return v2(w * h, w * b);
+}
+// fS (clFunctions.c:64-77)
+__device__ __forceinline__ V2 shakhov(const ugks_block_desc &d, P4 prim, V2 Q, V2 uv, V2 M) {
+  double cx = uv.x - prim.s1, cy = uv.y - prim.s2;
+  double s = 0.8 * (1 - d.Pr) * (prim.s3 * prim.s3) / prim.s0 * (cx * Q.x + cy * Q.y);
+  double part = 2 * prim.s3 * (cx * cx + cy * cy);
+  return v2((s * (part - 4)) * M.x, (s * (part - 2)) * M.y);
+}
+// fEQ (clFunctions.c:79-86)
+__device__ __forceinline__ V2 shakhov_eq(const ugks_block_desc &d, P4 prim, V2 Q, V2 uv, int v) {
+  V2 M = maxwellian(d, prim, uv, v);
+  V2 S = shakhov(d, prim, Q, uv, M);
+  return v2(M.x + S.x, M.y + S.y);
+}
+
+// getPrimary / getConserved / microSlope (clUGKS.c:16-45)
+__device__ __forceinline__ P4 to_primary(const ugks_block_desc &d, P4 w) {
+  P4 p = w;
+  p.s3 = 0.5 * w.s0 / (d.gam - 1.0) / (w.s3 - 0.5 * (w.s1 * w.s1 + w.s2 * w.s2) / w.s0);
+  p.s1 = w.s1 / w.s0;
+  p.s2 = w.s2 / w.s0;
+  return p;
+}
+__device__ __forceinline__ P4 to_conserved(const ugks_block_desc &d, P4 p) {
+  P4 w = p;
+  w.s3 = 0.5 * p.s0 / p.s3 / (d.gam - 1.0) + 0.5 * p.s0 * (p.s1 * p.s1 + p.s2 * p.s2);
+  w.s1 = p.s1 * p.s0;
+  w.s2 = p.s2 * p.s0;
+  return w;
+}
+__device__ __forceinline__ P4 micro_slope(const ugks_block_desc &d, P4 prim, P4 sw) {
+  const double K = d.K;
+  P4 a;
+  a.s3 = 4.0 * (prim.s3 * prim.s3) / (K + 2) / prim.s0 *
+         (2.0 * sw.s3 - 2.0 * prim.s1 * sw.s1 - 2.0 * prim.s2 * sw.s2 +
+          sw.s0 * ((prim.s1 * prim.s1 + prim.s2 * prim.s2) - 0.5 * (K + 2) / prim.s3));
+  a.s2 = 2.0 * prim.s3 / prim.s0 * (sw.s2 - prim.s2 * sw.s0) - prim.s2 * a.s3;
+  a.s1 = 2.0 * prim.s3 / prim.s0 * (sw.s1 - prim.s1 * sw.s0) - prim.s1 * a.s3;
+  a.s0 = sw.s0 / prim.s0 - prim.s1 * a.s1 - prim.s2 * a.s2 -
+         0.5 * ((prim.s1 * prim.s1) + (prim.s2 * prim.s2) + 0.5 * (K + 2) / prim.s3) * a.s3;
+  return a;
+}
+
+// momentU (clUGKS.c:47-80)
+__device__ inline void moments_u(const ugks_block_desc &d, P4 prim, double Mu[MNUM],
+                                 double Mv[MTUM], double Mxi[3], double MuL[MNUM],
+                                 double MuR[MNUM]) {
+  double sl = sqrt(prim.s3);
+  double g = 0.5 * exp(-prim.s3 * (prim.s1 * prim.s1)) / sqrt(d.PI * prim.s3);
+  MuL[0] = 0.5 * erfc(-sl * prim.s1);
+  MuL[1] = prim.s1 * MuL[0] + g;
+  MuR[0] = 0.5 * erfc(sl * prim.s1);
+  MuR[1] = prim.s1 * MuR[0] - g;
+#pragma unroll
+  for (int i = 2; i < MNUM; ++i) {
+    MuL[i] = prim.s1 * MuL[i - 1] + 0.5 * (i - 1) * MuL[i - 2] / prim.s3;
+    MuR[i] = prim.s1 * MuR[i - 1] + 0.5 * (i - 1) * MuR[i - 2] / prim.s3;
+  }
+#pragma unroll
+  for (int i = 0; i < MNUM; ++i) Mu[i] = MuL[i] + MuR[i];
+  Mv[0] = 1.0;
+  Mv[1] = prim.s2;
+#pragma unroll
+  for (int i = 2; i < MTUM; ++i) Mv[i] = prim.s2 * Mv[i - 1] + 0.5 * (i - 1) * Mv[i - 2] / prim.s3;
+  Mxi[0] = 1.0;
+  Mxi[1] = 0.5 * d.K / prim.s3;
+  Mxi[2] = (d.K * d.K + 2.0 * d.K) / (4.0 * prim.s3 * prim.s3);
+}
+// moment_uv (clUGKS.c:82-93)
+__device__ __forceinline__ P4 moment_uv(const double *Mu, const double *Mv, const double *Mxi,
+                                        int a, int b, int dd) {
+  return p4(Mu[a] * Mv[b] * Mxi[dd / 2], Mu[a + 1] * Mv[b] * Mxi[dd / 2],
+            Mu[a] * Mv[b + 1] * Mxi[dd / 2],
+            0.5 * (Mu[a + 2] * Mv[b] * Mxi[dd / 2] + Mu[a] * Mv[b + 2] * Mxi[dd / 2] +
+                   Mu[a] * Mv[b] * Mxi[(dd + 2) / 2]));
+}
+// moment_au (clUGKS.c:95-104)
+__device__ __forceinline__ P4 moment_au(P4 a, const double *Mu, const double *Mv,
+                                        const double *Mxi, int al, int be) {
+  P4 r = scale(a.s0, moment_uv(Mu, Mv, Mxi, al + 0, be + 0, 0));
+  r = add(r, scale(a.s1, moment_uv(Mu, Mv, Mxi, al + 1, be + 0, 0)));
+  r = add(r, scale(a.s2, moment_uv(Mu, Mv, Mxi, al + 0, be + 1, 0)));
+  r = add(r, scale(0.5 * a.s3, moment_uv(Mu, Mv, Mxi, al + 2, be + 0, 0)));
+  r = add(r, scale(0.5 * a.s3, moment_uv(Mu, Mv, Mxi, al + 0, be + 2, 0)));
+  r = add(r, scale(0.5 * a.s3, moment_uv(Mu, Mv, Mxi, al + 0, be + 0, 2)));
+  return r;
+}
+// time-integration weights (clUGKS.c:497-503)
+__device__ __forceinline__ void time_weights(double tau, double dt, double Mt[5]) {
+  double e = exp(-dt / tau);
+  Mt[3] = tau * (1.0 - e);
+  Mt[4] = -tau * dt * e + tau * Mt[3];
+  Mt[0] = dt - Mt[3];
+  Mt[1] = -tau * Mt[0] + Mt[4];
+  Mt[2] = (dt * dt) / 2.0 - tau * Mt[0];
+}
+
+// limiters (clFunctions.c:255-353)
+__device__ __forceinline__ double vanleer(double s1, double s2) {
+  return (ocl_sign(s1) + ocl_sign(s2)) * (fabs(s1) * fabs(s2)) / (fabs(s1) + fabs(s2) + 1e-16);
+}
+__device__ __forceinline__ double weno5(double S0, double S1, double S2, double S3, double S4,
+                                        double dx) {
+  const double eps = 1E-16;
+  double t1, t2;
+  t1 = S0 - 2.0 * S1 + S2;
+  t2 = S0 - 4.0 * S1 + 3.0 * S2;
+  double B0 = (13.0 / 12.0) * t1 * t1 + 0.25 * t2 * t2;
+  t1 = S1 - 2.0 * S2 + S3;
+  t2 = S1 - S3;
+  double B1 = (13.0 / 12.0) * t1 * t1 + 0.25 * t2 * t2;
+  t1 = S2 - 2.0 * S3 + S4;
+  t2 = 3.0 * S2 - 4.0 * S3 + S4;
+  double B2 = (13.0 / 12.0) * t1 * t1 + 0.25 * t2 * t2;
+  t1 = eps + B0; double a0 = 0.1 / (t1 * t1);
+  t1 = eps + B1; double a1 = 0.6 / (t1 * t1);
+  t1 = eps + B2; double a2 = 0.3 / (t1 * t1);
+  double s = a0 + a1 + a2;
+  double f0 = (1. / 3.) * S0 - (7. / 6.) * S1 + (11. / 6.) * S2;
+  double f1 = -(1. / 6.) * S1 + (5. / 6.) * S2 + (1. / 3.) * S3;
+  double f2 = (1. / 3.) * S2 + (5. / 6.) * S3 - (1. / 6.) * S4;
+  double fL = (a0 / s) * f0 + (a1 / s) * f1 + (a2 / s) * f2;
+  return (fL - S2) / dx;
+}
+__device__ __forceinline__ double minmod(double a, double b) {
+  double out = 0.0;
+  if ((fabs(a) < fabs(b)) && (a * b > 0)) out = a;
+  else if ((fabs(b) < fabs(a)) && (a * b > 0)) out = b;
+  else if (a == b) out = a;
+  return out;
+}
+
+// stickingProbability (clAdsorb.c:6-16)
+__device__ __forceinline__ double sticking(const ugks_block_desc &d, V2 uv, double T, int face) {
+  double nrm = 1.0 - d.beta_n[face] * exp(-uv.x * uv.x / T);
+  double tan_ = 1.0 - d.beta_t[face] * (1.0 - exp(-uv.y * uv.y / T));
+  return nrm * tan_;
+}
+
+// ---------------------------------------------------------------------------
+// block-wide sums: every thread passes N partial sums and receives the totals.
+// `scratch` is shared memory of at least N * (blockDim.x / 32) doubles.
+// ---------------------------------------------------------------------------
+template <int N>
+__device__ __forceinline__ void block_sum(double (&x)[N], double *scratch) {
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x[k] += __shfl_xor_sync(0xffffffffu, x[k], o);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();  // scratch may still be read by a previous call
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) scratch[k * nw + warp] = x[k];
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += scratch[k * nw + w];
+    x[k] = s;
+  }
+}
+
+// (h, b) pairs stored as double2 or float2
+template <typename T> struct Store;
+template <> struct Store<double> {
+  using vec = double2;
+  __device__ __forceinline__ static V2 load(const void *base, size_t k) {
+    double2 x = reinterpret_cast<const double2 *>(base)[k];
+    return v2(x.x, x.y);
+  }
+  __device__ __forceinline__ static void store(void *base, size_t k, V2 v) {
+    reinterpret_cast<double2 *>(base)[k] = make_double2(v.x, v.y);
+  }
+};
+template <> struct Store<float> {
+  using vec = float2;
+  __device__ __forceinline__ static V2 load(const void *base, size_t k) {
+    float2 x = reinterpret_cast<const float2 *>(base)[k];
+    return v2((double)x.x, (double)x.y);
+  }
+  __device__ __forceinline__ static void store(void *base, size_t k, V2 v) {
+    reinterpret_cast<float2 *>(base)[k] = make_float2((float)v.x, (float)v.y);
+  }
+};
+
+__device__ __forceinline__ void rot90(int &i, int &j, int n, int Ni, int Nj) {
+  for (int a = 0; a < n; a++) {
+    int t = i;
+    i = Nj - j - 1;
+    j = t;
+    t = Ni; Ni = Nj; Nj = t;
+  }
+}
+
+// getSwapIndex for cell indices (clGhostRoutines.c:47-138 with v == 0);
+// also used by the fused ghost kernel
+__device__ __forceinline__ void swap_cell_index(int NI, int NJ, int G, int this_face, int &iB, int &jB,
+                                     int that_face, int NIB, int NJB) {
+  switch (this_face) {
+    case GEAST:
+      if (that_face == GEAST) { iB = (NI - 1) - iB; iB += NIB - 2 * G; }
+      else if (that_face == GWEST) { iB -= NI - 2 * G; }
+      else if (that_face == GNORTH) { rot90(iB, jB, 3, NI, NJ); jB += NJB - 2 * G; }
+      else { rot90(iB, jB, 1, NI, NJ); jB -= NI - 2 * G; }
+      break;
+    case GWEST:
+      if (that_face == GWEST) { iB = (NI - 1) - iB; iB -= NI - 2 * G; }
+      else if (that_face == GEAST) { iB += NIB - 2 * G; }
+      else if (that_face == GNORTH) { rot90(iB, jB, 1, NI, NJ); jB += NJB - 2 * G; }
+      else { rot90(iB, jB, 3, NI, NJ); jB -= NI - 2 * G; }
+      break;
+    case GNORTH:
+      if (that_face == GNORTH) { jB = (NJ - 1) - jB; jB += NJB - 2 * G; }
+      else if (that_face == GSOUTH) { jB -= NJ - 2 * G; }
+      else if (that_face == GEAST) { rot90(iB, jB, 1, NI, NJ); iB += NIB - 2 * G; }
+      else { rot90(iB, jB, 3, NI, NJ); iB -= NJ - 2 * G; }
+      break;
+    default:
+      if (that_face == GSOUTH) { jB = (NJ - 1) - jB; jB -= NJ - 2 * G; }
+      else if (that_face == GNORTH) { jB += NJB - 2 * G; }
+      else if (that_face == GEAST) { rot90(iB, jB, 3, NI, NJ); iB += NIB - 2 * G; }
+      else { rot90(iB, jB, 1, NI, NJ); iB -= NJ - 2 * G; }
+      break;
+  }
+}
+
+
+}  // namespace ugks

@@ -1,0 +1,903 @@
+// ugks_fused.cu -- the whole UGKS time step in five launches, for every block
+// of every solve of a device-resident block table.
+//
+// Per step (UGKSim.one_step, ugks_sim.py:407-501):
+//   face pass   one CTA per face of either direction: reconstruction (iFace),
+//               face moments (getFaceCons/getAL/getAR), slopes (getPLR),
+//               initMacroFlux, calcFaceQ, macroFlux and distFlux fused, or the
+//               wall procedure for wall faces (accommodatingWallDist |
+//               adsorbingWall_P1 + adsorbingWallD_P2, then wallFlux and
+//               wallMassEnergyFluxes).  The per-velocity interface
+//               distribution and slope stay in shared memory between the
+//               three velocity sweeps a face needs (moments -> heat flux ->
+//               flux), so f is read once per face from HBM/L2.
+//   dt check    updateTimeStep inside the dt loop (ugks_sim.py:430-441):
+//               device-side, sets the retry flag of a solve whose dt changed.
+//   face pass   again, only for solves whose retry flag is set.
+//   cell pass   one CTA per cell: calcQ, updateMacro and UGKS_update fused,
+//               plus the cell's CFL frequency (clFindDT) and residual terms.
+//   dt update   calcTimeStep + updateTimeStep + time advance, device-side.
+//   ghost pass  one CTA per ghost cell of every block face (updateBC).
+// Nothing reads the host in between, so a step can be captured in a graph.
+#include <cuda_runtime.h>
+#include <float.h>
+
+#include "ugks_device.cuh"
+
+using namespace ugks;
+
+namespace {
+
+constexpr int FT = 128;  // threads per face / cell / ghost CTA
+
+inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+inline int launch_status() {
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? 0 : -(int)e;
+}
+
+// block of work item w: the last block whose begin <= w (begins are ascending)
+template <int WHICH>
+__device__ __forceinline__ int find_block(const ugks_fused_block *B, int nb, int w) {
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    int mid = (lo + hi + 1) >> 1;
+    int beg = WHICH == 0 ? B[mid].face_begin : (WHICH == 1 ? B[mid].cell_begin : B[mid].ghost_begin);
+    if (beg <= w) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ bool is_wall(int bc) { return bc == BC_DIFFUSE || bc == BC_ADSORBING; }
+
+// dt update of updateTimeStep (ugks_sim.py:285-311) with limit = True
+__device__ __forceinline__ double limited_dt(double dt_old, double dt_new, double delta) {
+  if (dt_old != dt_new) {
+    if (dt_new > (1.0 + delta) * dt_old) dt_new = (1.0 + delta) * dt_old;
+    return dt_new;
+  }
+  return dt_old;
+}
+
+// ---------------------------------------------------------------------------
+// face pass
+// ---------------------------------------------------------------------------
+struct FaceShared {
+  double scratch[16 * (FT / 32)];
+  double bcast[48];
+};
+
+template <typename T>
+__global__ void __launch_bounds__(FT) face_pass(const ugks_fused_block *__restrict__ B, int nb,
+                                                ugks_solve_state *__restrict__ solves, int retry_pass) {
+  extern __shared__ double dyn[];
+  __shared__ FaceShared sh;
+  using St = Store<T>;
+
+  const int w = blockIdx.x;
+  const int bi = find_block<0>(B, nb, w);
+  const ugks_fused_block &blk = B[bi];
+  const ugks_block_desc &d = blk.d;
+  ugks_solve_state &sol = solves[blk.solve];
+  if (!sol.active) return;
+  if (retry_pass && !sol.retry) return;
+  const double dt = sol.dt;
+
+  // work item -> (i, j, direction); items run over the (ni+1) x (nj+1) corner
+  // grid with S and W faces of the same (i, j) adjacent, so that both face
+  // directions of a cell read f while it is in L2
+  int lf = w - blk.face_begin;
+  const int dir = lf & 1;
+  lf >>= 1;
+  const int mi = lf / (d.nj + 1), mj = lf % (d.nj + 1);
+  if (dir == SOUTH ? (mi >= d.ni) : (mj >= d.nj)) return;
+
+  const int Nv = d.Nv, G = d.ghost;
+  const long gi = mi + G, gj = mj + G;
+  // wall id of this face, or -1
+  int wall = -1;
+  if (dir == SOUTH) {
+    if (mj == 0 && is_wall(blk.bc_type[GSOUTH])) wall = GSOUTH;
+    else if (mj == d.nj && is_wall(blk.bc_type[GNORTH])) wall = GNORTH;
+  } else {
+    if (mi == 0 && is_wall(blk.bc_type[GWEST])) wall = GWEST;
+    else if (mi == d.ni && is_wall(blk.bc_type[GEAST])) wall = GEAST;
+  }
+
+  double *fh = dyn, *fb = dyn + Nv, *sgh = dyn + 2 * Nv, *sgb = dyn + 3 * Nv;
+  const V2 n = ld2(blk.normal, faceidx(d, gi, gj, dir));
+  const V2 mid = ld2(blk.mid_side, faceidx(d, gi, gj, dir));
+  const int L = d.flux_method == 1 ? 5 : 3, MID = d.flux_method == 1 ? 2 : 1;
+  // stencil geometry for both upwind directions (iFace, clUGKS.c:148-176)
+  double dist[2], l1[2];
+#pragma unroll
+  for (int dl = 0; dl < 2; ++dl) {
+    long c0i, c0j, c1i, c1j;  // centre of cell MID and MID-1
+    if (dir == SOUTH) {
+      c0i = c1i = gi;
+      c0j = dl ? gj - MID - 1 + MID : gj + MID - MID;
+      c1j = dl ? gj - MID - 1 + MID - 1 : gj + MID - (MID - 1);
+    } else {
+      c0j = c1j = gj;
+      c0i = dl ? gi - MID - 1 + MID : gi + MID - MID;
+      c1i = dl ? gi - MID - 1 + MID - 1 : gi + MID - (MID - 1);
+    }
+    V2 c0 = ld2(blk.centre, gidx(d, c0i, c0j)), c1 = ld2(blk.centre, gidx(d, c1i, c1j));
+    dist[dl] = sqrt((mid.x - c0.x) * (mid.x - c0.x) + (mid.y - c0.y) * (mid.y - c0.y));
+    l1[dl] = sqrt((c0.x - c1.x) * (c0.x - c1.x) + (c0.y - c1.y) * (c0.y - c1.y));
+  }
+  const size_t step = dir == SOUTH ? (size_t)Nv : (size_t)d.Nj * Nv;  // stencil stride
+  const size_t base = fidx(d, gi, gj, 0);
+
+  // ---- sweep 1: reconstruction (+ interior: conserved moments W, WL, WR)
+  double m[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) m[k] = 0.0;
+  for (int v = threadIdx.x; v < Nv; v += FT) {
+    const V2 uv = face_velocity(d, v, n);
+    const int delta = (int)((ocl_sign(uv.x) + 1) / 2);
+    double sh_[5], sb_[5];
+#pragma unroll
+    for (int s = 0; s < 5; ++s) {
+      if (s < L) {
+        long off = delta ? (long)(-MID - 1 + s) : (long)(MID - s);
+        V2 f = St::load(blk.f, base + v + off * (long)step);
+        sh_[s] = f.x;
+        sb_[s] = f.y;
+      }
+    }
+    const double ds = dist[delta];
+    double sx, sy;
+    if (d.flux_method == 0) {
+      const double l = l1[delta];
+      sx = vanleer((sh_[1] - sh_[0]) / l, (sh_[2] - sh_[1]) / l);
+      sy = vanleer((sb_[1] - sb_[0]) / l, (sb_[2] - sb_[1]) / l);
+    } else if (d.flux_method == 1) {
+      sx = weno5(sh_[0], sh_[1], sh_[2], sh_[3], sh_[4], ds);
+      sy = weno5(sb_[0], sb_[1], sb_[2], sb_[3], sb_[4], ds);
+    } else {
+      sx = (sh_[1] + 0.5 * minmod(sh_[2] - sh_[1], sh_[1] - sh_[0]) - sh_[1]) / ds;
+      sy = (sb_[1] + 0.5 * minmod(sb_[2] - sb_[1], sb_[1] - sb_[0]) - sb_[1]) / ds;
+    }
+    const double ffh = sh_[MID] + sx * ds, ffb = sb_[MID] + sy * ds;
+    fh[v] = ffh;
+    fb[v] = ffb;
+    sgh[v] = sx;
+    sgb[v] = sy;
+    if (wall < 0) {
+      const double uu = uv.x * uv.x + uv.y * uv.y;
+      // left / right cells of the face are stencil cells MID and MID+1
+      const double lh = delta ? sh_[MID] : sh_[MID + 1], lb = delta ? sb_[MID] : sb_[MID + 1];
+      const double rh = delta ? sh_[MID + 1] : sh_[MID], rb = delta ? sb_[MID + 1] : sb_[MID];
+      m[0] += ffh; m[1] += uv.x * ffh; m[2] += uv.y * ffh; m[3] += 0.5 * (uu * ffh + ffb);
+      m[4] += lh; m[5] += uv.x * lh; m[6] += uv.y * lh; m[7] += 0.5 * (uu * lh + lb);
+      m[8] += rh; m[9] += uv.x * rh; m[10] += uv.y * rh; m[11] += 0.5 * (uu * rh + rb);
+    }
+  }
+  const double len = blk.side_length[faceidx(d, gi, gj, dir)];
+
+  if (wall < 0) {
+    // ---------------- interior face ----------------
+    block_sum<12>(m, sh.scratch);
+    if (threadIdx.x == 0) {
+      // getPLR (clUGKS.c:401-442)
+      const P4 W = p4(m[0], m[1], m[2], m[3]);
+      const P4 prim = to_primary(d, W);
+      const V2 cl = ld2(blk.centre, gidx(d, gi - dir, gj - (1 - dir)));
+      const V2 cr = ld2(blk.centre, gidx(d, gi, gj));
+      const double dl = sqrt((mid.x - cl.x) * (mid.x - cl.x) + (mid.y - cl.y) * (mid.y - cl.y));
+      const double dr = sqrt((mid.x - cr.x) * (mid.x - cr.x) + (mid.y - cr.y) * (mid.y - cr.y));
+      const P4 aL = micro_slope(d, prim, p4((W.s0 - m[4]) / dl, (W.s1 - m[5]) / dl,
+                                            (W.s2 - m[6]) / dl, (W.s3 - m[7]) / dl));
+      const P4 aR = micro_slope(d, prim, p4((m[8] - W.s0) / dr, (m[9] - W.s1) / dr,
+                                            (m[10] - W.s2) / dr, (m[11] - W.s3) / dr));
+      // initMacroFlux (clUGKS.c:446-518)
+      double Mu[MNUM], Mv[MTUM], Mxi[3], MuL[MNUM], MuR[MNUM], Mt[5];
+      moments_u(d, prim, Mu, Mv, Mxi, MuL, MuR);
+      const P4 aT = micro_slope(d, prim, scale(-prim.s0, add(moment_au(aL, MuL, Mv, Mxi, 1, 0),
+                                                             moment_au(aR, MuR, Mv, Mxi, 1, 0))));
+      time_weights(relax_time(d, prim), dt, Mt);
+      const P4 g0 = scale(prim.s0,
+                          add(add(scale(Mt[0], moment_uv(Mu, Mv, Mxi, 1, 0, 0)),
+                                  scale(Mt[1], add(moment_au(aL, MuL, Mv, Mxi, 2, 0),
+                                                   moment_au(aR, MuR, Mv, Mxi, 2, 0)))),
+                              scale(Mt[2], moment_au(aT, Mu, Mv, Mxi, 1, 0))));
+      double *c = sh.bcast;
+      c[0] = prim.s0; c[1] = prim.s1; c[2] = prim.s2; c[3] = prim.s3;
+      c[4] = aL.s0; c[5] = aL.s1; c[6] = aL.s2; c[7] = aL.s3;
+      c[8] = aR.s0; c[9] = aR.s1; c[10] = aR.s2; c[11] = aR.s3;
+      c[12] = aT.s0; c[13] = aT.s1; c[14] = aT.s2; c[15] = aT.s3;
+      c[16] = Mt[0]; c[17] = Mt[1]; c[18] = Mt[2]; c[19] = Mt[3]; c[20] = Mt[4];
+      c[21] = Mxi[2];
+      c[22] = g0.s0; c[23] = g0.s1; c[24] = g0.s2; c[25] = g0.s3;
+    }
+    __syncthreads();
+    const double *c = sh.bcast;
+    const P4 prim = p4(c[0], c[1], c[2], c[3]);
+    // ---- sweep 2: face heat flux (calcFaceQ, clUGKS.c:522-585)
+    double q[2] = {0.0, 0.0};
+    for (int v = threadIdx.x; v < Nv; v += FT) {
+      const V2 uv = face_velocity(d, v, n);
+      const double cx = uv.x - prim.s1, cy = uv.y - prim.s2, c2 = cx * cx + cy * cy;
+      const double t = c2 * fh[v] + fb[v] / d.K;
+      q[0] += 0.5 * (cx * t);
+      q[1] += 0.5 * (cy * t);
+    }
+    block_sum<2>(q, sh.scratch);
+    const V2 Q = v2(q[0], q[1]);
+    const P4 aL = p4(c[4], c[5], c[6], c[7]), aR = p4(c[8], c[9], c[10], c[11]);
+    const P4 aT = p4(c[12], c[13], c[14], c[15]);
+    const double Mt[5] = {c[16], c[17], c[18], c[19], c[20]};
+    const double Mxi2 = c[21];
+    // ---- sweep 3: macroFlux (587-681) and distFlux (683-772)
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    void *flux = dir == SOUTH ? blk.flux_S : blk.flux_W;
+    for (int v = threadIdx.x; v < Nv; v += FT) {
+      const V2 uv = face_velocity(d, v, n);
+      const int delta = (int)((ocl_sign(uv.x) + 1) / 2);
+      const V2 f0 = maxwellian(d, prim, uv, v);
+      const V2 F0 = shakhov(d, prim, Q, uv, f0);
+      const double u = uv.x, vt = uv.y, uu = u * u + vt * vt;
+      const double fdh = fh[v], fdb = fb[v], fsh = sgh[v], fsb = sgb[v];
+      acc[0] += Mt[0] * u * F0.x + Mt[3] * u * fdh - Mt[4] * u * u * fsh;
+      acc[1] += Mt[0] * u * u * F0.x + Mt[3] * u * u * fdh - Mt[4] * u * u * u * fsh;
+      acc[2] += Mt[0] * vt * u * F0.x + Mt[3] * vt * u * fdh - Mt[4] * vt * u * u * fsh;
+      acc[3] += Mt[0] * 0.5 * (u * uu * F0.x + u * F0.y) + Mt[3] * 0.5 * (u * uu * fdh + u * fdb) -
+                Mt[4] * 0.5 * (u * u * uu * fsh + u * u * fsb);
+      const P4 a = delta ? aL : aR;
+      const double ph = a.s0 * f0.x + a.s1 * u * f0.x + a.s2 * vt * f0.x + 0.5 * a.s3 * (uu * f0.x + f0.y);
+      const double pb = a.s0 * f0.y + a.s1 * u * f0.y + a.s2 * vt * f0.y + 0.5 * a.s3 * (uu * f0.y + Mxi2 * f0.x);
+      const double th = aT.s0 * f0.x + aT.s1 * u * f0.x + aT.s2 * vt * f0.x + 0.5 * aT.s3 * (uu * f0.x + f0.y);
+      const double tb = aT.s0 * f0.y + aT.s1 * u * f0.y + aT.s2 * vt * f0.y + 0.5 * aT.s3 * (uu * f0.y + Mxi2 * f0.x);
+      const double hx = Mt[0] * u * (f0.x + F0.x) + Mt[1] * (u * u) * ph + Mt[2] * u * th +
+                        Mt[3] * u * fdh - Mt[4] * (u * u) * fsh;
+      const double hy = Mt[0] * u * (f0.y + F0.y) + Mt[1] * (u * u) * pb + Mt[2] * u * tb +
+                        Mt[3] * u * fdb - Mt[4] * (u * u) * fsb;
+      St::store(flux, base + v, v2(len * hx, len * hy));
+    }
+    block_sum<4>(acc, sh.scratch);
+    if (threadIdx.x == 0) {
+      P4 out = add(p4(acc[0], acc[1], acc[2], acc[3]), p4(c[22], c[23], c[24], c[25]));
+      const V2 g = to_global(v2(out.s1, out.s2), n);
+      out.s1 = g.x;
+      out.s2 = g.y;
+      st4(dir == SOUTH ? blk.flux_macro_S : blk.flux_macro_W, gidx(d, gi, gj), scale(len, out));
+    }
+    return;
+  }
+
+  // ---------------- wall face ----------------
+  const int rot = (wall == GNORTH || wall == GEAST) ? -1 : 1;
+  const long ci = dir == SOUTH ? mi : mj;
+  P4 wl = ld4(blk.wall_prop, ci * 4 + wall);
+  {
+    const V2 t = to_local(v2(wl.s1, wl.s2), n);
+    wl.s1 = t.x;
+    wl.s2 = t.y;
+  }
+  __syncthreads();  // sweep 1 results in shared memory
+  if (blk.bc_type[wall] == BC_DIFFUSE) {
+    // accommodatingWallDist (clUGKS.c:774-906)
+    double s[2] = {0.0, 0.0};
+    for (int v = threadIdx.x; v < Nv; v += FT) {
+      const V2 uv = face_velocity(d, v, n);
+      const int delta = upwind_flag(uv.x, rot);
+      s[0] += uv.x * (1 - delta) * fh[v];
+      s[1] -= uv.x * delta * maxwellian(d, wl, uv, v).x;
+    }
+    block_sum<2>(s, sh.scratch);
+    const double ratio = s[0] / s[1];
+    for (int v = threadIdx.x; v < Nv; v += FT) {
+      const V2 uv = face_velocity(d, v, n);
+      const int delta = upwind_flag(uv.x, rot);
+      const V2 M = maxwellian(d, wl, uv, v);
+      fh[v] = ratio * delta * M.x + (1 - delta) * fh[v];
+      fb[v] = ratio * delta * M.y + (1 - delta) * fb[v];
+    }
+  } else {
+    // adsorbingWall_P1 (clAdsorb.c:253-482)
+    const long ti = dir == SOUTH ? mi : (wall == GEAST ? d.ni - 1 : 0);
+    const long tj = dir == SOUTH ? (wall == GNORTH ? d.nj - 1 : 0) : mj;
+    const double Tw = 1.0 / blk.macro[4 * midx(d, ti, tj) + 3];
+    double *cover = blk.wall_cover + 4 * (ci * 4 + wall);
+    const double theta = cover[0];
+    const double gf = d.gamma_f[wall];
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int v = threadIdx.x; v < Nv; v += FT) {
+      const V2 uv = face_velocity(d, v, n);
+      const int delta = upwind_flag(uv.x, rot);
+      const double k = -rot * uv.x * (1 - delta);
+      const V2 total = v2(k * fh[v], k * fb[v]);
+      const double beta = sticking(d, uv, Tw, wall);
+      V2 ads = v2(beta * total.x * gf * (1.0 - theta), beta * total.y * gf * (1.0 - theta));
+      const double fs = ocl_sign(total.x);
+      if ((fs * ads.x) > (fs * total.x)) ads = total;
+      const V2 refl = v2(total.x - ads.x, total.y - ads.y);
+      s[0] += refl.x;
+      s[1] += ads.x;
+      s[2] += beta * total.x;
+      st2(blk.wall_dist, (size_t)ci * Nv + v, v2(refl.x / uv.x, refl.y / uv.x));
+    }
+    block_sum<3>(s, sh.scratch);
+    if (threadIdx.x == 0) {
+      double ads_final = s[1], dvt = 0.0, des = 0.0;
+      bool ok = true;
+      if (gf > 0.0) {
+        if (d.dynamic[wall] == 1) {
+          dvt = dt * d.alpha_p[wall] * s[1];
+          if (dvt > (1 - theta)) {
+            dvt = 1 - theta;
+            ads_final = dvt / dt * d.alpha_p[wall];  // the reference's form (clAdsorb.c:420)
+          }
+        }
+        if (!d.constant_adsorb[wall]) {
+          atomicExch(&sol.status, 4);
+          ok = false;
+        } else {
+          if (d.k_des[wall] > 0.0) des = d.k_des[wall] * theta / d.alpha_p[wall];
+          else des = gf * (1.0 / d.adsorb[wall] - 1.0) * s[2] * theta;
+          if (d.dynamic[wall] == 1) {
+            dvt -= dt * d.alpha_p[wall] * des;
+            if ((theta + dvt) < 0.0) des = theta / (dt * d.alpha_p[wall]);
+          }
+        }
+      }
+      double corr = 1.0;
+      if (ok) {
+        const double refl_final = s[0] + s[1] - ads_final;
+        corr = refl_final / s[0];
+        cover[0] += dvt;
+        cover[1] = refl_final;
+        cover[2] = ads_final;
+        cover[3] = des;
+      }
+      sh.bcast[0] = corr;
+      sh.bcast[1] = ok ? 1.0 : 0.0;
+    }
+    __syncthreads();
+    const double corr = sh.bcast[0];
+    const bool ok = sh.bcast[1] != 0.0;
+    if (corr != 1.0)
+      for (int v = threadIdx.x; v < Nv; v += FT) {
+        const size_t k = (size_t)ci * Nv + v;
+        const V2 x = ld2(blk.wall_dist, k);
+        st2(blk.wall_dist, k, v2(x.x * corr, x.y * corr));
+      }
+    if (!ok) return;  // the reference skips the rest of this wall (ugks_block.py:949-950)
+    // adsorbingWallD_P2 (clAdsorb.c:821-975)
+    const double refl = cover[1], des = cover[3], ads = cover[2];
+    double ratio = 1.0;
+    if (refl > 0.0) {
+      double r[1] = {0.0};
+      for (int v = threadIdx.x; v < Nv; v += FT) {
+        const V2 uv = face_velocity(d, v, n);
+        const int delta = upwind_flag(uv.x, rot);
+        const V2 dif = delta ? maxwellian(d, wl, uv, v) : v2(0.0, 0.0);
+        fh[v] = delta * dif.x + (1 - delta) * fh[v];
+        fb[v] = delta * dif.y + (1 - delta) * fb[v];
+        r[0] += rot * uv.x * dif.x;
+      }
+      block_sum<1>(r, sh.scratch);
+      ratio = refl / r[0];
+    }
+    const int account = ((des == 0.0) && (ads > 0.0) && (refl == 0.0)) ? 1 : 0;
+    P4 wd = wl;
+    wd.s0 = 2 * des * sqrt(d.PI * wl.s3);
+    for (int v = threadIdx.x; v < Nv; v += FT) {
+      const V2 uv = face_velocity(d, v, n);
+      const int delta = upwind_flag(uv.x, rot);
+      const double sc = 1 - delta * (1 - ratio);
+      double x = fh[v] * sc, y = fb[v] * sc;
+      const V2 M = maxwellian(d, wd, uv, v);
+      x += delta * M.x;
+      y += delta * M.y;
+      x -= account * delta * x;
+      y -= account * delta * y;
+      fh[v] = x;
+      fb[v] = y;
+    }
+  }
+  // wallFlux (clUGKS.c:910-1011) and wallMassEnergyFluxes (1019-1147)
+  void *flux = dir == SOUTH ? blk.flux_S : blk.flux_W;
+  double s[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) s[k] = 0.0;
+  for (int v = threadIdx.x; v < Nv; v += FT) {
+    const V2 uv = face_velocity(d, v, n);
+    const double wh = fh[v], wb = fb[v];
+    const double oh = uv.x * wh * len * dt, ob = uv.x * wb * len * dt;
+    St::store(flux, base + v, v2(oh, ob));
+    const double uu = uv.x * uv.x + uv.y * uv.y;
+    s[0] += uv.x * wh;
+    s[1] += uv.x * uv.x * wh;
+    s[2] += uv.x * uv.y * wh;
+    s[3] += 0.5 * uv.x * (uu * wh + wb);
+    const int delta = upwind_flag(uv.x, rot);
+    const double ix = (1 - delta) * oh, iy = (1 - delta) * ob, ox = delta * oh, oy = delta * ob;
+    s[4] += ix; s[5] += uv.x * ix; s[6] += uv.y * ix; s[7] += 0.5 * (uu * ix + iy);
+    s[8] += ox; s[9] += uv.x * ox; s[10] += uv.y * ox; s[11] += 0.5 * (uu * ox + oy);
+  }
+  block_sum<12>(s, sh.scratch);
+  if (threadIdx.x == 0) {
+    const V2 g = to_global(v2(s[1], s[2]), n);
+    st4(dir == SOUTH ? blk.flux_macro_S : blk.flux_macro_W, gidx(d, gi, gj),
+        scale(dt * len, p4(s[0], g.x, g.y, s[3])));
+    double *wf = blk.wall_fluxes + 8 * (ci * 4 + wall);
+    wf[0] = -rot * s[4]; wf[1] = rot * s[8]; wf[2] = -rot * s[5]; wf[3] = rot * s[9];
+    wf[4] = -rot * s[6]; wf[5] = rot * s[10]; wf[6] = -rot * s[7]; wf[7] = rot * s[11];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// cell pass: calcQ (clKernel.c:480-543) + updateMacro (clUGKS.c:1158-1187) +
+// UGKS_update (clUGKS.c:1189-1257) + clFindDT (clKernel.c:224-308) + the
+// residual terms of getResidual (clUGKS.c:1259-1277)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double cfl_freq(const ugks_fused_block &blk, P4 m, long mi, long mj) {
+  const ugks_block_desc &d = blk.d;
+  const long G = d.ghost, NY = d.Nj + 1;
+  const double *xy = blk.xy;
+  const V2 a = ld2(xy, (mi + 1 + G) * NY + mj + G), b = ld2(xy, (mi + 1 + G) * NY + mj + 1 + G);
+  const V2 c = ld2(xy, (mi + G) * NY + mj + 1 + G), e = ld2(xy, (mi + G) * NY + mj + G);
+  const double dx = fmax(fmax(fmax(fabs(a.x - b.x), fabs(c.x - b.x)), fmax(fabs(c.x - e.x), fabs(a.x - e.x))),
+                         fmax(fabs(c.x - a.x), fabs(b.x - e.x)));
+  const double dy = fmax(fmax(fmax(fabs(a.y - b.y), fabs(c.y - b.y)), fmax(fabs(c.y - e.y), fabs(a.y - e.y))),
+                         fmax(fabs(c.y - a.y), fabs(b.y - e.y)));
+  const double sos = sqrt(0.5 * d.gam / m.s3);
+  const double lo_u = fmin(d.umax, fabs(m.s1) + sos), lo_v = fmin(d.vmax, fabs(m.s2) + sos);
+  const double hi_u = fmax(d.umax, fabs(m.s1) + sos), hi_v = fmax(d.vmax, fabs(m.s2) + sos);
+  // clFindDT is called with the host's unrounded Kn (ugks_block.py:1421)
+  const double sc = (erf(10 * (d.Kn_eff - 1e-3)) + 1) / 2.0;
+  const double u = sc * (hi_u - lo_u) + lo_u, v = sc * (hi_v - lo_v) + lo_v;
+  return (dx * u + dy * v) / blk.area[gidx(d, mi + G, mj + G)];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(FT) cell_pass(const ugks_fused_block *__restrict__ B, int nb,
+                                                ugks_solve_state *__restrict__ solves) {
+  __shared__ double scratch[2 * (FT / 32)];
+  __shared__ double bc[12];
+  using St = Store<T>;
+  const int w = blockIdx.x;
+  const int bi = find_block<1>(B, nb, w);
+  const ugks_fused_block &blk = B[bi];
+  const ugks_block_desc &d = blk.d;
+  ugks_solve_state &sol = solves[blk.solve];
+  if (!sol.active) return;
+  const double dt = sol.dt;
+  const int lc = w - blk.cell_begin;
+  const long mi = lc / d.nj, mj = lc % d.nj;
+  const long gi = mi + d.ghost, gj = mj + d.ghost;
+  const int Nv = d.Nv;
+  const size_t base = fidx(d, gi, gj, 0);
+  const P4 old = ld4(blk.macro, midx(d, mi, mj));
+  // calcQ on f^n with the macro of f^n
+  double q[2] = {0.0, 0.0};
+  for (int v = threadIdx.x; v < Nv; v += FT) {
+    const V2 f = St::load(blk.f, base + v);
+    const V2 e = quad_at(d, v);
+    const double cx = e.x - old.s1, cy = e.y - old.s2, c2 = cx * cx + cy * cy;
+    const double t = c2 * f.x + f.y / d.K;
+    q[0] += 0.5 * (cx * t);
+    q[1] += 0.5 * (cy * t);
+  }
+  block_sum<2>(q, scratch);
+  if (threadIdx.x == 0) {
+    st2(blk.Q, midx(d, mi, mj), v2(q[0], q[1]));
+    // updateMacro
+    const P4 wc = to_conserved(d, old);
+    const double A = blk.area[gidx(d, gi, gj)];
+    const P4 s0 = ld4(blk.flux_macro_S, gidx(d, gi, gj)), s1 = ld4(blk.flux_macro_S, gidx(d, gi, gj + 1));
+    const P4 w0 = ld4(blk.flux_macro_W, gidx(d, gi, gj)), w1 = ld4(blk.flux_macro_W, gidx(d, gi + 1, gj));
+    const P4 nw = p4(wc.s0 + (s0.s0 - s1.s0 + w0.s0 - w1.s0) / A, wc.s1 + (s0.s1 - s1.s1 + w0.s1 - w1.s1) / A,
+                     wc.s2 + (s0.s2 - s1.s2 + w0.s2 - w1.s2) / A, wc.s3 + (s0.s3 - s1.s3 + w0.s3 - w1.s3) / A);
+    const P4 prim = to_primary(d, nw);
+    st4(blk.macro, midx(d, mi, mj), prim);
+    st4(blk.prim_old, midx(d, mi, mj), old);
+    bc[0] = prim.s0; bc[1] = prim.s1; bc[2] = prim.s2; bc[3] = prim.s3;
+    bc[4] = relax_time(d, old);
+    bc[5] = relax_time(d, prim);
+    bc[6] = A;
+    // CFL frequency of the updated cell (clFindDT)
+    const double fq = cfl_freq(blk, prim, mi, mj);
+    atomicMax(&sol.max_freq, (unsigned long long)__double_as_longlong(fq));
+  }
+  __syncthreads();
+  const P4 prim = p4(bc[0], bc[1], bc[2], bc[3]);
+  const double tau_old = bc[4], tau = bc[5], A = bc[6];
+  const V2 Q = v2(q[0], q[1]);
+  const double den = 1.0 + 0.5 * dt / tau;
+  const size_t sj = (size_t)Nv, si = (size_t)d.Nj * Nv;
+  bool nan = false;
+  for (int v = threadIdx.x; v < Nv; v += FT) {
+    const V2 e = quad_at(d, v);
+    const V2 fo = shakhov_eq(d, old, Q, e, v);
+    const V2 fn = shakhov_eq(d, prim, Q, e, v);
+    const size_t k = base + v;
+    const V2 f = St::load(blk.f, k);
+    const V2 a0 = St::load(blk.flux_S, k), a1 = St::load(blk.flux_S, k + sj);
+    const V2 b0 = St::load(blk.flux_W, k), b1 = St::load(blk.flux_W, k + si);
+    const double flh = (a0.x - a1.x + b0.x - b1.x) / A, flb = (a0.y - a1.y + b0.y - b1.y) / A;
+    const double rh = fn.x / tau + (fo.x - f.x) / tau_old, rb = fn.y / tau + (fo.y - f.y) / tau_old;
+    const V2 out = v2((f.x + flh + 0.5 * dt * rh) / den, (f.y + flb + 0.5 * dt * rb) / den);
+    nan |= isnan(out.x) || isnan(out.y);
+    St::store(blk.f, k, out);
+  }
+  if (nan) atomicExch(&sol.status, 1);
+}
+
+// ---------------------------------------------------------------------------
+// ghost pass (UGKSBlock.updateBC, ugks_block.py:621-665): one CTA per ghost
+// cell of every block face
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(FT) ghost_pass(const ugks_fused_block *__restrict__ B, int nb,
+                                                 const ugks_solve_state *__restrict__ solves) {
+  using St = Store<T>;
+  const int w = blockIdx.x;
+  const int bi = find_block<2>(B, nb, w);
+  const ugks_fused_block &blk = B[bi];
+  const ugks_block_desc &d = blk.d;
+  if (!solves[blk.solve].active) return;
+  const int G = d.ghost, Nv = d.Nv;
+  // strips in face order N, E, S, W: N/S have ni*G cells, E/W G*nj
+  int lc = w - blk.ghost_begin;
+  int face = 0;
+  const int ns_cells = d.ni * G, ew_cells = G * d.nj;
+  for (face = 0; face < 4; ++face) {
+    const int c = (face == GNORTH || face == GSOUTH) ? ns_cells : ew_cells;
+    if (lc < c) break;
+    lc -= c;
+  }
+  long a, b;  // NDRange ids of the reference edge kernels
+  if (face == GNORTH || face == GSOUTH) { a = lc / G; b = lc % G; }
+  else { a = lc / d.nj; b = lc % d.nj; }
+  long gi = a, gj = b;
+  switch (face) {
+    case GNORTH: gi += G; gj += d.Nj - G; break;
+    case GEAST: gi += d.Ni - G; gj += G; break;
+    case GSOUTH: gi += G; break;
+    default: gj += G; break;
+  }
+  const size_t dst = fidx(d, gi, gj, 0);
+  const int t = blk.bc_type[face];
+  if (t == BC_ADJACENT || t == BC_PERIODIC) {
+    // edgeExchange (clGhostRoutines.c:407-538)
+    const ugks_fused_block &ob = B[blk.bc_block[face]];
+    const int that = blk.bc_face[face], NI = d.Ni, NJ = d.Nj, NIB = ob.d.Ni, NJB = ob.d.Nj;
+    int a1i, a1j, a2i, a2j, b1i, b1j, b2i, b2j;
+    auto corners = [&](int f, int NI_, int NJ_, int &p, int &q, int &r, int &s) {
+      switch (f) {
+        case GNORTH: p = G; q = NJ_ - G; r = NI_ - G; s = NJ_ - G; break;
+        case GEAST: p = NI_ - G; q = G; r = NI_ - G; s = NJ_ - G; break;
+        case GSOUTH: p = G; q = G; r = NI_ - G; s = G; break;
+        default: p = G; q = G; r = G; s = NJ_ - G; break;
+      }
+    };
+    corners(face, NI, NJ, a1i, a1j, a2i, a2j);
+    corners(that, NIB, NJB, b1i, b1j, b2i, b2j);
+    const V2 A1 = ld2(blk.xy, (size_t)a1i * (NJ + 1) + a1j), A2 = ld2(blk.xy, (size_t)a2i * (NJ + 1) + a2j);
+    const V2 B1 = ld2(ob.xy, (size_t)b1i * (NJB + 1) + b1j), B2 = ld2(ob.xy, (size_t)b2i * (NJB + 1) + b2j);
+    const bool misalign = !(fabs(A1.x - B1.x) <= 1e-6) || !(fabs(A1.y - B1.y) <= 1e-6) ||
+                          !(fabs(A2.x - B2.x) <= 1e-6) || !(fabs(A2.y - B2.y) <= 1e-6);
+    int iB = (int)gi, jB = (int)gj;
+    if (misalign && blk.bc_ori[face]) {
+      if (face == GEAST || face == GWEST) jB = (NJ - 1) - jB;
+      else iB = (NI - 1) - iB;
+    }
+    swap_cell_index(NI, NJ, G, face, iB, jB, that, NIB, NJB);
+    if (iB < 0 || iB >= NIB || jB < 0 || jB >= NJB || ob.d.Nv != Nv) {
+      // connection that does not map onto the neighbour: flag, do not read
+      if (threadIdx.x == 0) atomicExch(const_cast<int32_t *>(&solves[blk.solve].status), 6);
+      return;
+    }
+    const size_t src = ((size_t)iB * NJB + jB) * (size_t)Nv;
+    const int flip = blk.bc_flip[face];
+    const int32_t *perm = flip == FLIP_NS ? d.mirror_NS : (flip == FLIP_D ? d.mirror_D : d.mirror_EW);
+    using Vec = typename St::vec;
+    const Vec *s = reinterpret_cast<const Vec *>(ob.f) + src;
+    Vec *o = reinterpret_cast<Vec *>(blk.f) + dst;
+    for (int v = threadIdx.x; v < Nv; v += FT) o[v] = s[flip == NO_FLIP ? v : perm[v]];
+  } else if (t == BC_DIFFUSE || t == BC_ADSORBING) {
+    // edgeConstGrad (clGhostRoutines.c:967-1048)
+    long ei0, ej0, ei1, ej1;
+    double m;
+    switch (face) {
+      case GNORTH: ei1 = gi; ej1 = d.Nj - G - 1; ei0 = ei1; ej0 = ej1 - 1; m = (double)(gj - ej1); break;
+      case GEAST: ei1 = d.Ni - G - 1; ej1 = gj; ei0 = ei1 - 1; ej0 = ej1; m = (double)(gi - ei1); break;
+      case GSOUTH: ei1 = gi; ej1 = G; ei0 = ei1; ej0 = ej1 + 1; m = (double)(ej1 - gj); break;
+      default: ei1 = G; ej1 = gj; ei0 = ei1 + 1; ej0 = ej1; m = (double)(ei1 - gi); break;
+    }
+    const size_t k0 = fidx(d, ei0, ej0, 0), k1 = fidx(d, ei1, ej1, 0);
+    for (int v = threadIdx.x; v < Nv; v += FT) {
+      const V2 f0 = St::load(blk.f, k0 + v), f1 = St::load(blk.f, k1 + v);
+      St::store(blk.f, dst + v, v2(__dadd_rn(f1.x, __dmul_rn(m, __dsub_rn(f1.x, f0.x))),
+                                   __dadd_rn(f1.y, __dmul_rn(m, __dsub_rn(f1.y, f0.y)))));
+    }
+  } else if (t == BC_EXTRAPOLATE_OUT || t == BC_REFLECT || t == BC_BOUNCE_BACK) {
+    long si, sj;
+    const int32_t *perm = nullptr;
+    if (t == BC_EXTRAPOLATE_OUT) {  // edgeExtrapolate (544-597)
+      switch (face) {
+        case GNORTH: si = gi; sj = d.Nj - G - 1; break;
+        case GEAST: si = d.Ni - G - 1; sj = gj; break;
+        case GSOUTH: si = gi; sj = G; break;
+        default: si = G; sj = gj; break;
+      }
+    } else {  // edgeMirror / edgeBounceBack (845-961)
+      switch (face) {
+        case GNORTH: si = gi; sj = 2 * (d.Nj - G) - gj - 1; perm = d.mirror_NS; break;
+        case GEAST: si = 2 * (d.Ni - G) - gi - 1; sj = gj; perm = d.mirror_EW; break;
+        case GSOUTH: si = gi; sj = 2 * G - gj - 1; perm = d.mirror_NS; break;
+        default: si = 2 * G - gi - 1; sj = gj; perm = d.mirror_EW; break;
+      }
+      if (t == BC_BOUNCE_BACK) perm = d.mirror_D;
+    }
+    using Vec = typename St::vec;
+    Vec *F = reinterpret_cast<Vec *>(blk.f);
+    const size_t src = fidx(d, si, sj, 0);
+    for (int v = threadIdx.x; v < Nv; v += FT) F[dst + v] = F[src + (perm ? perm[v] : v)];
+  } else if (t == BC_CONSTANT || t == BC_INFLOW || t == BC_OUTFLOW) {
+    const long ci = (face == GNORTH || face == GSOUTH) ? a : b;
+    const P4 wp = ld4(blk.wall_prop, ci * 4 + face);
+    P4 prim = wp;
+    V2 Q = v2(0.0, 0.0);
+    if (t != BC_CONSTANT) {
+      // edgeInflow / edgeOutflow (664-839)
+      long ei, ej, noi, noj;
+      int fid;
+      switch (face) {
+        case GNORTH: ei = gi; ej = d.Nj - G - 1; noi = gi; noj = gj; fid = SOUTH; break;
+        case GEAST: ei = d.Ni - G - 1; ej = gj; noi = gi; noj = gj; fid = WEST; break;
+        case GSOUTH: ei = gi; ej = G; noi = ei; noj = ej; fid = SOUTH; break;
+        default: ei = G; ej = gj; noi = ei; noj = ej; fid = WEST; break;
+      }
+      Q = ld2(blk.Q, midx(d, ei - G, ej - G));
+      prim = ld4(blk.macro, midx(d, ei - G, ej - G));
+      const V2 uv = to_local(v2(prim.s1, prim.s2), ld2(blk.normal, faceidx(d, noi, noj, fid)));
+      prim.s1 = uv.x;
+      prim.s2 = uv.y;
+      if (t == BC_OUTFLOW) {
+        prim.s3 = prim.s0 / (wp.s0 / wp.s3);
+      } else {
+        prim.s0 = wp.s0;
+        prim.s3 = wp.s3;
+      }
+    }
+    for (int v = threadIdx.x; v < Nv; v += FT) St::store(blk.f, dst + v, shakhov_eq(d, prim, Q, quad_at(d, v), v));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// dt control (ugks_sim.py:285-311, 430-446, 458-460, 491)
+// ---------------------------------------------------------------------------
+// after a flux pass: updateTimeStep inside the dt loop; phase 0 sets retry
+__global__ void dt_check(ugks_solve_state *solves, int ns, int phase) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  ugks_solve_state &x = solves[s];
+  if (!x.active) return;
+  if (phase == 0) {
+    const double dt = limited_dt(x.dt, x.max_dt, x.delta_dt);
+    x.retry = dt != x.dt;
+    x.dt = dt;
+  } else if (x.retry) {
+    x.dt = limited_dt(x.dt, x.max_dt, x.delta_dt);
+    x.retries += 1;
+  }
+}
+
+// after the cell pass: calcTimeStep + updateTimeStep, time += dt, residual
+__global__ void dt_update(ugks_solve_state *solves, int ns) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  ugks_solve_state &x = solves[s];
+  if (!x.active) return;
+  const double fq = __longlong_as_double((long long)x.max_freq);
+  x.max_dt = x.CFL / fq;
+  x.dt = limited_dt(x.dt, x.max_dt, x.delta_dt);
+  x.time += x.dt;
+  x.steps += 1;
+  x.max_freq = 0ull;
+  x.retry = 0;
+}
+
+// ---------------------------------------------------------------------------
+// initial state (ugks_block.py:411-429, ugks_sim.py:88-92)
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(FT) init_cells(const ugks_fused_block *__restrict__ B, int nb,
+                                                 ugks_solve_state *__restrict__ solves) {
+  __shared__ double scratch[4 * (FT / 32)];
+  using St = Store<T>;
+  const int w = blockIdx.x;
+  const int bi = find_block<1>(B, nb, w);
+  const ugks_fused_block &blk = B[bi];
+  const ugks_block_desc &d = blk.d;
+  ugks_solve_state &sol = solves[blk.solve];
+  if (!sol.active) return;
+  const int lc = w - blk.cell_begin;
+  const long mi = lc / d.nj, mj = lc % d.nj;
+  const size_t base = fidx(d, mi + d.ghost, mj + d.ghost, 0);
+  // initFunctions
+  P4 prim = ld4(blk.macro, midx(d, mi, mj));
+  V2 Q = ld2(blk.Q, midx(d, mi, mj));
+  double m[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int v = threadIdx.x; v < d.Nv; v += FT) {
+    const V2 e = quad_at(d, v);
+    const V2 f = shakhov_eq(d, prim, Q, e, v);
+    St::store(blk.f, base + v, f);
+    const V2 fs = St::load(blk.f, base + v);  // moments of f as stored
+    m[0] += fs.x;
+    m[1] += e.x * fs.x;
+    m[2] += e.y * fs.x;
+    m[3] += 0.5 * ((e.x * e.x + e.y * e.y) * fs.x + fs.y);
+  }
+  // calcMacro
+  block_sum<4>(m, scratch);
+  prim = to_primary(d, p4(m[0], m[1], m[2], m[3]));
+  // calcQ
+  double q[2] = {0.0, 0.0};
+  for (int v = threadIdx.x; v < d.Nv; v += FT) {
+    const V2 f = St::load(blk.f, base + v);
+    const V2 e = quad_at(d, v);
+    const double cx = e.x - prim.s1, cy = e.y - prim.s2, c2 = cx * cx + cy * cy;
+    const double t = c2 * f.x + f.y / d.K;
+    q[0] += 0.5 * (cx * t);
+    q[1] += 0.5 * (cy * t);
+  }
+  block_sum<2>(q, scratch);
+  if (threadIdx.x == 0) {
+    st4(blk.macro, midx(d, mi, mj), prim);
+    st2(blk.Q, midx(d, mi, mj), v2(q[0], q[1]));
+    const double fq = cfl_freq(blk, prim, mi, mj);
+    atomicMax(&sol.max_freq, (unsigned long long)__double_as_longlong(fq));
+  }
+}
+
+// paraBC (clKernel.c:141-218) for constant wall values, every block
+__global__ void init_walls(const ugks_fused_block *B, int nb) {
+  const ugks_fused_block &blk = B[blockIdx.x];
+  const ugks_block_desc &d = blk.d;
+  const int wl = max(d.ni, d.nj);
+  for (int ci = threadIdx.x; ci < wl; ci += blockDim.x)
+    for (int f = 0; f < 4; ++f) {
+      const bool ns = (f == GNORTH || f == GSOUTH);
+      if (ns ? !(ci < d.ni) : !(ci < d.nj)) continue;
+      const double l = (d.wall_P[f] != -1) ? d.wall_P[f] / d.wall_D[f] : d.wall_T[f];
+      st4(blk.wall_prop, ci * 4 + f, p4(d.wall_D[f], d.wall_U[f], d.wall_V[f], l));
+    }
+}
+
+// calcTimeStep + updateTimeStep(limit=False) at start-up
+__global__ void dt_init(ugks_solve_state *solves, int ns) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  ugks_solve_state &x = solves[s];
+  if (!x.active) return;
+  x.max_dt = x.CFL / __longlong_as_double((long long)x.max_freq);
+  if (x.dt != x.max_dt) x.dt = x.max_dt;
+  x.max_freq = 0ull;
+  x.retry = 0;
+}
+
+template <typename T>
+int init_impl(const ugks_fused_block *B, int nb, int32_t n_cells, int32_t n_ghost,
+              ugks_solve_state *solves, int ns, void *stream) {
+  cudaStream_t st = S(stream);
+  init_walls<<<nb, 128, 0, st>>>(B, nb);
+  if (n_cells) init_cells<T><<<n_cells, FT, 0, st>>>(B, nb, solves);
+  dt_init<<<(ns + 127) / 128, 128, 0, st>>>(solves, ns);
+  if (n_ghost) ghost_pass<T><<<n_ghost, FT, 0, st>>>(B, nb, solves);
+  return launch_status();
+}
+
+template <typename T>
+int step_impl(const ugks_fused_block *B, int nb, int32_t n_faces, int32_t n_cells, int32_t n_ghost,
+              ugks_solve_state *solves, int ns, int max_nv, void *stream) {
+  cudaStream_t st = S(stream);
+  const size_t smem = (size_t)4 * sizeof(double) * (size_t)max_nv;
+  static bool attr_set = false;  // one flag per instantiation
+  if (!attr_set) {
+    cudaFuncSetAttribute(face_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    attr_set = true;
+  }
+  if (smem > 200 * 1024) return -(int)cudaErrorInvalidValue;
+  const unsigned sg = (unsigned)((ns + 127) / 128);
+  if (n_faces) face_pass<T><<<n_faces, FT, smem, st>>>(B, nb, solves, 0);
+  dt_check<<<sg, 128, 0, st>>>(solves, ns, 0);
+  if (n_faces) face_pass<T><<<n_faces, FT, smem, st>>>(B, nb, solves, 1);
+  dt_check<<<sg, 128, 0, st>>>(solves, ns, 1);
+  if (n_cells) cell_pass<T><<<n_cells, FT, 0, st>>>(B, nb, solves);
+  dt_update<<<sg, 128, 0, st>>>(solves, ns);
+  if (n_ghost) ghost_pass<T><<<n_ghost, FT, 0, st>>>(B, nb, solves);
+  return launch_status();
+}
+
+// residual (getResidual, clUGKS.c:1259-1277, and ugks_block.py:1316-1327):
+// one CTA per solve walks its blocks
+__global__ void residual_kernel(const ugks_fused_block *B, int nb, ugks_solve_state *solves, int ns) {
+  __shared__ double scratch[8 * (FT / 32)];
+  const int s = blockIdx.x;
+  if (s >= ns) return;
+  double r[4] = {0.0, 0.0, 0.0, 0.0};
+  int n = 0;
+  for (int b = 0; b < nb; ++b) {
+    if (B[b].solve != s) continue;
+    const ugks_fused_block &blk = B[b];
+    const int cells = blk.d.ni * blk.d.nj;
+    double a[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    for (int c = threadIdx.x; c < cells; c += blockDim.x) {
+      const P4 p = ld4(blk.macro, c), o = ld4(blk.prim_old, c);
+      a[0] += (p.s0 - o.s0) * (p.s0 - o.s0);
+      a[1] += (p.s1 - o.s1) * (p.s1 - o.s1);
+      a[2] += (p.s2 - o.s2) * (p.s2 - o.s2);
+      a[3] += (p.s3 - o.s3) * (p.s3 - o.s3);
+      a[4] += fabs(p.s0);
+      a[5] += fabs(p.s1);
+      a[6] += fabs(p.s2);
+      a[7] += fabs(p.s3);
+    }
+    block_sum<8>(a, scratch);
+    for (int k = 0; k < 4; ++k) {
+      const double v = sqrt((double)cells * a[k]) / (a[4 + k] + DBL_MIN);
+      r[k] += v <= 0.0 ? 1.0 : v;
+    }
+    ++n;
+  }
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 4; ++k) solves[s].residual[k] = n ? r[k] / n : 0.0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ugks_step_fp64(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_faces, int32_t n_cells,
+                   int32_t n_ghost, int32_t max_nv, ugks_solve_state *solves_dev, int nsolves,
+                   void *stream) {
+  return step_impl<double>(blocks_dev, nblocks, n_faces, n_cells, n_ghost, solves_dev, nsolves,
+                           max_nv, stream);
+}
+int ugks_step_mixed(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_faces, int32_t n_cells,
+                    int32_t n_ghost, int32_t max_nv, ugks_solve_state *solves_dev, int nsolves,
+                    void *stream) {
+  return step_impl<float>(blocks_dev, nblocks, n_faces, n_cells, n_ghost, solves_dev, nsolves,
+                          max_nv, stream);
+}
+int ugks_residual(const ugks_fused_block *blocks_dev, int nblocks, ugks_solve_state *solves_dev,
+                  int nsolves, void *stream) {
+  if (nsolves <= 0) return 0;
+  residual_kernel<<<nsolves, FT, 0, S(stream)>>>(blocks_dev, nblocks, solves_dev, nsolves);
+  return launch_status();
+}
+
+int ugks_fused_layout(ugks_fused_block *blocks, int nblocks, int32_t *n_faces, int32_t *n_cells,
+                      int32_t *n_ghost) {
+  int64_t f = 0, c = 0, g = 0;
+  for (int b = 0; b < nblocks; ++b) {
+    ugks_fused_block &x = blocks[b];
+    x.face_begin = (int32_t)f;
+    x.cell_begin = (int32_t)c;
+    x.ghost_begin = (int32_t)g;
+    f += 2ll * (x.d.ni + 1) * (x.d.nj + 1);
+    c += (int64_t)x.d.ni * x.d.nj;
+    g += 2ll * x.d.ghost * (x.d.ni + x.d.nj);
+  }
+  if (f > INT32_MAX || c > INT32_MAX || g > INT32_MAX) return -1;
+  *n_faces = (int32_t)f;
+  *n_cells = (int32_t)c;
+  *n_ghost = (int32_t)g;
+  return 0;
+}
+
+int ugks_init_fp64(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_cells, int32_t n_ghost,
+                   ugks_solve_state *solves_dev, int nsolves, void *stream) {
+  return init_impl<double>(blocks_dev, nblocks, n_cells, n_ghost, solves_dev, nsolves, stream);
+}
+int ugks_init_mixed(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_cells, int32_t n_ghost,
+                    ugks_solve_state *solves_dev, int nsolves, void *stream) {
+  return init_impl<float>(blocks_dev, nblocks, n_cells, n_ghost, solves_dev, nsolves, stream);
+}
+
+}  // extern "C"

@@ -42,5 +42,6 @@ ERR_ADSORB_TOO_MUCH = 2
 ERR_DESORB_TOO_MUCH = 3
 ERR_CLAMPING_ADSORB_ISOTHERM = 4
 ERR_TIMEOUT = 5
+ERR_BAD_CONNECTION = 6
 
 FLUX_METHODS = {"vanLeer": 0, "WENO5": 1, "minmod": 3}

@@ -1,0 +1,248 @@
+"""Fused time stepping: every block of every solve in one device-resident table.
+
+``FusedSolver`` owns, as torch CUDA tensors, all per-block state of one or
+more solves (a solve = one pyUGKS simulation, possibly multi-block) and
+advances them with the fused entry points of libugks_b200.so:
+
+* ``ugks_step_fp64`` / ``ugks_step_mixed``: one ``UGKSim.one_step`` of every
+  active solve in five kernel launches plus two tiny dt launches, with dt
+  control, the reference's single flux retry, and the ghost update done on
+  the device (no host synchronisation inside a step);
+* ``ugks_residual``: the reference residual on demand.
+
+``precision="fp64"`` stores f and the face fluxes as double (the plain
+method); ``"mixed"`` stores them as float, with moments, the conserved update,
+the relaxation and dt in FP64.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from . import defs as D
+from .problem import Constants, fill_arrays, geometry, wall_values
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class _Block:
+    pass
+
+
+class FusedSolver:
+    def __init__(self, cases, precision: str = "fp64", device="cuda", stream=None):
+        torch = _torch()
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(precision)
+        self.lib = _lib.lib()
+        if not torch.cuda.is_available():
+            raise RuntimeError("FusedSolver needs a CUDA device (no CPU fallback)")
+        self.precision = precision
+        self.device = torch.device(device)
+        self.sdtype = torch.float64 if precision == "fp64" else torch.float32
+        if isinstance(cases, dict):
+            cases = [cases]
+        self.cases = list(cases)
+        self.blocks = []
+        self.solve_blocks = []
+        self._keep = []
+        structs = []
+        for s, case in enumerate(self.cases):
+            const = Constants(case)
+            geoms = geometry(case, const.ghost)
+            vg = const.vgrid
+            tabs = dict(quad=self._dev(vg.quad), weight=self._dev(vg.weight),
+                        mNS=self._dev(vg.mirror_NS, torch.int32), mEW=self._dev(vg.mirror_EW, torch.int32),
+                        mD=self._dev(vg.mirror_D, torch.int32))
+            self._keep.append(tabs)
+            first = len(self.blocks)
+            ids = []
+            for k, (b, g) in enumerate(zip(case["blocks"], geoms)):
+                blk = self._make_block(s, k, first, case, b, g, const, tabs)
+                ids.append(len(self.blocks))
+                self.blocks.append(blk)
+                structs.append(blk.struct)
+            self.solve_blocks.append(ids)
+        arr = (_lib.FusedBlock * len(structs))(*structs)
+        nf, nc, ng = _lib.i32(), _lib.i32(), _lib.i32()
+        _lib.check(self.lib.ugks_fused_layout(arr, len(structs), C.byref(nf), C.byref(nc), C.byref(ng)) and -1,
+                   "ugks_fused_layout")
+        self.n_faces, self.n_cells, self.n_ghost = nf.value, nc.value, ng.value
+        self.max_nv = max(b.Nv for b in self.blocks)
+        raw = np.frombuffer(bytes(arr), dtype=np.uint8).copy()
+        self.table = torch.from_numpy(raw).to(self.device)
+        self.nblocks = len(structs)
+        st = (_lib.SolveState * len(self.cases))()
+        for s, case in enumerate(self.cases):
+            st[s].CFL = float(case["CFL"])
+            st[s].delta_dt = float(case.get("delta_dt", 1.0))
+            st[s].active = 1
+            st[s].nblocks = len(self.solve_blocks[s])
+        self.solves = torch.from_numpy(np.frombuffer(bytes(st), dtype=np.uint8).copy()).to(self.device)
+        self.nsolves = len(self.cases)
+        self._stream = stream
+        init = self.lib.ugks_init_fp64 if precision == "fp64" else self.lib.ugks_init_mixed
+        _lib.check(init(self.table.data_ptr(), self.nblocks, self.n_cells, self.n_ghost,
+                        self.solves.data_ptr(), self.nsolves, self._sptr()), "ugks_init")
+        self._step_fn = self.lib.ugks_step_fp64 if precision == "fp64" else self.lib.ugks_step_mixed
+        self.graph = None
+
+    # ---------------------------------------------------------------- set-up
+    def _dev(self, a, dtype=None):
+        torch = _torch()
+        t = torch.from_numpy(np.ascontiguousarray(a))
+        if dtype is not None:
+            t = t.to(dtype)
+        return t.to(self.device)
+
+    def _make_block(self, s, k, first, case, b, g, const, tabs):
+        torch = _torch()
+        blk = _Block()
+        G = const.ghost
+        ni, nj = b["ni"], b["nj"]
+        Ni, Nj, Nv = ni + 2 * G, nj + 2 * G, const.Nv
+        blk.solve, blk.index, blk.ni, blk.nj, blk.Ni, blk.Nj, blk.Nv, blk.G = s, k, ni, nj, Ni, Nj, Nv, G
+        blk.bc = b["bc"]
+        dev = self.device
+        z = lambda *shape, dt=torch.float64: torch.zeros(shape, dtype=dt, device=dev)
+        blk.f = z(Ni, Nj, Nv, 2, dt=self.sdtype)
+        blk.flux_S = z(Ni, Nj, Nv, 2, dt=self.sdtype)
+        blk.flux_W = z(Ni, Nj, Nv, 2, dt=self.sdtype)
+        blk.flux_macro_S = z(Ni, Nj, 4)
+        blk.flux_macro_W = z(Ni, Nj, 4)
+        macro, Q = fill_arrays(b)
+        blk.macro = self._dev(macro)
+        blk.Q = self._dev(Q)
+        blk.prim_old = z(ni, nj, 4)
+        for name in ("area", "centre", "mid_side", "normal", "side_length", "xy"):
+            setattr(blk, name, self._dev(np.nan_to_num(g[name], nan=0.0) if name != "xy" else g[name]))
+        wl = max(ni, nj)
+        blk.wall_prop = z(wl, 4, 4)
+        cover = np.zeros((wl, 4, 4))
+        for f, bc in enumerate(b["bc"]):
+            cover[:, f, 0] = bc.get("cover_initial", 0.0)
+        blk.wall_cover = self._dev(cover)
+        blk.wall_fluxes = z(wl, 4, 8)
+        blk.wall_dist = z(wl, Nv, 2)
+        x = _lib.FusedBlock()
+        d = x.d
+        d.ni, d.nj, d.Ni, d.Nj, d.ghost, d.Nv = ni, nj, Ni, Nj, G, Nv
+        d.flux_method, d.relax_type = const.flux_code, const.relax_type
+        d.PI, d.Pr, d.umax, d.vmax = const.PI, const.Pr, const.umax, const.vmax
+        d.Kn_eff, d.gam, d.K, d.omega = const.Kn_eff, const.gam, const.K, const.omega
+        d.quad, d.weight = tabs["quad"].data_ptr(), tabs["weight"].data_ptr()
+        d.mirror_NS, d.mirror_EW, d.mirror_D = (tabs["mNS"].data_ptr(), tabs["mEW"].data_ptr(),
+                                                tabs["mD"].data_ptr())
+        for f, bc in enumerate(b["bc"]):
+            d.wall_D[f], d.wall_U[f], d.wall_V[f], d.wall_T[f], d.wall_P[f] = wall_values(bc)
+            x.bc_type[f] = bc["type"]
+            if bc["type"] == D.ADJACENT:
+                x.bc_block[f] = first + bc["other_block"]
+                x.bc_face[f] = bc["other_face"]
+                x.bc_ori[f] = bc.get("orientation", 1)
+                x.bc_flip[f] = bc.get("flip", D.NO_FLIP)
+            if bc["type"] == D.ADSORBING:
+                d.beta_n[f] = float("%0.15e" % bc.get("beta_n", 0.0))
+                d.beta_t[f] = float("%0.15e" % bc.get("beta_t", 0.0))
+                d.gamma_f[f] = float("%0.15e" % bc["gamma_f"])
+                d.alpha_p[f] = float("%0.15e" % bc["alpha_p"])
+                d.dynamic[f] = int(bc.get("dynamic", 1))
+                scalar = np.ndim(bc["adsorb"]) == 0
+                d.constant_adsorb[f] = 1 if scalar else 0
+                d.adsorb[f] = float("%g" % bc["adsorb"]) if scalar else 0.0
+                d.k_des[f] = float(bc.get("k_des", 0.0))
+            else:
+                d.beta_n[f] = d.beta_t[f] = d.gamma_f[f] = d.alpha_p[f] = -1.0
+                d.dynamic[f] = -1
+        x.solve = s
+        for name in ("f", "flux_S", "flux_W", "flux_macro_S", "flux_macro_W", "macro", "Q", "prim_old",
+                     "area", "centre", "mid_side", "normal", "side_length", "xy", "wall_prop",
+                     "wall_cover", "wall_fluxes", "wall_dist"):
+            setattr(x, name, getattr(blk, name).data_ptr())
+        blk.struct = x
+        return blk
+
+    def _sptr(self):
+        torch = _torch()
+        s = self._stream if self._stream is not None else torch.cuda.current_stream(self.device)
+        return s.cuda_stream
+
+    # ---------------------------------------------------------------- stepping
+    def step(self, n: int = 1):
+        """Advance every active solve by n steps (asynchronous)."""
+        for _ in range(n):
+            _lib.check(self._step_fn(self.table.data_ptr(), self.nblocks, self.n_faces, self.n_cells,
+                                     self.n_ghost, self.max_nv, self.solves.data_ptr(), self.nsolves,
+                                     self._sptr()), "ugks_step")
+
+    def capture(self, steps: int):
+        """Capture `steps` steps as one CUDA graph; ``replay()`` runs it."""
+        torch = _torch()
+        # the first launch sets kernel attributes, which is not capturable
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream(self.device)
+        s.wait_stream(torch.cuda.current_stream(self.device))
+        old = self._stream
+        with torch.cuda.stream(s):
+            self._stream = s
+            with torch.cuda.graph(g, stream=s):
+                self.step(steps)
+        self._stream = old
+        torch.cuda.current_stream(self.device).wait_stream(s)
+        self.graph = g
+        self.graph_steps = steps
+        return g
+
+    def replay(self):
+        self.graph.replay()
+
+    def compute_residual(self):
+        _lib.check(self.lib.ugks_residual(self.table.data_ptr(), self.nblocks, self.solves.data_ptr(),
+                                          self.nsolves, self._sptr()), "ugks_residual")
+
+    # ---------------------------------------------------------------- readback
+    def solve_state(self):
+        """Host copy of every ugks_solve_state (synchronises)."""
+        raw = self.solves.cpu().numpy().tobytes()
+        arr = (_lib.SolveState * self.nsolves).from_buffer_copy(raw)
+        return [dict(dt=x.dt, time=x.time, max_dt=x.max_dt, status=x.status, steps=x.steps,
+                     retries=x.retries, active=x.active, residual=list(x.residual)) for x in arr]
+
+    def set_active(self, flags):
+        """Switch solves on/off for the next steps (device-side flag)."""
+        torch = _torch()
+        st = (_lib.SolveState * self.nsolves).from_buffer_copy(self.solves.cpu().numpy().tobytes())
+        for s, a in enumerate(flags):
+            st[s].active = 1 if a else 0
+        self.solves.copy_(torch.from_numpy(np.frombuffer(bytes(st), dtype=np.uint8).copy()))
+
+    def fields(self, solve: int = 0):
+        """Per block interior fields of one solve as numpy: rho, U, V, T, qx, qy
+        (Q re-taken from the current f, as the reference's updateHost does)."""
+        out = []
+        for bi in self.solve_blocks[solve]:
+            b = self.blocks[bi]
+            m = b.macro.cpu().numpy()
+            f = b.f[b.G:-b.G, b.G:-b.G].double().cpu().numpy()
+            q = self._heat_flux(b, f, m)
+            out.append(dict(rho=m[:, :, 0], U=m[:, :, 1], V=m[:, :, 2], T=1.0 / m[:, :, 3],
+                            qx=q[:, :, 0], qy=q[:, :, 1]))
+        return out
+
+    def _heat_flux(self, b, f, m):
+        vg = Constants(self.cases[b.solve]).vgrid
+        K = Constants(self.cases[b.solve]).K
+        cx = vg.quad[None, None, :, 0] - m[:, :, None, 1]
+        cy = vg.quad[None, None, :, 1] - m[:, :, None, 2]
+        t = (cx * cx + cy * cy) * f[..., 0] + f[..., 1] / K
+        return np.stack([0.5 * np.sum(cx * t, axis=-1), 0.5 * np.sum(cy * t, axis=-1)], -1)
+
+    def interior_f(self, solve: int = 0):
+        return [self.blocks[bi].f[self.blocks[bi].G:-self.blocks[bi].G,
+                                  self.blocks[bi].G:-self.blocks[bi].G].double().cpu().numpy()
+                for bi in self.solve_blocks[solve]]
