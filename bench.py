@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""Benchmark of the UGKS time step: cell-velocity updates per second.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--precision fp64|mixed] [--workload multiblock|cavity|channel|batched]
+
+Prints one JSON line.  A step is one ``UGKSim.one_step`` over every block of
+the workload; the metric counts interior cell x velocity points updated per
+second (ghost cells not counted).
+
+Default workload: the 128x128 lid-driven cavity in 2x2 blocks of 64x64 cells,
+33x33 = 1089 velocities on [-5,5]^2, WENO5, Kn 0.01, plain FP64 — 17.8 M
+cell-velocity points per step.  Its f and face-flux arrays (about 1 GB in FP64)
+are far larger than the 126 MB L2, so no flush is needed between steps.
+
+``--impl ours`` (default): the fused CUDA step on each GPU.  ``value`` is
+device time with the state resident in HBM (CUDA events on the launch stream);
+``e2e`` goes through the same public call with host buffers: the initial state
+is copied from pinned host memory inside the timed region, each step's solve
+record (dt, time, status) is copied back asynchronously, and the final
+macroscopic fields are read back.  ``roofline`` times the dominant kernel live
+with events recorded between the kernels of every timed step.
+
+``--impl reference``: the reference's own kernels compiled for the CPU
+(oracle/_ref, OpenMP over the host cores) driven by the reference's step
+sequence, on the same workload; rank 0 only.
+
+Several GPUs (torchrun): the path has no data exchange between independent
+solves, so every rank runs its own replica (weak scaling); the reported time is
+the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+from pyugks_b200 import configs  # noqa: E402
+
+METRIC = "cell-velocity updates/s"
+UNIT = "cell*velocity/s"
+BYTES_PER_UPDATE = {"fp64": 32, "mixed": 16}  # read + write of (h, b) per cell-velocity
+
+
+def workload(name: str):
+    if name == "multiblock":
+        case = configs.cavity_multiblock(nb=2, n=64, m=32, vlim=5.0, flux_method="WENO5", Kn=0.01)
+        desc = ("lid-driven cavity 128x128 as 2x2 blocks of 64x64 cells, 33x33 velocities on "
+                "[-5,5]^2 (Nv=1089), WENO5, Kn 0.01, CFL 0.8")
+        return [case], desc
+    if name == "cavity":
+        case = configs.cavity(n=32, m=24, vlim=4.0)
+        return [case], "lid-driven cavity 32x32, 25x25 velocities on [-4,4]^2 (Nv=625), vanLeer, Kn 0.075"
+    if name == "channel":
+        case = configs.channel(nblocks=4, n=64, m=32, Kn=0.05)
+        return [case], ("adsorbing channel 256x64 in 4 blocks, 33x33 velocities on [-5,5]^2, WENO5, "
+                        "Kn 0.05, inlet rho 1.2 / outlet rho 1.0")
+    if name == "batched":
+        cases = configs.batched_cavities(64, seed=1)
+        return cases, "64 independent cavities, n in {24..128}, m in {16..48}, seed 1"
+    raise ValueError(name)
+
+
+def units_per_step(cases) -> int:
+    return sum(configs.workload_size(c) for c in cases)
+
+
+# ---------------------------------------------------------------------------
+def sample_clocks(stop_file, out_file):
+    cmd = ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+           "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+           "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+           "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"]
+    try:
+        return subprocess.Popen(cmd, stdout=open(out_file, "w"), stderr=subprocess.DEVNULL)
+    except (FileNotFoundError, OSError):
+        return None
+
+
+def parse_clocks(path, gpu_index):
+    sm, mx, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    try:
+        with open(path) as fh:
+            for line in fh:
+                p = [x.strip() for x in line.split(",")]
+                if len(p) < 9 or p[0] != str(gpu_index):
+                    continue
+                try:
+                    sm.append(float(p[1]))
+                    mx = float(p[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, p[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(nm)
+    except OSError:
+        pass
+    return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+            "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def read_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def read_traffic(kernel: str, workload_name: str, precision: str):
+    """DRAM bytes per launch recorded from an ncu capture in profiles/."""
+    path = os.path.join(ROOT, "profiles", "%s_%s_%s.md" % (kernel, workload_name, precision))
+    try:
+        with open(path) as fh:
+            for line in fh:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return int(float(line.split(":", 1)[1]))
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------------------------
+def cpu_reference(cases, steps, warmup, threads=None, time_budget=None):
+    """Time the reference kernels compiled for the CPU (or the C restatement
+    if they are unavailable) on the workload.  Returns (units/s, kind, cores,
+    steps timed)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import host  # the checker / CPU baseline only
+    import programs
+    import ugks_setup
+    threads = threads or os.cpu_count()
+    kind = "reference"
+    for case in cases:
+        c = ugks_setup.Constants(case)
+        if not all(programs.reference_available(c, b, k) for k, b in enumerate(case["blocks"])):
+            kind = "port"
+    sims = [host.OracleSim(case, "ref" if kind == "reference" else "port", threads=threads)
+            for case in cases]
+    for _ in range(warmup):
+        for s in sims:
+            s.one_step()
+    t0 = time.perf_counter()
+    done = 0
+    for _ in range(steps):
+        for s in sims:
+            s.one_step()
+        done += 1
+        if time_budget and time.perf_counter() - t0 > time_budget:
+            break
+    el = time.perf_counter() - t0
+    return units_per_step(cases) * done / el, kind, (threads if kind == "reference" else 1), done
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    cases, desc = workload(args.workload)
+    val, kind, cores, done = cpu_reference(cases, args.steps, args.warmup)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": done, "warmup": args.warmup, "ms_per_step": units_per_step(cases) / val * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": desc, "precision": "fp64", "units_per_step": units_per_step(cases)},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": cores, "kind": kind,
+                         "sample": "%d full steps of the workload after %d warm-up steps" % (done, args.warmup)},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args, rank, world, dist):
+    import torch
+    from pyugks_b200 import _lib
+    from pyugks_b200.fused import FusedSolver
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    cases, desc = workload(args.workload)
+    units = units_per_step(cases)
+    stream = torch.cuda.Stream(dev)
+    with torch.cuda.stream(stream):
+        solver = FusedSolver(cases, precision=args.precision, device=dev, stream=stream)
+        L = solver.lib
+        mixed = 1 if args.precision == "mixed" else 0
+        # warm-up
+        solver.step(args.warmup)
+        torch.cuda.synchronize(dev)
+        if dist is not None:
+            dist.barrier()
+        # ---- device-resident timing, with per-kernel events every step
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(8)] for _ in range(args.steps)]
+        for row in evs:  # torch creates the CUDA event at its first record
+            for e in row:
+                e.record(stream)
+        torch.cuda.synchronize(dev)
+        handles = [(_lib.vp * 8)(*[e.cuda_event for e in row]) for row in evs]
+        clock_file = os.path.join("/tmp", "ugks_clocks_%d_%d.csv" % (os.getpid(), rank))
+        smi = sample_clocks(None, clock_file)
+        time.sleep(0.3)
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        start.record(stream)
+        for k in range(args.steps):
+            _lib.check(L.ugks_step_profiled(mixed, solver.table.data_ptr(), solver.nblocks, solver.n_faces,
+                                            solver.n_cells, solver.n_ghost, solver.max_nv,
+                                            solver.flux_methods, solver.solves.data_ptr(),
+                                            solver.nsolves, handles[k],
+                                            stream.cuda_stream), "ugks_step_profiled")
+        end.record(stream)
+        torch.cuda.synchronize(dev)
+        if smi is not None:
+            smi.terminate()
+            smi.wait()
+        ms = start.elapsed_time(end)
+        face = [evs[k][0].elapsed_time(evs[k][1]) for k in range(args.steps)]
+        retry = [evs[k][2].elapsed_time(evs[k][3]) for k in range(args.steps)]
+        cell = [evs[k][4].elapsed_time(evs[k][5]) for k in range(args.steps)]
+        ghost = [evs[k][6].elapsed_time(evs[k][7]) for k in range(args.steps)]
+        state = solver.solve_state()
+        if any(s["status"] != 0 for s in state):
+            raise RuntimeError("solver status %s" % [s["status"] for s in state])
+        # ---- end to end through the public call with host buffers
+        e2e = run_e2e(solver, args, stream, dev, units)
+    t_max = ms
+    if dist is not None:
+        t = torch.tensor([ms, e2e["ms"]], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_max, e2e_ms = float(t[0]), float(t[1])
+    else:
+        e2e_ms = e2e["ms"]
+    if rank != 0:
+        return
+    value = world * units * args.steps / (t_max / 1e3)
+    kernels = {"face_pass": statistics.mean(face), "cell_pass": statistics.mean(cell),
+               "ghost_pass": statistics.mean(ghost), "retry_face_pass": statistics.mean(retry)}
+    dom = max(("face_pass", "cell_pass"), key=lambda k: kernels[k])
+    peak, peak_kind = read_peaks()
+    bpu = BYTES_PER_UPDATE[args.precision]
+    achieved = bpu * units / (kernels[dom] / 1e3) / 1e9
+    clocks = parse_clocks(clock_file, local)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": desc, "precision": args.precision, "units_per_step": units,
+                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "l2": "working set > 126 MB L2 (f and face fluxes %.2f GB), no flush"
+                         % (solver_bytes(solver) / 1e9)},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": read_traffic(dom, args.workload, args.precision),
+                     "bytes_per_unit": bpu, "kernel_ms": kernels,
+                     "step_frac": bpu * units / (t_max / args.steps / 1e3) / 1e9 / peak},
+        "e2e": {"value": world * units * args.steps / (e2e_ms / 1e3), "unit": UNIT,
+                "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
+        "gpu_launches": 7 * args.steps,
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        budget = float(os.environ.get("UGKS_CPU_BASELINE_SECONDS", "20"))
+        val, kind, cores, done = cpu_reference(cases, steps=50, warmup=1, time_budget=budget)
+        line["cpu_baseline"] = {"value": val, "unit": UNIT, "cores": cores, "kind": kind,
+                                "sample": "%d full steps of the workload (time budget %.0f s) after 1 warm-up"
+                                          % (done, budget)}
+    print(json.dumps(line), flush=True)
+
+
+def solver_bytes(solver):
+    return sum(b.f.numel() * b.f.element_size() * 3 for b in solver.blocks)
+
+
+def run_e2e(solver, args, stream, dev, units):
+    """Host-buffer run: initial state H2D (pinned) + K steps with an async D2H
+    of each step's solve record + final D2H of the macroscopic fields."""
+    import torch
+    host_state = [(b.f.detach().cpu().pin_memory(), b.macro.detach().cpu().pin_memory(),
+                   b.Q.detach().cpu().pin_memory()) for b in solver.blocks]
+    rec = torch.empty((args.steps, solver.solves.numel()), dtype=torch.uint8).pin_memory()
+    fields = [torch.empty_like(b.macro, device="cpu").pin_memory() for b in solver.blocks]
+    h2d = sum(x.numel() * x.element_size() for t in host_state for x in t)
+    torch.cuda.synchronize(dev)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for b, (f, m, q) in zip(solver.blocks, host_state):
+        b.f.copy_(f, non_blocking=True)
+        b.macro.copy_(m, non_blocking=True)
+        b.Q.copy_(q, non_blocking=True)
+    for k in range(args.steps):
+        solver.step(1)
+        rec[k].copy_(solver.solves, non_blocking=True)
+    for b, out in zip(solver.blocks, fields):
+        out.copy_(b.macro, non_blocking=True)
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    d2h = rec.numel() + sum(x.numel() * x.element_size() for x in fields)
+    return {"ms": t0.elapsed_time(t1), "h2d": h2d // args.steps, "d2h": d2h // args.steps}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--workload", default="multiblock", choices=["multiblock", "cavity", "channel", "batched"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1 and args.impl == "ours":
+        import datetime
+
+        import torch.distributed as tdist
+        import torch
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        dist = tdist
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, dist)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

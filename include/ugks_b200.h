@@ -60,6 +60,10 @@ typedef struct ugks_block_desc {
   double k_des[4];
   int32_t dynamic[4];          /* DYNAMIC_VARTHETA                         */
   int32_t constant_adsorb[4];  /* CONSTANT_ADSORB_<face>                   */
+  /* tensor velocity grid: v = iu * v_num + jv with quad[v] = (u_iu, v_jv)
+     (ugks_data.py:287-292); u_num * v_num == Nv lets the fused kernels
+     factor the Maxwellian exponential; 0 for an unstructured set */
+  int32_t u_num, v_num;
 } ugks_block_desc;
 
 /* ------------------------------------------------------------------------
@@ -272,13 +276,24 @@ int ugks_init_mixed(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_c
 /* One UGKSim.one_step (ugks_sim.py:407-501) of every active solve: flux
    pass, dt check with the reference's single retry, cell update, new dt,
    time advance, ghost update.  max_nv: largest Nv of the table (sizes the
-   face pass's shared memory, 32 bytes per velocity). */
+   face pass's shared memory, 32 bytes per velocity); flux_methods: bit k set
+   when some block uses flux_method k (one face-pass launch per method). */
 int ugks_step_fp64(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_faces,
-                   int32_t n_cells, int32_t n_ghost, int32_t max_nv, ugks_solve_state *solves_dev,
-                   int nsolves, UGKS_STREAM);
+                   int32_t n_cells, int32_t n_ghost, int32_t max_nv, int32_t flux_methods,
+                   ugks_solve_state *solves_dev, int nsolves, UGKS_STREAM);
 int ugks_step_mixed(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_faces,
-                    int32_t n_cells, int32_t n_ghost, int32_t max_nv, ugks_solve_state *solves_dev,
-                    int nsolves, UGKS_STREAM);
+                    int32_t n_cells, int32_t n_ghost, int32_t max_nv, int32_t flux_methods,
+                    ugks_solve_state *solves_dev, int nsolves, UGKS_STREAM);
+
+/* The same step with cudaEventRecord of events[0..7] (cudaEvent_t) on the
+   stream around the phases: [0] start, [1] after the face pass, [2] after the
+   dt check, [3] after the retry face pass, [4] after the second dt check,
+   [5] after the cell pass, [6] after the dt update, [7] after the ghost pass.
+   mixed != 0 selects FP32 storage.  Used to time each kernel live. */
+int ugks_step_profiled(int mixed, const ugks_fused_block *blocks_dev, int nblocks, int32_t n_faces,
+                       int32_t n_cells, int32_t n_ghost, int32_t max_nv, int32_t flux_methods,
+                       ugks_solve_state *solves_dev, int nsolves, void *const *events,
+                       UGKS_STREAM);
 
 /* Residual of the last step (getResidual + the host reduction of
    ugks_block.py:1303-1327, averaged over a solve's blocks as

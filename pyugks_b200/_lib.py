@@ -10,7 +10,8 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libugks_b200.so")
+# UGKS_LIB_PATH selects another build of the same library (tuning builds)
+LIB_PATH = os.environ.get("UGKS_LIB_PATH", os.path.join(HERE, "libugks_b200.so"))
 
 i32, f64, vp = C.c_int32, C.c_double, C.c_void_p
 
@@ -28,6 +29,7 @@ class BlockDesc(C.Structure):
         ("beta_n", f64 * 4), ("beta_t", f64 * 4), ("gamma_f", f64 * 4), ("alpha_p", f64 * 4),
         ("adsorb", f64 * 4), ("k_des", f64 * 4),
         ("dynamic", i32 * 4), ("constant_adsorb", i32 * 4),
+        ("u_num", i32), ("v_num", i32),
     ]
 
 
@@ -105,7 +107,9 @@ def lib():
     for nm in ("ugks_step_fp64", "ugks_step_mixed"):
         fn = getattr(L, nm)
         fn.restype = C.c_int
-        fn.argtypes = [vp, C.c_int, i32, i32, i32, i32, vp, C.c_int, vp]
+        fn.argtypes = [vp, C.c_int, i32, i32, i32, i32, i32, vp, C.c_int, vp]
+    L.ugks_step_profiled.restype = C.c_int
+    L.ugks_step_profiled.argtypes = [C.c_int, vp, C.c_int, i32, i32, i32, i32, i32, vp, C.c_int, vp, vp]
     L.ugks_residual.restype = C.c_int
     L.ugks_residual.argtypes = [vp, C.c_int, vp, C.c_int, vp]
     L.ugks_version.restype = C.c_char_p

@@ -29,6 +29,12 @@ using namespace ugks;
 namespace {
 
 constexpr int FT = 128;  // threads per face / cell / ghost CTA
+#ifndef FACE_MIN_BLOCKS
+#define FACE_MIN_BLOCKS 4
+#endif
+#ifndef CELL_MIN_BLOCKS
+#define CELL_MIN_BLOCKS 8
+#endif
 
 inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 inline int launch_status() {
@@ -67,9 +73,83 @@ struct FaceShared {
   double bcast[48];
 };
 
-template <typename T>
-__global__ void __launch_bounds__(FT) face_pass(const ugks_fused_block *__restrict__ B, int nb,
-                                                ugks_solve_state *__restrict__ solves, int retry_pass) {
+// WENO5 slope (clFunctions.c:266-313) with the three nonlinear weights
+// normalised through one division: w_k = c_k / d_k / sum(c_j / d_j) =
+// c_k prod_{j!=k} d_j / sum_j c_j prod_{i!=j} d_i, d_k = (eps + beta_k)^2.
+__device__ __forceinline__ double weno5_slope(double S0, double S1, double S2, double S3,
+                                              double S4, double inv_dx) {
+  double t1 = S0 - 2.0 * S1 + S2, t2 = S0 - 4.0 * S1 + 3.0 * S2;
+  const double B0 = (13.0 / 12.0) * t1 * t1 + 0.25 * t2 * t2;
+  t1 = S1 - 2.0 * S2 + S3;
+  t2 = S1 - S3;
+  const double B1 = (13.0 / 12.0) * t1 * t1 + 0.25 * t2 * t2;
+  t1 = S2 - 2.0 * S3 + S4;
+  t2 = 3.0 * S2 - 4.0 * S3 + S4;
+  const double B2 = (13.0 / 12.0) * t1 * t1 + 0.25 * t2 * t2;
+  double d0 = 1e-16 + B0, d1 = 1e-16 + B1, d2 = 1e-16 + B2;
+  d0 *= d0;
+  d1 *= d1;
+  d2 *= d2;
+  const double a0 = 0.1 * (d1 * d2), a1 = 0.6 * (d0 * d2), a2 = 0.3 * (d0 * d1);
+  const double f0 = (1. / 3.) * S0 - (7. / 6.) * S1 + (11. / 6.) * S2;
+  const double f1 = -(1. / 6.) * S1 + (5. / 6.) * S2 + (1. / 3.) * S3;
+  const double f2 = (1. / 3.) * S2 + (5. / 6.) * S3 - (1. / 6.) * S4;
+  const double fL = (a0 * f0 + a1 * f1 + a2 * f2) * nr_rcp(a0 + a1 + a2);
+  return (fL - S2) * inv_dx;
+}
+
+// vanLeer limiter (clFunctions.c:255-261) with a Newton-Raphson reciprocal
+__device__ __forceinline__ double vanleer_fast(double s1, double s2) {
+  const double a1 = fabs(s1), a2 = fabs(s2);
+  return (ocl_sign(s1) + ocl_sign(s2)) * (a1 * a2) * nr_rcp(a1 + a2 + 1e-16);
+}
+
+// iFace (clUGKS.c:148-194) for one velocity: face value and slope of (h, b),
+// plus the left / right cell values (stencil cells MID and MID+1).
+template <typename T, int FM>
+__device__ __forceinline__ void reconstruct(const void *f, size_t kv, long step, int delta,
+                                            double inv_l, double ds, double inv_ds, double &fh,
+                                            double &fb, double &sh, double &sb, double &lh,
+                                            double &lb, double &rh, double &rb) {
+  constexpr int L = FM == 1 ? 5 : 3, MID = FM == 1 ? 2 : 1;
+  double Sh[L], Sb[L];
+#pragma unroll
+  for (int s = 0; s < L; ++s) {
+    const long off = delta ? (long)(-MID - 1 + s) : (long)(MID - s);
+    const V2 x = Store<T>::load(f, (size_t)((long)kv + off * step));
+    Sh[s] = x.x;
+    Sb[s] = x.y;
+  }
+  if (FM == 0) {
+    sh = vanleer_fast((Sh[1] - Sh[0]) * inv_l, (Sh[2] - Sh[1]) * inv_l);
+    sb = vanleer_fast((Sb[1] - Sb[0]) * inv_l, (Sb[2] - Sb[1]) * inv_l);
+  } else if (FM == 1) {
+    sh = weno5_slope(Sh[0], Sh[1], Sh[2], Sh[3], Sh[4], inv_ds);
+    sb = weno5_slope(Sb[0], Sb[1], Sb[2], Sb[3], Sb[4], inv_ds);
+  } else {
+    sh = (0.5 * minmod(Sh[2] - Sh[1], Sh[1] - Sh[0])) * inv_ds;
+    sb = (0.5 * minmod(Sb[2] - Sb[1], Sb[1] - Sb[0])) * inv_ds;
+  }
+  fh = Sh[MID] + sh * ds;
+  fb = Sb[MID] + sb * ds;
+  lh = delta ? Sh[MID] : Sh[MID + 1];
+  lb = delta ? Sb[MID] : Sb[MID + 1];
+  rh = delta ? Sh[MID + 1] : Sh[MID];
+  rb = delta ? Sb[MID + 1] : Sb[MID];
+}
+
+// exp(-lambda (x - c)^2) over the nodes of one velocity axis
+__device__ __forceinline__ void axis_exp(double *out, const double *quad, int n, int stride,
+                                         int comp, double c, double lambda, int t, int nt) {
+  for (int i = t; i < n; i += nt) {
+    const double x = quad[2 * (size_t)i * stride + comp] - c;
+    out[i] = exp(-lambda * (x * x));
+  }
+}
+
+template <typename T, int FM>
+__global__ void __launch_bounds__(FT, FACE_MIN_BLOCKS) face_pass(const ugks_fused_block *__restrict__ B, int nb,
+                                                   ugks_solve_state *__restrict__ solves, int retry_pass) {
   extern __shared__ double dyn[];
   __shared__ FaceShared sh;
   using St = Store<T>;
@@ -81,11 +161,11 @@ __global__ void __launch_bounds__(FT) face_pass(const ugks_fused_block *__restri
   ugks_solve_state &sol = solves[blk.solve];
   if (!sol.active) return;
   if (retry_pass && !sol.retry) return;
+  if (d.flux_method != FM) return;
   const double dt = sol.dt;
 
-  // work item -> (i, j, direction); items run over the (ni+1) x (nj+1) corner
-  // grid with S and W faces of the same (i, j) adjacent, so that both face
-  // directions of a cell read f while it is in L2
+  // work item -> (i, j, direction): S and W faces of one corner (i, j) are
+  // adjacent work items so that both directions read f while it is in L2
   int lf = w - blk.face_begin;
   const int dir = lf & 1;
   lf >>= 1;
@@ -94,7 +174,6 @@ __global__ void __launch_bounds__(FT) face_pass(const ugks_fused_block *__restri
 
   const int Nv = d.Nv, G = d.ghost;
   const long gi = mi + G, gj = mj + G;
-  // wall id of this face, or -1
   int wall = -1;
   if (dir == SOUTH) {
     if (mj == 0 && is_wall(blk.bc_type[GSOUTH])) wall = GSOUTH;
@@ -107,68 +186,38 @@ __global__ void __launch_bounds__(FT) face_pass(const ugks_fused_block *__restri
   double *fh = dyn, *fb = dyn + Nv, *sgh = dyn + 2 * Nv, *sgb = dyn + 3 * Nv;
   const V2 n = ld2(blk.normal, faceidx(d, gi, gj, dir));
   const V2 mid = ld2(blk.mid_side, faceidx(d, gi, gj, dir));
-  const int L = d.flux_method == 1 ? 5 : 3, MID = d.flux_method == 1 ? 2 : 1;
   // stencil geometry for both upwind directions (iFace, clUGKS.c:148-176)
-  double dist[2], l1[2];
+  double dist[2], inv_dist[2], inv_l1[2];
 #pragma unroll
   for (int dl = 0; dl < 2; ++dl) {
-    long c0i, c0j, c1i, c1j;  // centre of cell MID and MID-1
-    if (dir == SOUTH) {
-      c0i = c1i = gi;
-      c0j = dl ? gj - MID - 1 + MID : gj + MID - MID;
-      c1j = dl ? gj - MID - 1 + MID - 1 : gj + MID - (MID - 1);
-    } else {
-      c0j = c1j = gj;
-      c0i = dl ? gi - MID - 1 + MID : gi + MID - MID;
-      c1i = dl ? gi - MID - 1 + MID - 1 : gi + MID - (MID - 1);
-    }
-    V2 c0 = ld2(blk.centre, gidx(d, c0i, c0j)), c1 = ld2(blk.centre, gidx(d, c1i, c1j));
-    dist[dl] = sqrt((mid.x - c0.x) * (mid.x - c0.x) + (mid.y - c0.y) * (mid.y - c0.y));
-    l1[dl] = sqrt((c0.x - c1.x) * (c0.x - c1.x) + (c0.y - c1.y) * (c0.y - c1.y));
+    const long c0 = dl ? -1 : 0, c1 = dl ? -2 : 1;  // cells MID and MID-1 relative to the face
+    const long c0i = dir == SOUTH ? gi : gi + c0, c0j = dir == SOUTH ? gj + c0 : gj;
+    const long c1i = dir == SOUTH ? gi : gi + c1, c1j = dir == SOUTH ? gj + c1 : gj;
+    const V2 a = ld2(blk.centre, gidx(d, c0i, c0j)), b = ld2(blk.centre, gidx(d, c1i, c1j));
+    dist[dl] = sqrt((mid.x - a.x) * (mid.x - a.x) + (mid.y - a.y) * (mid.y - a.y));
+    inv_dist[dl] = 1.0 / dist[dl];
+    inv_l1[dl] = 1.0 / sqrt((a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y));
   }
-  const size_t step = dir == SOUTH ? (size_t)Nv : (size_t)d.Nj * Nv;  // stencil stride
+  const long step = dir == SOUTH ? (long)Nv : (long)d.Nj * Nv;
   const size_t base = fidx(d, gi, gj, 0);
 
-  // ---- sweep 1: reconstruction (+ interior: conserved moments W, WL, WR)
+  // ---- sweep 1: reconstruction (+ interior faces: moments W, WL, WR)
   double m[12];
 #pragma unroll
   for (int k = 0; k < 12; ++k) m[k] = 0.0;
+#pragma unroll 2
   for (int v = threadIdx.x; v < Nv; v += FT) {
     const V2 uv = face_velocity(d, v, n);
-    const int delta = (int)((ocl_sign(uv.x) + 1) / 2);
-    double sh_[5], sb_[5];
-#pragma unroll
-    for (int s = 0; s < 5; ++s) {
-      if (s < L) {
-        long off = delta ? (long)(-MID - 1 + s) : (long)(MID - s);
-        V2 f = St::load(blk.f, base + v + off * (long)step);
-        sh_[s] = f.x;
-        sb_[s] = f.y;
-      }
-    }
-    const double ds = dist[delta];
-    double sx, sy;
-    if (d.flux_method == 0) {
-      const double l = l1[delta];
-      sx = vanleer((sh_[1] - sh_[0]) / l, (sh_[2] - sh_[1]) / l);
-      sy = vanleer((sb_[1] - sb_[0]) / l, (sb_[2] - sb_[1]) / l);
-    } else if (d.flux_method == 1) {
-      sx = weno5(sh_[0], sh_[1], sh_[2], sh_[3], sh_[4], ds);
-      sy = weno5(sb_[0], sb_[1], sb_[2], sb_[3], sb_[4], ds);
-    } else {
-      sx = (sh_[1] + 0.5 * minmod(sh_[2] - sh_[1], sh_[1] - sh_[0]) - sh_[1]) / ds;
-      sy = (sb_[1] + 0.5 * minmod(sb_[2] - sb_[1], sb_[1] - sb_[0]) - sb_[1]) / ds;
-    }
-    const double ffh = sh_[MID] + sx * ds, ffb = sb_[MID] + sy * ds;
+    const int delta = uv.x > 0.0 ? 1 : 0;
+    double ffh, ffb, sx, sy, lh, lb, rh, rb;
+    reconstruct<T, FM>(blk.f, base + v, step, delta, inv_l1[delta], dist[delta], inv_dist[delta],
+                       ffh, ffb, sx, sy, lh, lb, rh, rb);
     fh[v] = ffh;
     fb[v] = ffb;
     sgh[v] = sx;
     sgb[v] = sy;
     if (wall < 0) {
       const double uu = uv.x * uv.x + uv.y * uv.y;
-      // left / right cells of the face are stencil cells MID and MID+1
-      const double lh = delta ? sh_[MID] : sh_[MID + 1], lb = delta ? sb_[MID] : sb_[MID + 1];
-      const double rh = delta ? sh_[MID + 1] : sh_[MID], rb = delta ? sb_[MID + 1] : sb_[MID];
       m[0] += ffh; m[1] += uv.x * ffh; m[2] += uv.y * ffh; m[3] += 0.5 * (uu * ffh + ffb);
       m[4] += lh; m[5] += uv.x * lh; m[6] += uv.y * lh; m[7] += 0.5 * (uu * lh + lb);
       m[8] += rh; m[9] += uv.x * rh; m[10] += uv.y * rh; m[11] += 0.5 * (uu * rh + rb);
@@ -179,80 +228,107 @@ __global__ void __launch_bounds__(FT) face_pass(const ugks_fused_block *__restri
   if (wall < 0) {
     // ---------------- interior face ----------------
     block_sum<12>(m, sh.scratch);
-    if (threadIdx.x == 0) {
-      // getPLR (clUGKS.c:401-442)
-      const P4 W = p4(m[0], m[1], m[2], m[3]);
-      const P4 prim = to_primary(d, W);
-      const V2 cl = ld2(blk.centre, gidx(d, gi - dir, gj - (1 - dir)));
-      const V2 cr = ld2(blk.centre, gidx(d, gi, gj));
-      const double dl = sqrt((mid.x - cl.x) * (mid.x - cl.x) + (mid.y - cl.y) * (mid.y - cl.y));
-      const double dr = sqrt((mid.x - cr.x) * (mid.x - cr.x) + (mid.y - cr.y) * (mid.y - cr.y));
-      const P4 aL = micro_slope(d, prim, p4((W.s0 - m[4]) / dl, (W.s1 - m[5]) / dl,
-                                            (W.s2 - m[6]) / dl, (W.s3 - m[7]) / dl));
-      const P4 aR = micro_slope(d, prim, p4((m[8] - W.s0) / dr, (m[9] - W.s1) / dr,
-                                            (m[10] - W.s2) / dr, (m[11] - W.s3) / dr));
-      // initMacroFlux (clUGKS.c:446-518)
-      double Mu[MNUM], Mv[MTUM], Mxi[3], MuL[MNUM], MuR[MNUM], Mt[5];
-      moments_u(d, prim, Mu, Mv, Mxi, MuL, MuR);
-      const P4 aT = micro_slope(d, prim, scale(-prim.s0, add(moment_au(aL, MuL, Mv, Mxi, 1, 0),
-                                                             moment_au(aR, MuR, Mv, Mxi, 1, 0))));
-      time_weights(relax_time(d, prim), dt, Mt);
-      const P4 g0 = scale(prim.s0,
-                          add(add(scale(Mt[0], moment_uv(Mu, Mv, Mxi, 1, 0, 0)),
-                                  scale(Mt[1], add(moment_au(aL, MuL, Mv, Mxi, 2, 0),
-                                                   moment_au(aR, MuR, Mv, Mxi, 2, 0)))),
-                              scale(Mt[2], moment_au(aT, Mu, Mv, Mxi, 1, 0))));
-      double *c = sh.bcast;
-      c[0] = prim.s0; c[1] = prim.s1; c[2] = prim.s2; c[3] = prim.s3;
-      c[4] = aL.s0; c[5] = aL.s1; c[6] = aL.s2; c[7] = aL.s3;
-      c[8] = aR.s0; c[9] = aR.s1; c[10] = aR.s2; c[11] = aR.s3;
-      c[12] = aT.s0; c[13] = aT.s1; c[14] = aT.s2; c[15] = aT.s3;
-      c[16] = Mt[0]; c[17] = Mt[1]; c[18] = Mt[2]; c[19] = Mt[3]; c[20] = Mt[4];
-      c[21] = Mxi[2];
-      c[22] = g0.s0; c[23] = g0.s1; c[24] = g0.s2; c[25] = g0.s3;
-    }
-    __syncthreads();
-    const double *c = sh.bcast;
-    const P4 prim = p4(c[0], c[1], c[2], c[3]);
-    // ---- sweep 2: face heat flux (calcFaceQ, clUGKS.c:522-585)
+    const P4 W = p4(m[0], m[1], m[2], m[3]);
+    const P4 prim = to_primary(d, W);  // getPLR (clUGKS.c:421-422), every thread
+    const int un = d.u_num, vn = d.v_num;
+    const bool sep = un > 0 && un * vn == Nv && un + vn <= 512;
+    double *Eu = dyn + 4 * Nv, *Ev = Eu + (sep ? un : 0);
+    const V2 Ug = to_global(v2(prim.s1, prim.s2), n);  // face mean velocity, global frame
     double q[2] = {0.0, 0.0};
-    for (int v = threadIdx.x; v < Nv; v += FT) {
-      const V2 uv = face_velocity(d, v, n);
-      const double cx = uv.x - prim.s1, cy = uv.y - prim.s2, c2 = cx * cx + cy * cy;
-      const double t = c2 * fh[v] + fb[v] / d.K;
-      q[0] += 0.5 * (cx * t);
-      q[1] += 0.5 * (cy * t);
+    if (threadIdx.x < 32) {
+      if (threadIdx.x == 0) {
+        // getPLR slopes (clUGKS.c:424-436) and initMacroFlux (446-518)
+        const V2 cl = ld2(blk.centre, gidx(d, gi - dir, gj - (1 - dir)));
+        const V2 cr = ld2(blk.centre, gidx(d, gi, gj));
+        const double idl = 1.0 / sqrt((mid.x - cl.x) * (mid.x - cl.x) + (mid.y - cl.y) * (mid.y - cl.y));
+        const double idr = 1.0 / sqrt((mid.x - cr.x) * (mid.x - cr.x) + (mid.y - cr.y) * (mid.y - cr.y));
+        const P4 aL = micro_slope(d, prim, p4((W.s0 - m[4]) * idl, (W.s1 - m[5]) * idl,
+                                              (W.s2 - m[6]) * idl, (W.s3 - m[7]) * idl));
+        const P4 aR = micro_slope(d, prim, p4((m[8] - W.s0) * idr, (m[9] - W.s1) * idr,
+                                              (m[10] - W.s2) * idr, (m[11] - W.s3) * idr));
+        double Mu[MNUM], Mv[MTUM], Mxi[3], MuL[MNUM], MuR[MNUM], Mt[5];
+        moments_u(d, prim, Mu, Mv, Mxi, MuL, MuR);
+        const P4 aT = micro_slope(d, prim, scale(-prim.s0, add(moment_au(aL, MuL, Mv, Mxi, 1, 0),
+                                                               moment_au(aR, MuR, Mv, Mxi, 1, 0))));
+        time_weights(relax_time(d, prim), dt, Mt);
+        const P4 g0 = scale(prim.s0,
+                            add(add(scale(Mt[0], moment_uv(Mu, Mv, Mxi, 1, 0, 0)),
+                                    scale(Mt[1], add(moment_au(aL, MuL, Mv, Mxi, 2, 0),
+                                                     moment_au(aR, MuR, Mv, Mxi, 2, 0)))),
+                                scale(Mt[2], moment_au(aT, Mu, Mv, Mxi, 1, 0))));
+        double *c = sh.bcast;
+        c[4] = aL.s0; c[5] = aL.s1; c[6] = aL.s2; c[7] = aL.s3;
+        c[8] = aR.s0; c[9] = aR.s1; c[10] = aR.s2; c[11] = aR.s3;
+        c[12] = aT.s0; c[13] = aT.s1; c[14] = aT.s2; c[15] = aT.s3;
+        c[16] = Mt[0]; c[17] = Mt[1]; c[18] = Mt[2]; c[19] = Mt[3]; c[20] = Mt[4];
+        c[21] = Mxi[2];
+        c[22] = g0.s0; c[23] = g0.s1; c[24] = g0.s2; c[25] = g0.s3;
+      }
+    } else {
+      // meanwhile: face heat flux (calcFaceQ, clUGKS.c:522-585) and the
+      // axis factors of the face Maxwellian
+      const int t = threadIdx.x - 32, nt = FT - 32;
+      const double Kinv = 1.0 / d.K;
+      for (int v = t; v < Nv; v += nt) {
+        const V2 uv = face_velocity(d, v, n);
+        const double cx = uv.x - prim.s1, cy = uv.y - prim.s2, c2 = cx * cx + cy * cy;
+        const double tq = c2 * fh[v] + fb[v] * Kinv;
+        q[0] += 0.5 * (cx * tq);
+        q[1] += 0.5 * (cy * tq);
+      }
+      if (sep) {
+        axis_exp(Eu, d.quad, un, vn, 0, Ug.x, prim.s3, t, nt);
+        axis_exp(Ev, d.quad, vn, 1, 1, Ug.y, prim.s3, t, nt);
+      }
     }
     block_sum<2>(q, sh.scratch);
+    const double *c = sh.bcast;
     const V2 Q = v2(q[0], q[1]);
     const P4 aL = p4(c[4], c[5], c[6], c[7]), aR = p4(c[8], c[9], c[10], c[11]);
     const P4 aT = p4(c[12], c[13], c[14], c[15]);
-    const double Mt[5] = {c[16], c[17], c[18], c[19], c[20]};
-    const double Mxi2 = c[21];
+    const double Mt0 = c[16], Mt1 = c[17], Mt2 = c[18], Mt3 = c[19], Mt4 = c[20], Mxi2 = c[21];
+    // per-face constants of the Maxwellian (fM, clFunctions.c:49-58) and the
+    // Shakhov factor (fS, clFunctions.c:64-77)
+    const double ch = prim.s0 * (prim.s3 / d.PI);
+    const double kb = d.K / (2.0 * prim.s3);
+    const double s0 = 0.8 * (1 - d.Pr) * (prim.s3 * prim.s3) / prim.s0;
     // ---- sweep 3: macroFlux (587-681) and distFlux (683-772)
     double acc[4] = {0.0, 0.0, 0.0, 0.0};
     void *flux = dir == SOUTH ? blk.flux_S : blk.flux_W;
+    const int qs = sep ? FT / vn : 0, rs = sep ? FT % vn : 0;
+    int iu = sep ? threadIdx.x / vn : 0, jv = sep ? threadIdx.x % vn : 0;
     for (int v = threadIdx.x; v < Nv; v += FT) {
       const V2 uv = face_velocity(d, v, n);
-      const int delta = (int)((ocl_sign(uv.x) + 1) / 2);
-      const V2 f0 = maxwellian(d, prim, uv, v);
-      const V2 F0 = shakhov(d, prim, Q, uv, f0);
       const double u = uv.x, vt = uv.y, uu = u * u + vt * vt;
+      const double cx = u - prim.s1, cy = vt - prim.s2;
+      double E;
+      if (sep) {
+        E = Eu[iu] * Ev[jv];
+        jv += rs;
+        iu += qs;
+        if (jv >= vn) { jv -= vn; ++iu; }
+      } else {
+        E = exp(-prim.s3 * (cx * cx + cy * cy));
+      }
+      const double h0 = d.weight[v] * ch * E, b0 = h0 * kb;
+      const double S = s0 * (cx * Q.x + cy * Q.y), part = 2 * prim.s3 * (cx * cx + cy * cy);
+      const double F0h = (S * (part - 4)) * h0, F0b = (S * (part - 2)) * b0;
       const double fdh = fh[v], fdb = fb[v], fsh = sgh[v], fsb = sgb[v];
-      acc[0] += Mt[0] * u * F0.x + Mt[3] * u * fdh - Mt[4] * u * u * fsh;
-      acc[1] += Mt[0] * u * u * F0.x + Mt[3] * u * u * fdh - Mt[4] * u * u * u * fsh;
-      acc[2] += Mt[0] * vt * u * F0.x + Mt[3] * vt * u * fdh - Mt[4] * vt * u * u * fsh;
-      acc[3] += Mt[0] * 0.5 * (u * uu * F0.x + u * F0.y) + Mt[3] * 0.5 * (u * uu * fdh + u * fdb) -
-                Mt[4] * 0.5 * (u * u * uu * fsh + u * u * fsb);
-      const P4 a = delta ? aL : aR;
-      const double ph = a.s0 * f0.x + a.s1 * u * f0.x + a.s2 * vt * f0.x + 0.5 * a.s3 * (uu * f0.x + f0.y);
-      const double pb = a.s0 * f0.y + a.s1 * u * f0.y + a.s2 * vt * f0.y + 0.5 * a.s3 * (uu * f0.y + Mxi2 * f0.x);
-      const double th = aT.s0 * f0.x + aT.s1 * u * f0.x + aT.s2 * vt * f0.x + 0.5 * aT.s3 * (uu * f0.x + f0.y);
-      const double tb = aT.s0 * f0.y + aT.s1 * u * f0.y + aT.s2 * vt * f0.y + 0.5 * aT.s3 * (uu * f0.y + Mxi2 * f0.x);
-      const double hx = Mt[0] * u * (f0.x + F0.x) + Mt[1] * (u * u) * ph + Mt[2] * u * th +
-                        Mt[3] * u * fdh - Mt[4] * (u * u) * fsh;
-      const double hy = Mt[0] * u * (f0.y + F0.y) + Mt[1] * (u * u) * pb + Mt[2] * u * tb +
-                        Mt[3] * u * fdb - Mt[4] * (u * u) * fsb;
+      const double uu2 = u * u;
+      acc[0] += Mt0 * u * F0h + Mt3 * u * fdh - Mt4 * uu2 * fsh;
+      acc[1] += Mt0 * uu2 * F0h + Mt3 * uu2 * fdh - Mt4 * uu2 * u * fsh;
+      acc[2] += Mt0 * vt * u * F0h + Mt3 * vt * u * fdh - Mt4 * vt * uu2 * fsh;
+      acc[3] += Mt0 * 0.5 * (u * uu * F0h + u * F0b) + Mt3 * 0.5 * (u * uu * fdh + u * fdb) -
+                Mt4 * 0.5 * (uu2 * uu * fsh + uu2 * fsb);
+      const P4 a = u > 0.0 ? aL : aR;
+      const double pa = a.s0 + a.s1 * u + a.s2 * vt;
+      const double pt = aT.s0 + aT.s1 * u + aT.s2 * vt;
+      const double ph = h0 * (pa + 0.5 * a.s3 * (uu + kb));
+      const double pb = b0 * pa + 0.5 * a.s3 * (uu * b0 + Mxi2 * h0);
+      const double th = h0 * (pt + 0.5 * aT.s3 * (uu + kb));
+      const double tb = b0 * pt + 0.5 * aT.s3 * (uu * b0 + Mxi2 * h0);
+      const double hx = Mt0 * u * (h0 + F0h) + Mt1 * uu2 * ph + Mt2 * u * th + Mt3 * u * fdh - Mt4 * uu2 * fsh;
+      const double hy = Mt0 * u * (b0 + F0b) + Mt1 * uu2 * pb + Mt2 * u * tb + Mt3 * u * fdb - Mt4 * uu2 * fsb;
       St::store(flux, base + v, v2(len * hx, len * hy));
     }
     block_sum<4>(acc, sh.scratch);
@@ -275,7 +351,7 @@ __global__ void __launch_bounds__(FT) face_pass(const ugks_fused_block *__restri
     wl.s1 = t.x;
     wl.s2 = t.y;
   }
-  __syncthreads();  // sweep 1 results in shared memory
+  __syncthreads();
   if (blk.bc_type[wall] == BC_DIFFUSE) {
     // accommodatingWallDist (clUGKS.c:774-906)
     double s[2] = {0.0, 0.0};
@@ -430,8 +506,7 @@ __global__ void __launch_bounds__(FT) face_pass(const ugks_fused_block *__restri
 
 // ---------------------------------------------------------------------------
 // cell pass: calcQ (clKernel.c:480-543) + updateMacro (clUGKS.c:1158-1187) +
-// UGKS_update (clUGKS.c:1189-1257) + clFindDT (clKernel.c:224-308) + the
-// residual terms of getResidual (clUGKS.c:1259-1277)
+// UGKS_update (clUGKS.c:1189-1257) + clFindDT (clKernel.c:224-308)
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double cfl_freq(const ugks_fused_block &blk, P4 m, long mi, long mj) {
   const ugks_block_desc &d = blk.d;
@@ -453,10 +528,11 @@ __device__ __forceinline__ double cfl_freq(const ugks_fused_block &blk, P4 m, lo
 }
 
 template <typename T>
-__global__ void __launch_bounds__(FT) cell_pass(const ugks_fused_block *__restrict__ B, int nb,
-                                                ugks_solve_state *__restrict__ solves) {
+__global__ void __launch_bounds__(FT, CELL_MIN_BLOCKS) cell_pass(const ugks_fused_block *__restrict__ B, int nb,
+                                                   ugks_solve_state *__restrict__ solves) {
   __shared__ double scratch[2 * (FT / 32)];
   __shared__ double bc[12];
+  extern __shared__ double dyn[];  // axis factors: old (u, v), new (u, v)
   using St = Store<T>;
   const int w = blockIdx.x;
   const int bi = find_block<1>(B, nb, w);
@@ -468,58 +544,92 @@ __global__ void __launch_bounds__(FT) cell_pass(const ugks_fused_block *__restri
   const int lc = w - blk.cell_begin;
   const long mi = lc / d.nj, mj = lc % d.nj;
   const long gi = mi + d.ghost, gj = mj + d.ghost;
-  const int Nv = d.Nv;
+  const int Nv = d.Nv, un = d.u_num, vn = d.v_num;
+  const bool sep = un > 0 && un * vn == Nv && un + vn <= 512;
+  double *Eou = dyn, *Eov = Eou + un, *Enu = Eov + vn, *Env = Enu + un;
   const size_t base = fidx(d, gi, gj, 0);
   const P4 old = ld4(blk.macro, midx(d, mi, mj));
   // calcQ on f^n with the macro of f^n
   double q[2] = {0.0, 0.0};
+  const double Kinv = 1.0 / d.K;
   for (int v = threadIdx.x; v < Nv; v += FT) {
     const V2 f = St::load(blk.f, base + v);
     const V2 e = quad_at(d, v);
     const double cx = e.x - old.s1, cy = e.y - old.s2, c2 = cx * cx + cy * cy;
-    const double t = c2 * f.x + f.y / d.K;
+    const double t = c2 * f.x + f.y * Kinv;
     q[0] += 0.5 * (cx * t);
     q[1] += 0.5 * (cy * t);
   }
-  block_sum<2>(q, scratch);
   if (threadIdx.x == 0) {
-    st2(blk.Q, midx(d, mi, mj), v2(q[0], q[1]));
     // updateMacro
     const P4 wc = to_conserved(d, old);
-    const double A = blk.area[gidx(d, gi, gj)];
+    const double iA = 1.0 / blk.area[gidx(d, gi, gj)];
     const P4 s0 = ld4(blk.flux_macro_S, gidx(d, gi, gj)), s1 = ld4(blk.flux_macro_S, gidx(d, gi, gj + 1));
     const P4 w0 = ld4(blk.flux_macro_W, gidx(d, gi, gj)), w1 = ld4(blk.flux_macro_W, gidx(d, gi + 1, gj));
-    const P4 nw = p4(wc.s0 + (s0.s0 - s1.s0 + w0.s0 - w1.s0) / A, wc.s1 + (s0.s1 - s1.s1 + w0.s1 - w1.s1) / A,
-                     wc.s2 + (s0.s2 - s1.s2 + w0.s2 - w1.s2) / A, wc.s3 + (s0.s3 - s1.s3 + w0.s3 - w1.s3) / A);
+    const P4 nw = p4(wc.s0 + (s0.s0 - s1.s0 + w0.s0 - w1.s0) * iA, wc.s1 + (s0.s1 - s1.s1 + w0.s1 - w1.s1) * iA,
+                     wc.s2 + (s0.s2 - s1.s2 + w0.s2 - w1.s2) * iA, wc.s3 + (s0.s3 - s1.s3 + w0.s3 - w1.s3) * iA);
     const P4 prim = to_primary(d, nw);
     st4(blk.macro, midx(d, mi, mj), prim);
     st4(blk.prim_old, midx(d, mi, mj), old);
     bc[0] = prim.s0; bc[1] = prim.s1; bc[2] = prim.s2; bc[3] = prim.s3;
-    bc[4] = relax_time(d, old);
-    bc[5] = relax_time(d, prim);
-    bc[6] = A;
-    // CFL frequency of the updated cell (clFindDT)
+    bc[4] = 1.0 / relax_time(d, old);
+    bc[5] = 1.0 / relax_time(d, prim);
+    bc[6] = iA;
     const double fq = cfl_freq(blk, prim, mi, mj);
     atomicMax(&sol.max_freq, (unsigned long long)__double_as_longlong(fq));
+  } else if (sep && threadIdx.x >= 32) {
+    axis_exp(Eou, d.quad, un, vn, 0, old.s1, old.s3, threadIdx.x - 32, FT - 32);
+    axis_exp(Eov, d.quad, vn, 1, 1, old.s2, old.s3, threadIdx.x - 32, FT - 32);
   }
-  __syncthreads();
+  block_sum<2>(q, scratch);
+  if (threadIdx.x == 0) st2(blk.Q, midx(d, mi, mj), v2(q[0], q[1]));
   const P4 prim = p4(bc[0], bc[1], bc[2], bc[3]);
-  const double tau_old = bc[4], tau = bc[5], A = bc[6];
+  const double itau_old = bc[4], itau = bc[5], iA = bc[6];
+  if (sep) {
+    axis_exp(Enu, d.quad, un, vn, 0, prim.s1, prim.s3, threadIdx.x, FT);
+    axis_exp(Env, d.quad, vn, 1, 1, prim.s2, prim.s3, threadIdx.x, FT);
+    __syncthreads();
+  }
   const V2 Q = v2(q[0], q[1]);
-  const double den = 1.0 + 0.5 * dt / tau;
+  const double co = old.s0 * (old.s3 / d.PI), cn = prim.s0 * (prim.s3 / d.PI);
+  const double ko = d.K / (2.0 * old.s3), kn = d.K / (2.0 * prim.s3);
+  const double so = 0.8 * (1 - d.Pr) * (old.s3 * old.s3) / old.s0;
+  const double sn = 0.8 * (1 - d.Pr) * (prim.s3 * prim.s3) / prim.s0;
+  const double hdt = 0.5 * dt, iden = 1.0 / (1.0 + 0.5 * dt * itau);
   const size_t sj = (size_t)Nv, si = (size_t)d.Nj * Nv;
+  const int qs = sep ? FT / vn : 0, rs = sep ? FT % vn : 0;
+  int iu = sep ? threadIdx.x / vn : 0, jv = sep ? threadIdx.x % vn : 0;
   bool nan = false;
+#pragma unroll 2
   for (int v = threadIdx.x; v < Nv; v += FT) {
     const V2 e = quad_at(d, v);
-    const V2 fo = shakhov_eq(d, old, Q, e, v);
-    const V2 fn = shakhov_eq(d, prim, Q, e, v);
+    const double wv = d.weight[v];
+    const double ox = e.x - old.s1, oy = e.y - old.s2, o2 = ox * ox + oy * oy;
+    const double nx = e.x - prim.s1, ny = e.y - prim.s2, n2 = nx * nx + ny * ny;
+    double Eo, En;
+    if (sep) {
+      Eo = Eou[iu] * Eov[jv];
+      En = Enu[iu] * Env[jv];
+      jv += rs;
+      iu += qs;
+      if (jv >= vn) { jv -= vn; ++iu; }
+    } else {
+      Eo = exp(-old.s3 * o2);
+      En = exp(-prim.s3 * n2);
+    }
+    // fEQ (clFunctions.c:79-86) at the old and the new macro state
+    const double ho = wv * co * Eo, bo = ho * ko, hn = wv * cn * En, bn = hn * kn;
+    const double So = so * (ox * Q.x + oy * Q.y), po = 2 * old.s3 * o2;
+    const double Sn = sn * (nx * Q.x + ny * Q.y), pn = 2 * prim.s3 * n2;
+    const double foh = ho + (So * (po - 4)) * ho, fob = bo + (So * (po - 2)) * bo;
+    const double fnh = hn + (Sn * (pn - 4)) * hn, fnb = bn + (Sn * (pn - 2)) * bn;
     const size_t k = base + v;
     const V2 f = St::load(blk.f, k);
     const V2 a0 = St::load(blk.flux_S, k), a1 = St::load(blk.flux_S, k + sj);
     const V2 b0 = St::load(blk.flux_W, k), b1 = St::load(blk.flux_W, k + si);
-    const double flh = (a0.x - a1.x + b0.x - b1.x) / A, flb = (a0.y - a1.y + b0.y - b1.y) / A;
-    const double rh = fn.x / tau + (fo.x - f.x) / tau_old, rb = fn.y / tau + (fo.y - f.y) / tau_old;
-    const V2 out = v2((f.x + flh + 0.5 * dt * rh) / den, (f.y + flb + 0.5 * dt * rb) / den);
+    const double flh = (a0.x - a1.x + b0.x - b1.x) * iA, flb = (a0.y - a1.y + b0.y - b1.y) * iA;
+    const double rh = fnh * itau + (foh - f.x) * itau_old, rb = fnb * itau + (fob - f.y) * itau_old;
+    const V2 out = v2((f.x + flh + hdt * rh) * iden, (f.y + flb + hdt * rb) * iden);
     nan |= isnan(out.x) || isnan(out.y);
     St::store(blk.f, k, out);
   }
@@ -794,23 +904,45 @@ int init_impl(const ugks_fused_block *B, int nb, int32_t n_cells, int32_t n_ghos
 
 template <typename T>
 int step_impl(const ugks_fused_block *B, int nb, int32_t n_faces, int32_t n_cells, int32_t n_ghost,
-              ugks_solve_state *solves, int ns, int max_nv, void *stream) {
+              ugks_solve_state *solves, int ns, int max_nv, void *stream,
+              void *const *events = nullptr, int fm_mask = 3) {
   cudaStream_t st = S(stream);
-  const size_t smem = (size_t)4 * sizeof(double) * (size_t)max_nv;
+  // face pass: (h, b) and slopes per velocity + the two axis factor tables
+  const size_t smem = (size_t)4 * sizeof(double) * (size_t)max_nv + 2 * sizeof(double) * 512;
+  const size_t csmem = 4 * sizeof(double) * 512;
   static bool attr_set = false;  // one flag per instantiation
   if (!attr_set) {
-    cudaFuncSetAttribute(face_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(face_pass<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(face_pass<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    cudaFuncSetAttribute(face_pass<T, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_set = true;
   }
   if (smem > 200 * 1024) return -(int)cudaErrorInvalidValue;
   const unsigned sg = (unsigned)((ns + 127) / 128);
-  if (n_faces) face_pass<T><<<n_faces, FT, smem, st>>>(B, nb, solves, 0);
+  auto mark = [&](int k) {
+    if (events) cudaEventRecord(reinterpret_cast<cudaEvent_t>(events[k]), st);
+  };
+  auto faces = [&](int retry) {
+    if (!n_faces) return;
+    if (fm_mask & 1) face_pass<T, 0><<<n_faces, FT, smem, st>>>(B, nb, solves, retry);
+    if (fm_mask & 2) face_pass<T, 1><<<n_faces, FT, smem, st>>>(B, nb, solves, retry);
+    if (fm_mask & 8) face_pass<T, 3><<<n_faces, FT, smem, st>>>(B, nb, solves, retry);
+  };
+  mark(0);
+  faces(0);
+  mark(1);
   dt_check<<<sg, 128, 0, st>>>(solves, ns, 0);
-  if (n_faces) face_pass<T><<<n_faces, FT, smem, st>>>(B, nb, solves, 1);
+  mark(2);
+  faces(1);
+  mark(3);
   dt_check<<<sg, 128, 0, st>>>(solves, ns, 1);
-  if (n_cells) cell_pass<T><<<n_cells, FT, 0, st>>>(B, nb, solves);
+  mark(4);
+  if (n_cells) cell_pass<T><<<n_cells, FT, csmem, st>>>(B, nb, solves);
+  mark(5);
   dt_update<<<sg, 128, 0, st>>>(solves, ns);
+  mark(6);
   if (n_ghost) ghost_pass<T><<<n_ghost, FT, 0, st>>>(B, nb, solves);
+  mark(7);
   return launch_status();
 }
 
@@ -854,16 +986,25 @@ __global__ void residual_kernel(const ugks_fused_block *B, int nb, ugks_solve_st
 extern "C" {
 
 int ugks_step_fp64(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_faces, int32_t n_cells,
-                   int32_t n_ghost, int32_t max_nv, ugks_solve_state *solves_dev, int nsolves,
-                   void *stream) {
+                   int32_t n_ghost, int32_t max_nv, int32_t flux_methods,
+                   ugks_solve_state *solves_dev, int nsolves, void *stream) {
   return step_impl<double>(blocks_dev, nblocks, n_faces, n_cells, n_ghost, solves_dev, nsolves,
-                           max_nv, stream);
+                           max_nv, stream, nullptr, flux_methods);
 }
 int ugks_step_mixed(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_faces, int32_t n_cells,
-                    int32_t n_ghost, int32_t max_nv, ugks_solve_state *solves_dev, int nsolves,
-                    void *stream) {
+                    int32_t n_ghost, int32_t max_nv, int32_t flux_methods,
+                    ugks_solve_state *solves_dev, int nsolves, void *stream) {
   return step_impl<float>(blocks_dev, nblocks, n_faces, n_cells, n_ghost, solves_dev, nsolves,
-                          max_nv, stream);
+                          max_nv, stream, nullptr, flux_methods);
+}
+int ugks_step_profiled(int mixed, const ugks_fused_block *blocks_dev, int nblocks, int32_t n_faces,
+                       int32_t n_cells, int32_t n_ghost, int32_t max_nv, int32_t flux_methods,
+                       ugks_solve_state *solves_dev, int nsolves, void *const *events,
+                       void *stream) {
+  return mixed ? step_impl<float>(blocks_dev, nblocks, n_faces, n_cells, n_ghost, solves_dev,
+                                  nsolves, max_nv, stream, events, flux_methods)
+               : step_impl<double>(blocks_dev, nblocks, n_faces, n_cells, n_ghost, solves_dev,
+                                   nsolves, max_nv, stream, events, flux_methods);
 }
 int ugks_residual(const ugks_fused_block *blocks_dev, int nblocks, ugks_solve_state *solves_dev,
                   int nsolves, void *stream) {

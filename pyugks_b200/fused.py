@@ -74,6 +74,9 @@ class FusedSolver:
                    "ugks_fused_layout")
         self.n_faces, self.n_cells, self.n_ghost = nf.value, nc.value, ng.value
         self.max_nv = max(b.Nv for b in self.blocks)
+        self.flux_methods = 0
+        for case in self.cases:
+            self.flux_methods |= 1 << D.FLUX_METHODS[case["flux_method"]]
         raw = np.frombuffer(bytes(arr), dtype=np.uint8).copy()
         self.table = torch.from_numpy(raw).to(self.device)
         self.nblocks = len(structs)
@@ -133,6 +136,7 @@ class FusedSolver:
         d = x.d
         d.ni, d.nj, d.Ni, d.Nj, d.ghost, d.Nv = ni, nj, Ni, Nj, G, Nv
         d.flux_method, d.relax_type = const.flux_code, const.relax_type
+        d.u_num, d.v_num = const.vgrid.u_num, const.vgrid.v_num
         d.PI, d.Pr, d.umax, d.vmax = const.PI, const.Pr, const.umax, const.vmax
         d.Kn_eff, d.gam, d.K, d.omega = const.Kn_eff, const.gam, const.K, const.omega
         d.quad, d.weight = tabs["quad"].data_ptr(), tabs["weight"].data_ptr()
@@ -177,8 +181,8 @@ class FusedSolver:
         """Advance every active solve by n steps (asynchronous)."""
         for _ in range(n):
             _lib.check(self._step_fn(self.table.data_ptr(), self.nblocks, self.n_faces, self.n_cells,
-                                     self.n_ghost, self.max_nv, self.solves.data_ptr(), self.nsolves,
-                                     self._sptr()), "ugks_step")
+                                     self.n_ghost, self.max_nv, self.flux_methods, self.solves.data_ptr(),
+                                     self.nsolves, self._sptr()), "ugks_step")
 
     def capture(self, steps: int):
         """Capture `steps` steps as one CUDA graph; ``replay()`` runs it."""

@@ -1,0 +1,72 @@
+"""Generate the golden fixtures of tests/golden/ from the reference itself.
+
+Runs pyUGKS's own OpenCL kernels, compiled for the CPU by oracle/ref_build.py
+from the reference sources (so it needs them, under $UGKS_REFERENCE or
+/root/reference), driven by the oracle's restatement of the reference step
+sequence (oracle/host.py), and stores macroscopic fields (rho, U, V, T, qx,
+qy), dt and time at several step counts -- plus the full interior f for the
+small cases -- as compressed .npz files:
+
+    python tests/golden/make_golden.py
+
+Cases:
+  cavity8      8x8 cavity, 9x9 velocities on [-4,4]^2, vanLeer        (f, steps 1/10/50)
+  multiblock8  2x2 blocks of 8x8, 9x9 velocities on [-5,5]^2, WENO5   (f, steps 1/10/30)
+  channel8     2-block adsorbing channel 8x8, Langmuir desorption     (f + coverage, 1/10/30)
+  cavity32     the 32x32 cavity, 25x25 velocities on [-4,4]^2, vanLeer, Kn 0.075,
+               CFL 0.8, lid 0.15 (fields at steps 1/10/100/1000)
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+
+import host  # noqa: E402
+from pyugks_b200 import configs  # noqa: E402
+
+CASES = {
+    "cavity8": (lambda: configs.cavity(n=8, m=8, vlim=4.0), (1, 10, 50), True),
+    "multiblock8": (lambda: configs.cavity_multiblock(nb=2, n=8, m=8), (1, 10, 30), True),
+    "channel8": (lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0), (1, 10, 30), True),
+    "cavity32": (lambda: configs.cavity(n=32, m=24, vlim=4.0), (1, 10, 100, 1000), False),
+}
+
+
+def record(sim, with_f):
+    out = {"dt": np.array(sim.dt), "time": np.array(sim.time)}
+    for k, fl in enumerate(sim.fields()):
+        for name, arr in fl.items():
+            out["b%d_%s" % (k, name)] = arr
+    if with_f:
+        for k, f in enumerate(sim.interior_f()):
+            out["b%d_f" % k] = f
+        for k, b in enumerate(sim.blocks):
+            out["b%d_cover" % k] = b.wall_cover.copy()
+    return out
+
+
+def main(names=None):
+    for name, (make, steps, with_f) in CASES.items():
+        if names and name not in names:
+            continue
+        sim = host.OracleSim(make(), "ref", threads=os.cpu_count())
+        data = {}
+        done = 0
+        for s in steps:
+            while done < s:
+                sim.one_step()
+                done += 1
+            for k, v in record(sim, with_f).items():
+                data["s%d_%s" % (s, k)] = v
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, **data)
+        print(path, os.path.getsize(path))
+
+
+if __name__ == "__main__":
+    main(sys.argv[1:])
