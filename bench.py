@@ -32,6 +32,7 @@ the max over ranks.
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import statistics
@@ -216,11 +217,10 @@ def run_ours(args, rank, world, dist):
         torch.cuda.synchronize(dev)
         start.record(stream)
         for k in range(args.steps):
-            _lib.check(L.ugks_step_profiled(mixed, solver.table.data_ptr(), solver.nblocks, solver.n_faces,
-                                            solver.n_cells, solver.n_ghost, solver.max_nv,
-                                            solver.flux_methods, solver.solves.data_ptr(),
-                                            solver.nsolves, handles[k],
-                                            stream.cuda_stream), "ugks_step_profiled")
+            _lib.check(L.ugks_step_profiled(mixed, solver.table.data_ptr(), solver.nblocks,
+                                            C.byref(solver.sizes), solver.solves.data_ptr(),
+                                            solver.nsolves, handles[k], stream.cuda_stream),
+                       "ugks_step_profiled")
         end.record(stream)
         torch.cuda.synchronize(dev)
         if smi is not None:

@@ -254,35 +254,44 @@ typedef struct ugks_solve_state {
   int32_t retries;             /* flux passes redone so far                 */
   int32_t active;              /* 0: skipped by every fused kernel          */
   int32_t nblocks;             /* blocks of this solve                      */
+  int32_t first_block;         /* index of its first block in the table     */
+  int32_t pad_;
   double residual[4];          /* written by ugks_residual: mean over blocks
                                   of sqrt(ni nj sum (dprim)^2) / sum |prim|
                                   (ugks_block.py:1319-1327, ugks_sim.py:463-468) */
 } ugks_solve_state;
 
-/* Work sizes of a block table (computed on the host): number of face,
-   cell and ghost-cell work items.  Fills face_begin/cell_begin/ghost_begin
-   of the host copy `blocks` and returns the totals. */
-int ugks_fused_layout(ugks_fused_block *blocks, int nblocks, int32_t *n_faces,
-                      int32_t *n_cells, int32_t *n_ghost);
+/* Work sizes of a block table, computed on the host by ugks_fused_layout. */
+typedef struct ugks_fused_sizes {
+  int32_t n_faces;        /* face work items (2 per cell corner of every block) */
+  int32_t n_cells;        /* interior cells                                    */
+  int32_t n_ghost;        /* ghost cells of the four strips of every block     */
+  int32_t max_nv;         /* largest Nv (sizes the face pass's shared memory)  */
+  int32_t face_begin[4];  /* first face work item of the blocks of flux_method k */
+  int32_t face_count[4];  /* their number (0 when no block uses method k)      */
+} ugks_fused_sizes;
+
+/* Fills face_begin/cell_begin/ghost_begin of the host copy `blocks` and the
+   sizes.  The blocks of one solve must be contiguous and in the order of
+   their solve index, and the blocks of one flux method contiguous (group the
+   solves by flux method).  Returns 0, -1 when a count exceeds INT32_MAX, -2
+   when the ordering rule is broken. */
+int ugks_fused_layout(ugks_fused_block *blocks, int nblocks, ugks_fused_sizes *sizes);
 
 /* Initial state (ugks_block.py:411-429, ugks_sim.py:88-92): f := fEQ(macro,
    Q) on interior cells, macro := moments(f), Q := heat flux(f), wall_prop
    from the wall values, ghosts filled, dt := CFL / max frequency. */
-int ugks_init_fp64(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_cells,
-                   int32_t n_ghost, ugks_solve_state *solves_dev, int nsolves, UGKS_STREAM);
-int ugks_init_mixed(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_cells,
-                    int32_t n_ghost, ugks_solve_state *solves_dev, int nsolves, UGKS_STREAM);
+int ugks_init_fp64(const ugks_fused_block *blocks_dev, int nblocks, const ugks_fused_sizes *sizes,
+                   ugks_solve_state *solves_dev, int nsolves, UGKS_STREAM);
+int ugks_init_mixed(const ugks_fused_block *blocks_dev, int nblocks, const ugks_fused_sizes *sizes,
+                    ugks_solve_state *solves_dev, int nsolves, UGKS_STREAM);
 
 /* One UGKSim.one_step (ugks_sim.py:407-501) of every active solve: flux
    pass, dt check with the reference's single retry, cell update, new dt,
-   time advance, ghost update.  max_nv: largest Nv of the table (sizes the
-   face pass's shared memory, 32 bytes per velocity); flux_methods: bit k set
-   when some block uses flux_method k (one face-pass launch per method). */
-int ugks_step_fp64(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_faces,
-                   int32_t n_cells, int32_t n_ghost, int32_t max_nv, int32_t flux_methods,
+   time advance, ghost update. */
+int ugks_step_fp64(const ugks_fused_block *blocks_dev, int nblocks, const ugks_fused_sizes *sizes,
                    ugks_solve_state *solves_dev, int nsolves, UGKS_STREAM);
-int ugks_step_mixed(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_faces,
-                    int32_t n_cells, int32_t n_ghost, int32_t max_nv, int32_t flux_methods,
+int ugks_step_mixed(const ugks_fused_block *blocks_dev, int nblocks, const ugks_fused_sizes *sizes,
                     ugks_solve_state *solves_dev, int nsolves, UGKS_STREAM);
 
 /* The same step with cudaEventRecord of events[0..7] (cudaEvent_t) on the
@@ -290,10 +299,9 @@ int ugks_step_mixed(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_f
    dt check, [3] after the retry face pass, [4] after the second dt check,
    [5] after the cell pass, [6] after the dt update, [7] after the ghost pass.
    mixed != 0 selects FP32 storage.  Used to time each kernel live. */
-int ugks_step_profiled(int mixed, const ugks_fused_block *blocks_dev, int nblocks, int32_t n_faces,
-                       int32_t n_cells, int32_t n_ghost, int32_t max_nv, int32_t flux_methods,
-                       ugks_solve_state *solves_dev, int nsolves, void *const *events,
-                       UGKS_STREAM);
+int ugks_step_profiled(int mixed, const ugks_fused_block *blocks_dev, int nblocks,
+                       const ugks_fused_sizes *sizes, ugks_solve_state *solves_dev, int nsolves,
+                       void *const *events, UGKS_STREAM);
 
 /* Residual of the last step (getResidual + the host reduction of
    ugks_block.py:1303-1327, averaged over a solve's blocks as

@@ -53,9 +53,15 @@ class SolveState(C.Structure):
         ("dt", f64), ("time", f64), ("CFL", f64), ("delta_dt", f64), ("max_dt", f64),
         ("max_freq", C.c_uint64),
         ("retry", i32), ("status", i32), ("steps", i32), ("retries", i32), ("active", i32),
-        ("nblocks", i32),
+        ("nblocks", i32), ("first_block", i32), ("pad_", i32),
         ("residual", f64 * 4),
     ]
+
+
+class FusedSizes(C.Structure):
+    """ugks_fused_sizes"""
+    _fields_ = [("n_faces", i32), ("n_cells", i32), ("n_ghost", i32), ("max_nv", i32),
+                ("face_begin", i32 * 4), ("face_count", i32 * 4)]
 
 
 # argument kinds of the drop-in kernels in reference order (p pointer, i int,
@@ -98,18 +104,13 @@ def lib():
     L.ugks_array_max.restype = C.c_int
     L.ugks_array_max.argtypes = [vp, C.c_size_t, vp, vp]
     L.ugks_fused_layout.restype = C.c_int
-    L.ugks_fused_layout.argtypes = [C.POINTER(FusedBlock), C.c_int, C.POINTER(i32), C.POINTER(i32),
-                                    C.POINTER(i32)]
-    for nm in ("ugks_init_fp64", "ugks_init_mixed"):
+    L.ugks_fused_layout.argtypes = [C.POINTER(FusedBlock), C.c_int, C.POINTER(FusedSizes)]
+    for nm in ("ugks_init_fp64", "ugks_init_mixed", "ugks_step_fp64", "ugks_step_mixed"):
         fn = getattr(L, nm)
         fn.restype = C.c_int
-        fn.argtypes = [vp, C.c_int, i32, i32, vp, C.c_int, vp]
-    for nm in ("ugks_step_fp64", "ugks_step_mixed"):
-        fn = getattr(L, nm)
-        fn.restype = C.c_int
-        fn.argtypes = [vp, C.c_int, i32, i32, i32, i32, i32, vp, C.c_int, vp]
+        fn.argtypes = [vp, C.c_int, C.POINTER(FusedSizes), vp, C.c_int, vp]
     L.ugks_step_profiled.restype = C.c_int
-    L.ugks_step_profiled.argtypes = [C.c_int, vp, C.c_int, i32, i32, i32, i32, i32, vp, C.c_int, vp, vp]
+    L.ugks_step_profiled.argtypes = [C.c_int, vp, C.c_int, C.POINTER(FusedSizes), vp, C.c_int, vp, vp]
     L.ugks_residual.restype = C.c_int
     L.ugks_residual.argtypes = [vp, C.c_int, vp, C.c_int, vp]
     L.ugks_version.restype = C.c_char_p

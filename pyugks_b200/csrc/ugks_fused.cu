@@ -147,14 +147,15 @@ __device__ __forceinline__ void axis_exp(double *out, const double *quad, int n,
   }
 }
 
+// one face work item (all threads of the CTA take part)
 template <typename T, int FM>
-__global__ void __launch_bounds__(FT, FACE_MIN_BLOCKS) face_pass(const ugks_fused_block *__restrict__ B, int nb,
-                                                   ugks_solve_state *__restrict__ solves, int retry_pass) {
+__device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B, int nb,
+                                          ugks_solve_state *__restrict__ solves, const int w,
+                                          int retry_pass) {
   extern __shared__ double dyn[];
   __shared__ FaceShared sh;
   using St = Store<T>;
 
-  const int w = blockIdx.x;
   const int bi = find_block<0>(B, nb, w);
   const ugks_fused_block &blk = B[bi];
   const ugks_block_desc &d = blk.d;
@@ -501,6 +502,34 @@ __global__ void __launch_bounds__(FT, FACE_MIN_BLOCKS) face_pass(const ugks_fuse
     double *wf = blk.wall_fluxes + 8 * (ci * 4 + wall);
     wf[0] = -rot * s[4]; wf[1] = rot * s[8]; wf[2] = -rot * s[5]; wf[3] = rot * s[9];
     wf[4] = -rot * s[6]; wf[5] = rot * s[10]; wf[6] = -rot * s[7]; wf[7] = rot * s[11];
+  }
+}
+
+// main face pass: one CTA per face work item of the blocks of one flux method
+template <typename T, int FM>
+__global__ void __launch_bounds__(FT, FACE_MIN_BLOCKS) face_pass(const ugks_fused_block *__restrict__ B, int nb,
+                                                                 ugks_solve_state *__restrict__ solves,
+                                                                 int first) {
+  face_item<T, FM>(B, nb, solves, first + (int)blockIdx.x, 0);
+}
+
+// the flux pass redone after a dt change (ugks_sim.py:432-441): RETRY_CTAS
+// CTAs per solve; a solve whose retry flag is clear costs one early exit each
+constexpr int RETRY_CTAS = 148;
+template <typename T, int FM>
+__global__ void __launch_bounds__(FT, FACE_MIN_BLOCKS) face_retry(const ugks_fused_block *__restrict__ B, int nb,
+                                                                  ugks_solve_state *__restrict__ solves,
+                                                                  int ns) {
+  const int s = blockIdx.x / RETRY_CTAS, r = blockIdx.x % RETRY_CTAS;
+  if (s >= ns) return;
+  const ugks_solve_state &x = solves[s];
+  if (!x.active || !x.retry || x.nblocks <= 0) return;
+  const ugks_fused_block &b0 = B[x.first_block], &bl = B[x.first_block + x.nblocks - 1];
+  if (b0.d.flux_method != FM) return;
+  const int end = bl.face_begin + 2 * (bl.d.ni + 1) * (bl.d.nj + 1);
+  for (int w = b0.face_begin + r; w < end; w += RETRY_CTAS) {
+    face_item<T, FM>(B, nb, solves, w, 1);
+    __syncthreads();  // the next item reuses the shared tables
   }
 }
 
@@ -892,56 +921,60 @@ __global__ void dt_init(ugks_solve_state *solves, int ns) {
 }
 
 template <typename T>
-int init_impl(const ugks_fused_block *B, int nb, int32_t n_cells, int32_t n_ghost,
-              ugks_solve_state *solves, int ns, void *stream) {
+int init_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks_solve_state *solves,
+              int ns, void *stream) {
   cudaStream_t st = S(stream);
   init_walls<<<nb, 128, 0, st>>>(B, nb);
-  if (n_cells) init_cells<T><<<n_cells, FT, 0, st>>>(B, nb, solves);
+  if (z->n_cells) init_cells<T><<<z->n_cells, FT, 0, st>>>(B, nb, solves);
   dt_init<<<(ns + 127) / 128, 128, 0, st>>>(solves, ns);
-  if (n_ghost) ghost_pass<T><<<n_ghost, FT, 0, st>>>(B, nb, solves);
+  if (z->n_ghost) ghost_pass<T><<<z->n_ghost, FT, 0, st>>>(B, nb, solves);
   return launch_status();
 }
 
+template <typename T, int FM>
+void set_face_attributes() {
+  cudaFuncSetAttribute(face_pass<T, FM>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(face_retry<T, FM>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+}
+
 template <typename T>
-int step_impl(const ugks_fused_block *B, int nb, int32_t n_faces, int32_t n_cells, int32_t n_ghost,
-              ugks_solve_state *solves, int ns, int max_nv, void *stream,
-              void *const *events = nullptr, int fm_mask = 3) {
+int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks_solve_state *solves,
+              int ns, void *stream, void *const *events = nullptr) {
   cudaStream_t st = S(stream);
   // face pass: (h, b) and slopes per velocity + the two axis factor tables
-  const size_t smem = (size_t)4 * sizeof(double) * (size_t)max_nv + 2 * sizeof(double) * 512;
+  const size_t smem = (size_t)4 * sizeof(double) * (size_t)z->max_nv + 2 * sizeof(double) * 512;
   const size_t csmem = 4 * sizeof(double) * 512;
   static bool attr_set = false;  // one flag per instantiation
   if (!attr_set) {
-    cudaFuncSetAttribute(face_pass<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(face_pass<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(face_pass<T, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    set_face_attributes<T, 0>();
+    set_face_attributes<T, 1>();
+    set_face_attributes<T, 3>();
     attr_set = true;
   }
   if (smem > 200 * 1024) return -(int)cudaErrorInvalidValue;
   const unsigned sg = (unsigned)((ns + 127) / 128);
+  const unsigned rg = (unsigned)ns * RETRY_CTAS;
   auto mark = [&](int k) {
     if (events) cudaEventRecord(reinterpret_cast<cudaEvent_t>(events[k]), st);
   };
-  auto faces = [&](int retry) {
-    if (!n_faces) return;
-    if (fm_mask & 1) face_pass<T, 0><<<n_faces, FT, smem, st>>>(B, nb, solves, retry);
-    if (fm_mask & 2) face_pass<T, 1><<<n_faces, FT, smem, st>>>(B, nb, solves, retry);
-    if (fm_mask & 8) face_pass<T, 3><<<n_faces, FT, smem, st>>>(B, nb, solves, retry);
-  };
   mark(0);
-  faces(0);
+  if (z->face_count[0]) face_pass<T, 0><<<z->face_count[0], FT, smem, st>>>(B, nb, solves, z->face_begin[0]);
+  if (z->face_count[1]) face_pass<T, 1><<<z->face_count[1], FT, smem, st>>>(B, nb, solves, z->face_begin[1]);
+  if (z->face_count[3]) face_pass<T, 3><<<z->face_count[3], FT, smem, st>>>(B, nb, solves, z->face_begin[3]);
   mark(1);
   dt_check<<<sg, 128, 0, st>>>(solves, ns, 0);
   mark(2);
-  faces(1);
+  if (z->face_count[0]) face_retry<T, 0><<<rg, FT, smem, st>>>(B, nb, solves, ns);
+  if (z->face_count[1]) face_retry<T, 1><<<rg, FT, smem, st>>>(B, nb, solves, ns);
+  if (z->face_count[3]) face_retry<T, 3><<<rg, FT, smem, st>>>(B, nb, solves, ns);
   mark(3);
   dt_check<<<sg, 128, 0, st>>>(solves, ns, 1);
   mark(4);
-  if (n_cells) cell_pass<T><<<n_cells, FT, csmem, st>>>(B, nb, solves);
+  if (z->n_cells) cell_pass<T><<<z->n_cells, FT, csmem, st>>>(B, nb, solves);
   mark(5);
   dt_update<<<sg, 128, 0, st>>>(solves, ns);
   mark(6);
-  if (n_ghost) ghost_pass<T><<<n_ghost, FT, 0, st>>>(B, nb, solves);
+  if (z->n_ghost) ghost_pass<T><<<z->n_ghost, FT, 0, st>>>(B, nb, solves);
   mark(7);
   return launch_status();
 }
@@ -985,26 +1018,19 @@ __global__ void residual_kernel(const ugks_fused_block *B, int nb, ugks_solve_st
 
 extern "C" {
 
-int ugks_step_fp64(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_faces, int32_t n_cells,
-                   int32_t n_ghost, int32_t max_nv, int32_t flux_methods,
+int ugks_step_fp64(const ugks_fused_block *blocks_dev, int nblocks, const ugks_fused_sizes *sizes,
                    ugks_solve_state *solves_dev, int nsolves, void *stream) {
-  return step_impl<double>(blocks_dev, nblocks, n_faces, n_cells, n_ghost, solves_dev, nsolves,
-                           max_nv, stream, nullptr, flux_methods);
+  return step_impl<double>(blocks_dev, nblocks, sizes, solves_dev, nsolves, stream);
 }
-int ugks_step_mixed(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_faces, int32_t n_cells,
-                    int32_t n_ghost, int32_t max_nv, int32_t flux_methods,
+int ugks_step_mixed(const ugks_fused_block *blocks_dev, int nblocks, const ugks_fused_sizes *sizes,
                     ugks_solve_state *solves_dev, int nsolves, void *stream) {
-  return step_impl<float>(blocks_dev, nblocks, n_faces, n_cells, n_ghost, solves_dev, nsolves,
-                          max_nv, stream, nullptr, flux_methods);
+  return step_impl<float>(blocks_dev, nblocks, sizes, solves_dev, nsolves, stream);
 }
-int ugks_step_profiled(int mixed, const ugks_fused_block *blocks_dev, int nblocks, int32_t n_faces,
-                       int32_t n_cells, int32_t n_ghost, int32_t max_nv, int32_t flux_methods,
-                       ugks_solve_state *solves_dev, int nsolves, void *const *events,
-                       void *stream) {
-  return mixed ? step_impl<float>(blocks_dev, nblocks, n_faces, n_cells, n_ghost, solves_dev,
-                                  nsolves, max_nv, stream, events, flux_methods)
-               : step_impl<double>(blocks_dev, nblocks, n_faces, n_cells, n_ghost, solves_dev,
-                                   nsolves, max_nv, stream, events, flux_methods);
+int ugks_step_profiled(int mixed, const ugks_fused_block *blocks_dev, int nblocks,
+                       const ugks_fused_sizes *sizes, ugks_solve_state *solves_dev, int nsolves,
+                       void *const *events, void *stream) {
+  return mixed ? step_impl<float>(blocks_dev, nblocks, sizes, solves_dev, nsolves, stream, events)
+               : step_impl<double>(blocks_dev, nblocks, sizes, solves_dev, nsolves, stream, events);
 }
 int ugks_residual(const ugks_fused_block *blocks_dev, int nblocks, ugks_solve_state *solves_dev,
                   int nsolves, void *stream) {
@@ -1013,32 +1039,54 @@ int ugks_residual(const ugks_fused_block *blocks_dev, int nblocks, ugks_solve_st
   return launch_status();
 }
 
-int ugks_fused_layout(ugks_fused_block *blocks, int nblocks, int32_t *n_faces, int32_t *n_cells,
-                      int32_t *n_ghost) {
+int ugks_fused_layout(ugks_fused_block *blocks, int nblocks, ugks_fused_sizes *z) {
   int64_t f = 0, c = 0, g = 0;
+  int32_t max_nv = 0;
+  int64_t fb[4] = {0, 0, 0, 0}, fc[4] = {0, 0, 0, 0};
+  int last_method = -1, seen = 0, last_solve = -1;
   for (int b = 0; b < nblocks; ++b) {
     ugks_fused_block &x = blocks[b];
+    const int m = x.d.flux_method;
+    if (m < 0 || m > 3) return -2;
+    if (m != last_method) {
+      if (seen & (1 << m)) return -2;  // methods must be contiguous
+      seen |= 1 << m;
+      fb[m] = f;
+      last_method = m;
+    }
+    if (x.solve != last_solve) {
+      if (x.solve != last_solve + 1) return -2;  // solves contiguous and in order
+      last_solve = x.solve;
+    }
     x.face_begin = (int32_t)f;
     x.cell_begin = (int32_t)c;
     x.ghost_begin = (int32_t)g;
-    f += 2ll * (x.d.ni + 1) * (x.d.nj + 1);
+    const int64_t nf = 2ll * (x.d.ni + 1) * (x.d.nj + 1);
+    f += nf;
+    fc[m] += nf;
     c += (int64_t)x.d.ni * x.d.nj;
     g += 2ll * x.d.ghost * (x.d.ni + x.d.nj);
+    if (x.d.Nv > max_nv) max_nv = x.d.Nv;
   }
   if (f > INT32_MAX || c > INT32_MAX || g > INT32_MAX) return -1;
-  *n_faces = (int32_t)f;
-  *n_cells = (int32_t)c;
-  *n_ghost = (int32_t)g;
+  z->n_faces = (int32_t)f;
+  z->n_cells = (int32_t)c;
+  z->n_ghost = (int32_t)g;
+  z->max_nv = max_nv;
+  for (int m = 0; m < 4; ++m) {
+    z->face_begin[m] = (int32_t)fb[m];
+    z->face_count[m] = (int32_t)fc[m];
+  }
   return 0;
 }
 
-int ugks_init_fp64(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_cells, int32_t n_ghost,
+int ugks_init_fp64(const ugks_fused_block *blocks_dev, int nblocks, const ugks_fused_sizes *sizes,
                    ugks_solve_state *solves_dev, int nsolves, void *stream) {
-  return init_impl<double>(blocks_dev, nblocks, n_cells, n_ghost, solves_dev, nsolves, stream);
+  return init_impl<double>(blocks_dev, nblocks, sizes, solves_dev, nsolves, stream);
 }
-int ugks_init_mixed(const ugks_fused_block *blocks_dev, int nblocks, int32_t n_cells, int32_t n_ghost,
+int ugks_init_mixed(const ugks_fused_block *blocks_dev, int nblocks, const ugks_fused_sizes *sizes,
                     ugks_solve_state *solves_dev, int nsolves, void *stream) {
-  return init_impl<float>(blocks_dev, nblocks, n_cells, n_ghost, solves_dev, nsolves, stream);
+  return init_impl<float>(blocks_dev, nblocks, sizes, solves_dev, nsolves, stream);
 }
 
 }  // extern "C"

@@ -47,7 +47,15 @@ class FusedSolver:
         self.sdtype = torch.float64 if precision == "fp64" else torch.float32
         if isinstance(cases, dict):
             cases = [cases]
-        self.cases = list(cases)
+        cases = list(cases)
+        # solves are stored grouped by flux method (one face-pass launch per
+        # method covers a contiguous range); order[k] is the internal index
+        # of the caller's solve k
+        perm = sorted(range(len(cases)), key=lambda k: D.FLUX_METHODS[cases[k]["flux_method"]])
+        self.order = [0] * len(cases)
+        for internal, k in enumerate(perm):
+            self.order[k] = internal
+        self.cases = [cases[k] for k in perm]
         self.blocks = []
         self.solve_blocks = []
         self._keep = []
@@ -69,14 +77,12 @@ class FusedSolver:
                 structs.append(blk.struct)
             self.solve_blocks.append(ids)
         arr = (_lib.FusedBlock * len(structs))(*structs)
-        nf, nc, ng = _lib.i32(), _lib.i32(), _lib.i32()
-        _lib.check(self.lib.ugks_fused_layout(arr, len(structs), C.byref(nf), C.byref(nc), C.byref(ng)) and -1,
-                   "ugks_fused_layout")
-        self.n_faces, self.n_cells, self.n_ghost = nf.value, nc.value, ng.value
-        self.max_nv = max(b.Nv for b in self.blocks)
-        self.flux_methods = 0
-        for case in self.cases:
-            self.flux_methods |= 1 << D.FLUX_METHODS[case["flux_method"]]
+        self.sizes = _lib.FusedSizes()
+        rc = self.lib.ugks_fused_layout(arr, len(structs), C.byref(self.sizes))
+        if rc != 0:
+            raise RuntimeError("ugks_fused_layout rejected the block table (%d)" % rc)
+        self.n_faces, self.n_cells, self.n_ghost = self.sizes.n_faces, self.sizes.n_cells, self.sizes.n_ghost
+        self.max_nv = self.sizes.max_nv
         raw = np.frombuffer(bytes(arr), dtype=np.uint8).copy()
         self.table = torch.from_numpy(raw).to(self.device)
         self.nblocks = len(structs)
@@ -86,11 +92,12 @@ class FusedSolver:
             st[s].delta_dt = float(case.get("delta_dt", 1.0))
             st[s].active = 1
             st[s].nblocks = len(self.solve_blocks[s])
+            st[s].first_block = self.solve_blocks[s][0]
         self.solves = torch.from_numpy(np.frombuffer(bytes(st), dtype=np.uint8).copy()).to(self.device)
         self.nsolves = len(self.cases)
         self._stream = stream
         init = self.lib.ugks_init_fp64 if precision == "fp64" else self.lib.ugks_init_mixed
-        _lib.check(init(self.table.data_ptr(), self.nblocks, self.n_cells, self.n_ghost,
+        _lib.check(init(self.table.data_ptr(), self.nblocks, C.byref(self.sizes),
                         self.solves.data_ptr(), self.nsolves, self._sptr()), "ugks_init")
         self._step_fn = self.lib.ugks_step_fp64 if precision == "fp64" else self.lib.ugks_step_mixed
         self.graph = None
@@ -180,9 +187,8 @@ class FusedSolver:
     def step(self, n: int = 1):
         """Advance every active solve by n steps (asynchronous)."""
         for _ in range(n):
-            _lib.check(self._step_fn(self.table.data_ptr(), self.nblocks, self.n_faces, self.n_cells,
-                                     self.n_ghost, self.max_nv, self.flux_methods, self.solves.data_ptr(),
-                                     self.nsolves, self._sptr()), "ugks_step")
+            _lib.check(self._step_fn(self.table.data_ptr(), self.nblocks, C.byref(self.sizes),
+                                     self.solves.data_ptr(), self.nsolves, self._sptr()), "ugks_step")
 
     def capture(self, steps: int):
         """Capture `steps` steps as one CUDA graph; ``replay()`` runs it."""
@@ -214,22 +220,24 @@ class FusedSolver:
         """Host copy of every ugks_solve_state (synchronises)."""
         raw = self.solves.cpu().numpy().tobytes()
         arr = (_lib.SolveState * self.nsolves).from_buffer_copy(raw)
-        return [dict(dt=x.dt, time=x.time, max_dt=x.max_dt, status=x.status, steps=x.steps,
-                     retries=x.retries, active=x.active, residual=list(x.residual)) for x in arr]
+        out = [dict(dt=x.dt, time=x.time, max_dt=x.max_dt, status=x.status, steps=x.steps,
+                    retries=x.retries, active=x.active, residual=list(x.residual)) for x in arr]
+        return [out[self.order[k]] for k in range(self.nsolves)]
 
     def set_active(self, flags):
         """Switch solves on/off for the next steps (device-side flag)."""
         torch = _torch()
         st = (_lib.SolveState * self.nsolves).from_buffer_copy(self.solves.cpu().numpy().tobytes())
-        for s, a in enumerate(flags):
-            st[s].active = 1 if a else 0
+        for k, a in enumerate(flags):
+            st[self.order[k]].active = 1 if a else 0
         self.solves.copy_(torch.from_numpy(np.frombuffer(bytes(st), dtype=np.uint8).copy()))
 
     def fields(self, solve: int = 0):
-        """Per block interior fields of one solve as numpy: rho, U, V, T, qx, qy
-        (Q re-taken from the current f, as the reference's updateHost does)."""
+        """Per block interior fields of one solve (caller's index) as numpy:
+        rho, U, V, T, qx, qy (Q re-taken from the current f, as the
+        reference's updateHost does)."""
         out = []
-        for bi in self.solve_blocks[solve]:
+        for bi in self.solve_blocks[self.order[solve]]:
             b = self.blocks[bi]
             m = b.macro.cpu().numpy()
             f = b.f[b.G:-b.G, b.G:-b.G].double().cpu().numpy()
@@ -249,4 +257,8 @@ class FusedSolver:
     def interior_f(self, solve: int = 0):
         return [self.blocks[bi].f[self.blocks[bi].G:-self.blocks[bi].G,
                                   self.blocks[bi].G:-self.blocks[bi].G].double().cpu().numpy()
-                for bi in self.solve_blocks[solve]]
+                for bi in self.solve_blocks[self.order[solve]]]
+
+    def solve_block_ids(self, solve: int):
+        """Indices in self.blocks of the blocks of the caller's solve."""
+        return self.solve_blocks[self.order[solve]]

@@ -27,12 +27,26 @@ def rel_err(a, b):
     return float(num / den) if den > 0 else float(num)
 
 
+def vec_err(ax, ay, bx, by):
+    """Error of a 2-vector field relative to its largest magnitude."""
+    den = max(float(np.max(np.abs(bx))), float(np.max(np.abs(by))))
+    num = max(float(np.max(np.abs(np.asarray(ax) - bx))), float(np.max(np.abs(np.asarray(ay) - by))))
+    return num / den if den > 0 else num
+
+
+def field_errors(x, y):
+    """Per-field errors: rho and T relative to their maxima, velocity (U, V)
+    and heat flux (qx, qy) relative to the largest vector magnitude."""
+    return {"rho": rel_err(x["rho"], y["rho"]), "T": rel_err(x["T"], y["T"]),
+            "UV": vec_err(x["U"], x["V"], y["U"], y["V"]),
+            "q": vec_err(x["qx"], x["qy"], y["qx"], y["qy"])}
+
+
 def fields_err(fa, fb):
-    """Worst rel_err over blocks and over rho, U, V, T, qx, qy."""
+    """Worst field error over blocks."""
     worst = 0.0
     for x, y in zip(fa, fb):
-        for k in ("rho", "U", "V", "T", "qx", "qy"):
-            worst = max(worst, rel_err(x[k], y[k]))
+        worst = max(worst, max(field_errors(x, y).values()))
     return worst
 
 

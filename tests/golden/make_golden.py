@@ -15,6 +15,11 @@ Cases:
   channel8     2-block adsorbing channel 8x8, Langmuir desorption     (f + coverage, 1/10/30)
   cavity32     the 32x32 cavity, 25x25 velocities on [-4,4]^2, vanLeer, Kn 0.075,
                CFL 0.8, lid 0.15 (fields at steps 1/10/100/1000)
+  cavity32_perturbed
+               the same case run by the reference a second time with f
+               multiplied by (1 + 1e-14 N(0,1)) after start-up (fields at
+               steps 100 and 1000): the scheme amplifies round-off after ~100
+               steps, and this run measures by how much
 """
 import os
 import sys
@@ -50,6 +55,29 @@ def record(sim, with_f):
     return out
 
 
+def perturbed_envelope(name, steps, amp=1e-14, seed=0):
+    """The reference against itself: the same case with f multiplied by
+    (1 + amp N(0,1)) after start-up.  The field differences at `steps` are
+    the round-off envelope of the reference scheme for this case."""
+    make = CASES[name][0]
+    a = host.OracleSim(make(), "ref", threads=os.cpu_count())
+    b = host.OracleSim(make(), "ref", threads=os.cpu_count())
+    rng = np.random.default_rng(seed)
+    for blk in b.blocks:
+        blk.f *= 1.0 + amp * rng.standard_normal(blk.f.shape)
+    out = {}
+    done = 0
+    for s in steps:
+        while done < s:
+            a.one_step()
+            b.one_step()
+            done += 1
+        for k, (x, y) in enumerate(zip(a.fields(), b.fields())):
+            for key in x:
+                out["s%d_b%d_%s" % (s, k, key)] = y[key]
+    return out
+
+
 def main(names=None):
     for name, (make, steps, with_f) in CASES.items():
         if names and name not in names:
@@ -65,6 +93,10 @@ def main(names=None):
                 data["s%d_%s" % (s, k)] = v
         path = os.path.join(HERE, name + ".npz")
         np.savez_compressed(path, **data)
+        print(path, os.path.getsize(path))
+    if not names or "cavity32_perturbed" in names:
+        path = os.path.join(HERE, "cavity32_perturbed.npz")
+        np.savez_compressed(path, **perturbed_envelope("cavity32", (100, 1000)))
         print(path, os.path.getsize(path))
 
 

@@ -33,8 +33,9 @@ class TeeProgram:
     """Runs each kernel on the oracle and on the GPU and records the worst
     relative difference of every buffer argument."""
 
-    def __init__(self, port, gpu, errors):
+    def __init__(self, port, gpu, errors, where=None):
         self.port, self.gpu, self.errors = port, gpu, errors
+        self.where = where if where is not None else {}
         self.cache = {}
 
     def _dev(self, a):
@@ -52,24 +53,35 @@ class TeeProgram:
             getattr(self.port, name)(gsize, *args)
             torch.cuda.synchronize()
             worst = 0.0
-            for a, d in zip(args, dev):
+            for ai, (a, d) in enumerate(zip(args, dev)):
                 if isinstance(a, np.ndarray):
                     g = d.cpu().numpy()
                     if name in BIT_EXACT:
-                        worst = max(worst, 0.0 if np.array_equal(g, a, equal_nan=True) else 1.0)
+                        e = 0.0 if np.array_equal(g, a, equal_nan=True) else 1.0
                     else:
                         fin = np.isfinite(a)
                         ga, aa = np.where(fin, g, 0), np.where(fin, a, 0)
                         floor = SCALE_FLOOR.get(name, 0.0)
+                        if name == "iFace":  # slopes: scale of f (round-off sized at equilibrium)
+                            floor = float(np.max(np.abs(args[0])))
                         den = max(float(np.max(np.abs(aa))), floor)
-                        num = float(np.max(np.abs(ga - aa)))
-                        worst = max(worst, num / den if den > 0 else num)
+                        diff = np.abs(ga - aa)
+                        num = float(np.max(diff))
+                        e = num / den if den > 0 else num
+                        if not np.all(np.isfinite(ga[fin])):
+                            e = np.inf
+                    if e > worst:
+                        worst = e
+                        if e > KERNEL_TOL:
+                            loc = np.unravel_index(np.argmax(np.where(np.isfinite(g - a), np.abs(g - a), np.inf)), a.shape)
+                            self.where[name] = (ai, tuple(int(x) for x in loc), float(a[loc]), float(g[loc]), gsize)
             self.errors[name] = max(self.errors.get(name, 0.0), worst)
         return call
 
 
 def tee_sim(case):
     errors = {}
+    where = {}
     sim = host.OracleSim.__new__(host.OracleSim)
     # build the oracle simulation with tee programs in place of the port
     import ugks_setup as us
@@ -87,7 +99,7 @@ def tee_sim(case):
         port = programs.PortProgram(sim.const, b, bid)
         desc = block_desc(pconst, b, tabs)
         sim._keep.append(desc)
-        tee = TeeProgram(port, KernelProgram(desc), errors)
+        tee = TeeProgram(port, KernelProgram(desc), errors, where)
         sim.blocks.append(host.OracleBlock(sim, bid, b, g, tee))
     sim.is_open = any(bc["type"] in (us.EXTRAPOLATE_OUT, us.INFLOW, us.OUTFLOW, us.CONSTANT)
                       for b in case["blocks"] for bc in b["bc"])
@@ -99,6 +111,7 @@ def tee_sim(case):
     sim.initial_mass_total = sum(sim.total_mass())
     sim.global_residual = None
     sim.flux_passes = 0
+    sim.where = where
     return sim, errors
 
 
@@ -118,7 +131,7 @@ def test_every_kernel_matches_oracle(cuda, name):
     assert errors, "no kernel ran"
     bad = {k: v for k, v in errors.items()
            if (v != 0.0 if k in BIT_EXACT else v > KERNEL_TOL)}
-    assert not bad, bad
+    assert not bad, (bad, sim.where)
 
 
 @pytest.mark.parametrize("name", ["cavity_vanleer", "multiblock_weno5", "channel_first_order"])

@@ -50,7 +50,7 @@ def test_channel_adsorbing_fp64(cuda):
     case = configs.channel(nblocks=2, n=8, m=8, k_des=0.01)
     ora, gpu = run_both(case, 20)
     assert fields_err(gpu.fields(), ora.fields()) < FP64_TOL
-    for bi, ob in zip(gpu.solve_blocks[0], ora.blocks):
+    for bi, ob in zip(gpu.solve_block_ids(0), ora.blocks):
         cov = gpu.blocks[bi].wall_cover.cpu().numpy()
         assert rel_err(cov[:8, 2, :], ob.wall_cover[:8, 2, :]) < FP64_TOL
 

@@ -6,7 +6,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import rel_err
+from conftest import field_errors, rel_err
 from pyugks_b200 import configs
 from pyugks_b200.fused import FusedSolver
 from pyugks_b200.ugks_sim import UGKSim
@@ -23,12 +23,34 @@ CASES = {
 }
 
 
-def check(g, s, fields, fs, dt, time):
+# The 32x32 cavity amplifies round-off after ~100 steps in the reference
+# scheme itself: tests/golden/cavity32_perturbed.npz holds the reference run
+# again with f perturbed by 1e-14 relative, and its distance from the golden
+# run is the envelope that any non-bit-identical implementation must stay in.
+ENVELOPE = {"cavity32": ("cavity32_perturbed", 100)}
+
+
+def envelope(name, s, k, gold_fields):
+    pert_name, strict_until = ENVELOPE.get(name, (None, None))
+    if pert_name is None or s <= strict_until:
+        return None
+    p = np.load(os.path.join(GOLDEN, pert_name + ".npz"))
+    pert = {key: p["s%d_b%d_%s" % (s, k, key)] for key in gold_fields}
+    return field_errors(pert, gold_fields)
+
+
+def check(g, s, fields, fs, dt, time, name=None):
     assert abs(dt - float(g["s%d_dt" % s])) <= 1e-12 * dt
     assert abs(time - float(g["s%d_time" % s])) <= 1e-12 * time
     for k, fl in enumerate(fields):
-        for key, arr in fl.items():
-            assert rel_err(arr, g["s%d_b%d_%s" % (s, k, key)]) < TOL, (s, k, key)
+        gold = {key: g["s%d_b%d_%s" % (s, k, key)] for key in fl}
+        errs = field_errors(fl, gold)
+        env = envelope(name, s, k, gold)
+        if env is None:
+            assert max(errs.values()) < TOL, (s, k, errs)
+        else:
+            for key, e in errs.items():
+                assert e <= max(TOL, 10.0 * env[key]), (s, k, key, e, env[key])
     if fs is not None and ("s%d_b0_f" % s) in g:
         for k, f in enumerate(fs):
             assert rel_err(f, g["s%d_b%d_f" % (s, k)]) < TOL
@@ -45,7 +67,7 @@ def test_fused_fp64_matches_golden(cuda, name):
         done = s
         st = gpu.solve_state()[0]
         assert st["status"] == 0
-        check(g, s, gpu.fields(), gpu.interior_f(), st["dt"], st["time"])
+        check(g, s, gpu.fields(), gpu.interior_f(), st["dt"], st["time"], name)
 
 
 @pytest.mark.parametrize("name", ["cavity8", "multiblock8", "channel8"])

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import host
-from conftest import rel_err
+from conftest import field_errors, rel_err
 from pyugks_b200 import configs
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
@@ -36,8 +36,9 @@ def test_port_matches_reference_golden(name):
         assert abs(sim.dt - float(g["s%d_dt" % s])) == 0.0
         assert abs(sim.time - float(g["s%d_time" % s])) <= 1e-15 * sim.time
         for k, fl in enumerate(sim.fields()):
-            for key, arr in fl.items():
-                assert rel_err(arr, g["s%d_b%d_%s" % (s, k, key)]) <= TOL, (name, s, k, key)
+            gold = {key: g["s%d_b%d_%s" % (s, k, key)] for key in fl}
+            errs = field_errors(fl, gold)
+            assert max(errs.values()) <= TOL, (name, s, k, errs)
         key = "s%d_b0_f" % s
         if key in g:
             for k, f in enumerate(sim.interior_f()):
