@@ -309,6 +309,34 @@ int ugks_step_profiled(int mixed, const ugks_fused_block *blocks_dev, int nblock
 int ugks_residual(const ugks_fused_block *blocks_dev, int nblocks, ugks_solve_state *solves_dev,
                   int nsolves, UGKS_STREAM);
 
+/* ------------------------------------------------------------------------
+ * 3. Time-step frequency without device allocation.  No counterpart in the
+ *    reference.  For callers that cannot allocate device memory (a host
+ *    runtime that forbids cudaMalloc while it drives the solver, or one that
+ *    runs from a fixed memory plan): the same maximum CFL frequency that
+ *    ugks_clFindDT followed by ugks_array_max yields (the quantity
+ *    UGKSBlock.getDT turns into max_dt = CFL / max_freq), with the per-cell
+ *    frequencies kept in a static array inside the library instead of a
+ *    caller buffer.  The caller passes the inputs and max_freq (one double,
+ *    device memory) only.
+ *
+ *    - At most UGKS_NOALLOC_MAX_CELLS interior cells (ni * nj) per call;
+ *      larger blocks return UGKS_ERR_TOO_LARGE without launching anything.
+ *    - The array (8 MiB) is held on every GPU that loads the library until
+ *      the process exits.
+ *    - The first call on a device looks up the array's device address
+ *      (cudaGetSymbolAddress) with that device current; make that first call
+ *      before any stream capture.
+ *    - All calls share the array and it keeps the last call's contents:
+ *      calls that overlap on the GPU (different streams, no ordering) race.
+ *    Returns 0, UGKS_ERR_TOO_LARGE, UGKS_ERR_BAD_SIZE or a negative cudaError_t.
+ * --------------------------------------------------------------------- */
+#define UGKS_NOALLOC_MAX_CELLS (1 << 20)
+#define UGKS_ERR_TOO_LARGE (-10001)
+#define UGKS_ERR_BAD_SIZE (-10002)
+int ugks_getDT_noalloc(const ugks_block_desc *d, const double *xy, const double *area,
+                       const double *macro, double Kn, double *max_freq, UGKS_STREAM);
+
 /* Library identification: returns a static version string. */
 const char *ugks_version(void);
 /* sizeof(ugks_block_desc), sizeof(ugks_fused_block), sizeof(ugks_solve_state),

@@ -80,6 +80,11 @@ KERNEL_SIGNATURES = {
 }
 _CT = {"p": vp, "i": C.c_int, "d": f64}
 
+# ugks_getDT_noalloc limits and error codes (include/ugks_b200.h)
+NOALLOC_MAX_CELLS = 1 << 20
+ERR_TOO_LARGE = -10001
+ERR_BAD_SIZE = -10002
+
 _LIB = None
 
 
@@ -113,6 +118,8 @@ def lib():
     L.ugks_step_profiled.argtypes = [C.c_int, vp, C.c_int, C.POINTER(FusedSizes), vp, C.c_int, vp, vp]
     L.ugks_residual.restype = C.c_int
     L.ugks_residual.argtypes = [vp, C.c_int, vp, C.c_int, vp]
+    L.ugks_getDT_noalloc.restype = C.c_int
+    L.ugks_getDT_noalloc.argtypes = [C.POINTER(BlockDesc), vp, vp, vp, f64, vp, vp]
     L.ugks_version.restype = C.c_char_p
     L.ugks_abi_sizes.restype = C.c_int
     L.ugks_abi_sizes.argtypes = [C.POINTER(C.c_int64), C.c_int]
