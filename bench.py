@@ -56,7 +56,7 @@ def workload(name: str):
     if name == "multiblock":
         case = configs.cavity_multiblock(nb=2, n=64, m=32, vlim=5.0, flux_method="WENO5", Kn=0.01)
         desc = ("lid-driven cavity 128x128 as 2x2 blocks of 64x64 cells, 33x33 velocities on "
-                "[-5,5]^2 (Nv=1089), WENO5, Kn 0.01, CFL 0.8")
+                "[-5,5]^2 (Nv=1089), WENO5, Kn 0.01, CFL 0.3")
         return [case], desc
     if name == "cavity":
         case = configs.cavity(n=32, m=24, vlim=4.0)
@@ -236,16 +236,10 @@ def run_ours(args, rank, world, dist):
             raise RuntimeError("solver status %s" % [s["status"] for s in state])
         # ---- end to end through the public call with host buffers
         e2e = run_e2e(solver, args, stream, dev, units)
-    t_max = ms
-    if dist is not None:
-        t = torch.tensor([ms, e2e["ms"]], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max, e2e_ms = float(t[0]), float(t[1])
-    else:
-        e2e_ms = e2e["ms"]
+    t_max, e2e_ms = max_over_ranks([ms, e2e["ms"]], dist, dev)
     if rank != 0:
         return
-    value = world * units * args.steps / (t_max / 1e3)
+    value = job_throughput(units, args.steps, world, t_max)
     kernels = {"face_pass": statistics.mean(face), "cell_pass": statistics.mean(cell),
                "ghost_pass": statistics.mean(ghost), "retry_face_pass": statistics.mean(retry)}
     dom = max(("face_pass", "cell_pass"), key=lambda k: kernels[k])
@@ -266,7 +260,7 @@ def run_ours(args, rank, world, dist):
                      "traffic": read_traffic(dom, args.workload, args.precision),
                      "bytes_per_unit": bpu, "kernel_ms": kernels,
                      "step_frac": bpu * units / (t_max / args.steps / 1e3) / 1e9 / peak},
-        "e2e": {"value": world * units * args.steps / (e2e_ms / 1e3), "unit": UNIT,
+        "e2e": {"value": job_throughput(units, args.steps, world, e2e_ms), "unit": UNIT,
                 "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
         "gpu_launches": 7 * args.steps,
         "clocks": clocks,
@@ -278,6 +272,23 @@ def run_ours(args, rank, world, dist):
                                 "sample": "%d full steps of the workload (time budget %.0f s) after 1 warm-up"
                                           % (done, budget)}
     print(json.dumps(line), flush=True)
+
+
+def max_over_ranks(values, dist, device=None):
+    """Max over all ranks of a few local timings (each rank times its own
+    replica; the job's time is the slowest rank's)."""
+    if dist is None:
+        return list(values)
+    import torch
+    t = torch.tensor(values, dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
+def job_throughput(units_per_step, steps, world, t_max_ms):
+    """Whole-job cell-velocity updates per second: every rank advances its own
+    replica of the workload by `steps` steps in at most t_max_ms."""
+    return world * units_per_step * steps / (t_max_ms / 1e3)
 
 
 def solver_bytes(solver):
@@ -312,6 +323,37 @@ def run_e2e(solver, args, stream, dev, units):
     return {"ms": t0.elapsed_time(t1), "h2d": h2d // args.steps, "d2h": d2h // args.steps}
 
 
+def run_serving(args):
+    """Config-5 style stream on one GPU: Poisson arrivals (rate 20/s, seed 2)
+    for --arrival-seconds, 70% cavities / 30% adsorbing channels with the
+    config-5 size distributions, each solve run to density residual < 1e-6 or
+    --max-steps, admission by HBM footprint against 150 GB."""
+    import torch
+    from pyugks_b200.serving import Server, request_stream
+    if args.impl == "reference":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "the reference has no serving loop; its CPU step is timed by the default workload"}))
+        return
+    reqs = request_stream(seed=2, rate=20.0, duration=args.arrival_seconds, max_steps=args.max_steps,
+                          tol=1e-6)
+    server = Server(budget_bytes=150e9, precision=args.precision, steps_per_tick=25)
+    done = server.run(reqs)
+    lat = np.array([r.finished - r.arrival for r in done])
+    line = {
+        "metric": METRIC, "value": server.units / server.wall, "unit": UNIT, "n_gpus": 1,
+        "steps": None, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "serving stream: %d requests over %.1f s (Poisson 20/s, seed 2), "
+                               "max %d steps or residual < 1e-6" % (len(reqs), args.arrival_seconds,
+                                                                     args.max_steps),
+                   "precision": args.precision},
+        "latency": {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                    "completed": len(done), "converged": sum(r.reason == "converged" for r in done),
+                    "wall_s": server.wall},
+    }
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -319,7 +361,11 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--workload", default="multiblock", choices=["multiblock", "cavity", "channel", "batched"])
+    ap.add_argument("--workload", default="multiblock",
+                    choices=["multiblock", "cavity", "channel", "batched", "serving"])
+    ap.add_argument("--arrival-seconds", type=float, default=3.0,
+                    help="serving: length of the Poisson arrival window (rate 20/s)")
+    ap.add_argument("--max-steps", type=int, default=400, help="serving: step limit per solve")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
@@ -336,7 +382,10 @@ def main():
         tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
         dist = tdist
     try:
-        if args.impl == "reference":
+        if args.workload == "serving":
+            if rank == 0:
+                run_serving(args)
+        elif args.impl == "reference":
             run_reference(args, rank, world)
         else:
             run_ours(args, rank, world, dist)

@@ -1,0 +1,277 @@
+"""Continuous batching of independent UGKS solves on one GPU.
+
+``SolvePool`` keeps every admitted solve resident in HBM (f, face fluxes,
+macro, walls) and advances all of them together with the fused step
+(``ugks_step_*``), one launch per phase for the whole pool.  Membership changes
+between launches:
+
+* ``admit(case)`` allocates the new solve's arrays, initialises it on a block
+  table of its own (``ugks_init_*``), then rebuilds the shared table;
+* ``retire(id)`` drops a solve and rebuilds the table;
+* solves already in flight are untouched by either (their arrays stay where
+  they are and their solve records are carried over), so a solve's result is
+  the same alone and in any mix.
+
+``Server`` runs a request stream against a pool: requests are admitted in
+arrival order while their HBM footprint fits the budget; every tick advances
+the pool by a fixed number of steps; after a tick the reference residual
+(``ugks_block.py:1303-1327``) of every solve is computed on the device and a
+solve leaves when its density residual is below the tolerance or it reached
+its step limit.  Time-to-converged is measured from arrival to retirement.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import heapq
+import time
+
+import numpy as np
+
+from . import _lib
+from . import defs as D
+from .fused import FusedSolver
+
+
+def footprint_bytes(case: dict, precision: str) -> int:
+    """HBM bytes a solve keeps resident: f and the two face-flux arrays, plus
+    the per-cell and per-face FP64 arrays."""
+    from .problem import VelocityGrid
+    q = case["quad"]
+    nv = VelocityGrid(q).Nv
+    G = 3 if case["flux_method"] == "WENO5" else 2
+    es = 8 if precision == "fp64" else 4
+    total = 0
+    for b in case["blocks"]:
+        Ni, Nj = b["ni"] + 2 * G, b["nj"] + 2 * G
+        total += 3 * Ni * Nj * nv * 2 * es
+        total += Ni * Nj * 8 * (4 * 2 + 2 + 2 * 2 + 1 + 2 + 2 * 2 + 2)
+        total += max(b["ni"], b["nj"]) * 4 * 8 * (4 + 4 + 8) + max(b["ni"], b["nj"]) * nv * 16
+    return total
+
+
+class _Solve:
+    def __init__(self, sid, case, solver):
+        self.id = sid
+        self.case = case
+        self.solver = solver          # its own FusedSolver (arrays + one-solve table)
+        self.cells = sum(b["ni"] * b["nj"] for b in case["blocks"])
+        self.nv = solver.blocks[0].Nv
+        self.record = None            # latest ugks_solve_state (bytes) while in the pool
+
+
+class SolvePool:
+    def __init__(self, precision="fp64", device="cuda"):
+        import torch
+        self.precision = precision
+        self.device = torch.device(device)
+        self.lib = _lib.lib()
+        self.solves = {}              # id -> _Solve, admission order
+        self._next = 0
+        self._table = None
+        self._states = None
+        self._sizes = None
+        self._order = []
+        self._dirty = True
+        self._step_fn = self.lib.ugks_step_fp64 if precision == "fp64" else self.lib.ugks_step_mixed
+
+    # -------------------------------------------------------------- membership
+    def admit(self, case) -> int:
+        """Allocate and initialise a solve; returns its id."""
+        solver = FusedSolver(case, precision=self.precision, device=self.device)
+        sid = self._next
+        self._next += 1
+        s = _Solve(sid, case, solver)
+        s.record = solver.solves.clone()
+        self.solves[sid] = s
+        self._dirty = True
+        return sid
+
+    def retire(self, sid):
+        self._sync_records()
+        s = self.solves.pop(sid)
+        self._dirty = True
+        return s
+
+    def _sync_records(self):
+        """Copy each solve's state record out of the shared array."""
+        if self._states is None or not self._order:
+            return
+        sz = C.sizeof(_lib.SolveState)
+        for k, sid in enumerate(self._order):
+            if sid in self.solves:
+                self.solves[sid].record = self._states[k * sz:(k + 1) * sz].clone()
+
+    def _rebuild(self):
+        import torch
+        self._sync_records()
+        # group by limiter, then admission order (ugks_fused_layout's rule)
+        order = sorted(self.solves, key=lambda sid: (D.FLUX_METHODS[self.solves[sid].case["flux_method"]], sid))
+        structs, records = [], []
+        for k, sid in enumerate(order):
+            s = self.solves[sid]
+            first = len(structs)
+            for blk in s.solver.blocks:
+                x = _lib.FusedBlock.from_buffer_copy(bytes(blk.struct))
+                x.solve = k
+                for f in range(4):
+                    if blk.bc[f]["type"] == D.ADJACENT:
+                        x.bc_block[f] = first + blk.bc[f]["other_block"]
+                structs.append(x)
+            rec = _lib.SolveState.from_buffer_copy(s.record.cpu().numpy().tobytes())
+            rec.first_block = first
+            rec.nblocks = len(s.solver.blocks)
+            records.append(rec)
+        self._order = order
+        if not structs:
+            self._table = self._states = None
+            self._dirty = False
+            return
+        arr = (_lib.FusedBlock * len(structs))(*structs)
+        self._sizes = _lib.FusedSizes()
+        rc = self.lib.ugks_fused_layout(arr, len(structs), C.byref(self._sizes))
+        if rc != 0:
+            raise RuntimeError("ugks_fused_layout: %d" % rc)
+        self._nblocks = len(structs)
+        self._table = torch.from_numpy(np.frombuffer(bytes(arr), dtype=np.uint8).copy()).to(self.device)
+        st = (_lib.SolveState * len(records))(*records)
+        self._states = torch.from_numpy(np.frombuffer(bytes(st), dtype=np.uint8).copy()).to(self.device)
+        self._dirty = False
+
+    # -------------------------------------------------------------- stepping
+    def step(self, n=1):
+        import torch
+        if self._dirty:
+            self._rebuild()
+        if self._table is None:
+            return
+        stream = torch.cuda.current_stream(self.device).cuda_stream
+        for _ in range(n):
+            _lib.check(self._step_fn(self._table.data_ptr(), self._nblocks, C.byref(self._sizes),
+                                     self._states.data_ptr(), len(self._order), stream), "ugks_step")
+
+    def states(self):
+        """{id: solve record dict} with the residual of the last step."""
+        import torch
+        if self._dirty:
+            self._rebuild()
+        if self._table is None:
+            return {}
+        _lib.check(self.lib.ugks_residual(self._table.data_ptr(), self._nblocks, self._states.data_ptr(),
+                                          len(self._order), torch.cuda.current_stream(self.device).cuda_stream),
+                   "ugks_residual")
+        arr = (_lib.SolveState * len(self._order)).from_buffer_copy(self._states.cpu().numpy().tobytes())
+        return {sid: dict(dt=x.dt, time=x.time, steps=x.steps, status=x.status, residual=list(x.residual))
+                for sid, x in zip(self._order, arr)}
+
+    def fields(self, sid):
+        return self.solves[sid].solver.fields(0)
+
+    def interior_f(self, sid):
+        return self.solves[sid].solver.interior_f(0)
+
+    def units_per_step(self):
+        return sum(s.cells * s.nv for s in self.solves.values())
+
+
+class Request:
+    def __init__(self, rid, arrival, case, max_steps, tol):
+        self.id, self.arrival, self.case = rid, arrival, case
+        self.max_steps, self.tol = max_steps, tol
+        self.admitted = self.finished = None
+        self.steps = 0
+        self.reason = None
+
+
+class Server:
+    def __init__(self, budget_bytes=150e9, precision="mixed", steps_per_tick=50, device="cuda"):
+        self.pool = SolvePool(precision, device)
+        self.budget = budget_bytes
+        self.precision = precision
+        self.steps_per_tick = steps_per_tick
+        self.used = 0
+        self.done = []
+        self.units = 0
+
+    def run(self, requests, time_limit=None):
+        """Serve a list of Request (arrival in seconds from the start).
+        Returns the completed requests."""
+        import torch
+        queue = sorted(requests, key=lambda r: r.arrival)
+        waiting = []
+        active = {}
+        t0 = time.perf_counter()
+        i = 0
+        while i < len(queue) or waiting or active:
+            now = time.perf_counter() - t0
+            if time_limit is not None and now > time_limit:
+                break
+            while i < len(queue) and queue[i].arrival <= now:
+                waiting.append(queue[i])
+                i += 1
+            # admit in arrival order while the footprint fits
+            while waiting:
+                r = waiting[0]
+                need = footprint_bytes(r.case, self.precision)
+                if self.used + need > self.budget and active:
+                    break
+                waiting.pop(0)
+                sid = self.pool.admit(r.case)
+                r.admitted, r.need, r.sid = time.perf_counter() - t0, need, sid
+                self.used += need
+                active[sid] = r
+            if not active:
+                if i < len(queue):
+                    time.sleep(max(0.0, min(queue[i].arrival - now, 0.05)))
+                continue
+            units = self.pool.units_per_step()
+            self.pool.step(self.steps_per_tick)
+            self.units += units * self.steps_per_tick
+            states = self.pool.states()   # synchronises
+            now = time.perf_counter() - t0
+            for sid, st in states.items():
+                r = active[sid]
+                r.steps = st["steps"]
+                reason = None
+                if st["status"] != 0:
+                    reason = "error"
+                elif st["residual"][0] < r.tol:
+                    reason = "converged"
+                elif st["steps"] >= r.max_steps:
+                    reason = "max_steps"
+                if reason:
+                    r.finished, r.reason = now, reason
+                    self.pool.retire(sid)
+                    self.used -= r.need
+                    del active[sid]
+                    self.done.append(r)
+        self.wall = time.perf_counter() - t0
+        return self.done
+
+
+def request_stream(seed=2, rate=20.0, duration=600.0, max_steps=20000, tol=1e-6):
+    """Poisson arrivals of cavity (p = 0.7, the batched-cavity distributions)
+    and adsorbing-channel solves (p = 0.3: 64k x 16k cells, k in {1,2,4},
+    m in {16,24,32}, Kn log-uniform on [0.01, 0.5])."""
+    from . import configs
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t > duration:
+            break
+        if rng.random() < 0.7:
+            n = int(rng.choice(configs.CAVITY_SIZES))
+            m = int(rng.choice(configs.CAVITY_VGRIDS))
+            Kn = float(10 ** rng.uniform(np.log10(0.005), 0.0))
+            lid = float(rng.uniform(0.05, 0.3))
+            Tw = float(rng.uniform(0.8, 1.2))
+            scheme = "WENO5" if rng.random() < 0.5 else "vanLeer"
+            case = configs.cavity(n=n, m=m, vlim=5.0, flux_method=scheme, Kn=Kn, lid=lid, T_wall=Tw,
+                                  CFL=0.3)
+        else:
+            k = int(rng.choice([1, 2, 4]))
+            m = int(rng.choice([16, 24, 32]))
+            Kn = float(10 ** rng.uniform(np.log10(0.01), np.log10(0.5)))
+            case = configs.channel(nblocks=4, n=16 * k, nj=16 * k, m=m, Kn=Kn)
+        out.append(Request(len(out), t, case, max_steps, tol))
+    return out

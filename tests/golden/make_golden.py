@@ -11,8 +11,10 @@ small cases -- as compressed .npz files:
 
 Cases:
   cavity8      8x8 cavity, 9x9 velocities on [-4,4]^2, vanLeer        (f, steps 1/10/50)
-  multiblock8  2x2 blocks of 8x8, 9x9 velocities on [-5,5]^2, WENO5   (f, steps 1/10/30)
-  channel8     2-block adsorbing channel 8x8, Langmuir desorption     (f + coverage, 1/10/30)
+  multiblock8  2x2 blocks of 8x8, 9x9 velocities on [-5,5]^2, WENO5, CFL 0.3
+               (f, steps 1/10/30)
+  channel8     2-block adsorbing channel 8x8, Langmuir desorption, CFL 0.3
+               (f + coverage, 1/10/30)
   cavity32     the 32x32 cavity, 25x25 velocities on [-4,4]^2, vanLeer, Kn 0.075,
                CFL 0.8, lid 0.15 (fields at steps 1/10/100/1000)
   cavity32_perturbed
