@@ -238,6 +238,10 @@ typedef struct ugks_fused_block {
   double *wall_cover;          /* [max(ni,nj)][4] x 4                       */
   double *wall_fluxes;         /* [max(ni,nj)][4] x 8                       */
   double *wall_dist;           /* [max(ni,nj)][Nv] x 2                      */
+  double *cell_mom;            /* [Ni][Nj] x 4: sum over v of f (1, u, v,
+                                  (u^2+v^2)/2 | 1/2) per cell, global frame;
+                                  written by the init, cell and ghost passes,
+                                  read by the face pass (getAL/getAR)       */
 } ugks_fused_block;
 
 typedef struct ugks_solve_state {

@@ -298,6 +298,8 @@ template <> struct Store<double> {
   __device__ __forceinline__ static void store(void *base, size_t k, V2 v) {
     reinterpret_cast<double2 *>(base)[k] = make_double2(v.x, v.y);
   }
+  // the value a store followed by a load gives back
+  __device__ __forceinline__ static V2 as_stored(V2 v) { return v; }
 };
 template <> struct Store<float> {
   using vec = float2;
@@ -307,6 +309,9 @@ template <> struct Store<float> {
   }
   __device__ __forceinline__ static void store(void *base, size_t k, V2 v) {
     reinterpret_cast<float2 *>(base)[k] = make_float2((float)v.x, (float)v.y);
+  }
+  __device__ __forceinline__ static V2 as_stored(V2 v) {
+    return v2((double)(float)v.x, (double)(float)v.y);
   }
 };
 

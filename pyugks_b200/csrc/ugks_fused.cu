@@ -73,44 +73,35 @@ struct FaceShared {
   double bcast[48];
 };
 
-// WENO5 slope (clFunctions.c:266-313) with the three nonlinear weights
-// normalised through one division: w_k = c_k / d_k / sum(c_j / d_j) =
-// c_k prod_{j!=k} d_j / sum_j c_j prod_{i!=j} d_i, d_k = (eps + beta_k)^2.
-__device__ __forceinline__ double weno5_slope(double S0, double S1, double S2, double S3,
-                                              double S4, double inv_dx) {
-  double t1 = S0 - 2.0 * S1 + S2, t2 = S0 - 4.0 * S1 + 3.0 * S2;
-  const double B0 = (13.0 / 12.0) * t1 * t1 + 0.25 * t2 * t2;
-  t1 = S1 - 2.0 * S2 + S3;
-  t2 = S1 - S3;
-  const double B1 = (13.0 / 12.0) * t1 * t1 + 0.25 * t2 * t2;
-  t1 = S2 - 2.0 * S3 + S4;
-  t2 = 3.0 * S2 - 4.0 * S3 + S4;
-  const double B2 = (13.0 / 12.0) * t1 * t1 + 0.25 * t2 * t2;
-  double d0 = 1e-16 + B0, d1 = 1e-16 + B1, d2 = 1e-16 + B2;
-  d0 *= d0;
-  d1 *= d1;
-  d2 *= d2;
-  const double a0 = 0.1 * (d1 * d2), a1 = 0.6 * (d0 * d2), a2 = 0.3 * (d0 * d1);
-  const double f0 = (1. / 3.) * S0 - (7. / 6.) * S1 + (11. / 6.) * S2;
-  const double f1 = -(1. / 6.) * S1 + (5. / 6.) * S2 + (1. / 3.) * S3;
-  const double f2 = (1. / 3.) * S2 + (5. / 6.) * S3 - (1. / 6.) * S4;
-  const double fL = (a0 * f0 + a1 * f1 + a2 * f2) * nr_rcp(a0 + a1 + a2);
-  return (fL - S2) * inv_dx;
+// WENO5 (clFunctions.c:266-313) of one component, up to the final division:
+// slope * dx = num / den.  Written in the first differences D_k = S_{k+1} - S_k:
+//   12 beta_k = 13 (D_{k+1} - D_k)^2 + 3 r_k^2,  r = (3 D1 - D0, D1 + D2, D3 - 3 D2)
+//   f_k - S2  = (-D0/3 + 5 D1/6, D1/6 + D2/3, 2 D2/3 - D3/6)
+// and the weights c_k / (eps + beta_k)^2 multiplied through by
+// prod_j (eps + beta_j)^2 / 0.1 (a common factor of num and den; eps scales
+// with beta).
+__device__ __forceinline__ void weno5_part(const double (&S)[5], double &num, double &den) {
+  const double D0 = S[1] - S[0], D1 = S[2] - S[1], D2 = S[3] - S[2], D3 = S[4] - S[3];
+  const double p0 = D1 - D0, p1 = D2 - D1, p2 = D3 - D2;
+  const double r0 = fma(3.0, D1, -D0), r1 = D1 + D2, r2 = fma(-3.0, D2, D3);
+  const double e0 = 12e-16 + fma(13.0 * p0, p0, (3.0 * r0) * r0);
+  const double e1 = 12e-16 + fma(13.0 * p1, p1, (3.0 * r1) * r1);
+  const double e2 = 12e-16 + fma(13.0 * p2, p2, (3.0 * r2) * r2);
+  const double q0 = e0 * e0, q1 = e1 * e1, q2 = e2 * e2;
+  const double a0 = q1 * q2, a1 = 6.0 * (q0 * q2), a2 = 3.0 * (q0 * q1);
+  const double f0 = fma(-1.0 / 3.0, D0, (5.0 / 6.0) * D1);
+  const double f1 = fma(1.0 / 6.0, D1, (1.0 / 3.0) * D2);
+  const double f2 = fma(2.0 / 3.0, D2, (-1.0 / 6.0) * D3);
+  num = fma(a0, f0, fma(a1, f1, a2 * f2));
+  den = (a0 + a1) + a2;
 }
 
-// vanLeer limiter (clFunctions.c:255-261) with a Newton-Raphson reciprocal
-__device__ __forceinline__ double vanleer_fast(double s1, double s2) {
-  const double a1 = fabs(s1), a2 = fabs(s2);
-  return (ocl_sign(s1) + ocl_sign(s2)) * (a1 * a2) * nr_rcp(a1 + a2 + 1e-16);
-}
-
-// iFace (clUGKS.c:148-194) for one velocity: face value and slope of (h, b),
-// plus the left / right cell values (stencil cells MID and MID+1).
+// iFace (clUGKS.c:148-194) for one velocity: face value and slope of (h, b).
+// The two components share one reciprocal: 1/x = y * 1/(x y).
 template <typename T, int FM>
 __device__ __forceinline__ void reconstruct(const void *f, size_t kv, long step, int delta,
                                             double inv_l, double ds, double inv_ds, double &fh,
-                                            double &fb, double &sh, double &sb, double &lh,
-                                            double &lb, double &rh, double &rb) {
+                                            double &fb, double &sh, double &sb) {
   constexpr int L = FM == 1 ? 5 : 3, MID = FM == 1 ? 2 : 1;
   double Sh[L], Sb[L];
 #pragma unroll
@@ -120,30 +111,36 @@ __device__ __forceinline__ void reconstruct(const void *f, size_t kv, long step,
     Sh[s] = x.x;
     Sb[s] = x.y;
   }
-  if (FM == 0) {
-    sh = vanleer_fast((Sh[1] - Sh[0]) * inv_l, (Sh[2] - Sh[1]) * inv_l);
-    sb = vanleer_fast((Sb[1] - Sb[0]) * inv_l, (Sb[2] - Sb[1]) * inv_l);
-  } else if (FM == 1) {
-    sh = weno5_slope(Sh[0], Sh[1], Sh[2], Sh[3], Sh[4], inv_ds);
-    sb = weno5_slope(Sb[0], Sb[1], Sb[2], Sb[3], Sb[4], inv_ds);
+  if constexpr (FM == 0) {
+    // vanLeer (clFunctions.c:255-261)
+    const double h1 = (Sh[1] - Sh[0]) * inv_l, h2 = (Sh[2] - Sh[1]) * inv_l;
+    const double b1 = (Sb[1] - Sb[0]) * inv_l, b2 = (Sb[2] - Sb[1]) * inv_l;
+    const double dh = fabs(h1) + fabs(h2) + 1e-16, db = fabs(b1) + fabs(b2) + 1e-16;
+    const double r = nr_rcp(dh * db);
+    sh = (ocl_sign(h1) + ocl_sign(h2)) * (fabs(h1) * fabs(h2)) * (db * r);
+    sb = (ocl_sign(b1) + ocl_sign(b2)) * (fabs(b1) * fabs(b2)) * (dh * r);
+  } else if constexpr (FM == 1) {
+    double nh, dh, nb, db;
+    weno5_part(Sh, nh, dh);
+    weno5_part(Sb, nb, db);
+    const double r = nr_rcp(dh * db) * inv_ds;
+    sh = nh * (db * r);
+    sb = nb * (dh * r);
   } else {
     sh = (0.5 * minmod(Sh[2] - Sh[1], Sh[1] - Sh[0])) * inv_ds;
     sb = (0.5 * minmod(Sb[2] - Sb[1], Sb[1] - Sb[0])) * inv_ds;
   }
   fh = Sh[MID] + sh * ds;
   fb = Sb[MID] + sb * ds;
-  lh = delta ? Sh[MID] : Sh[MID + 1];
-  lb = delta ? Sb[MID] : Sb[MID + 1];
-  rh = delta ? Sh[MID + 1] : Sh[MID];
-  rb = delta ? Sb[MID + 1] : Sb[MID];
 }
 
-// exp(-lambda (x - c)^2) over the nodes of one velocity axis
+// scale * exp(-lambda (x - c)^2) over the nodes of one velocity axis
 __device__ __forceinline__ void axis_exp(double *out, const double *quad, int n, int stride,
-                                         int comp, double c, double lambda, int t, int nt) {
+                                         int comp, double c, double lambda, int t, int nt,
+                                         double scale = 1.0) {
   for (int i = t; i < n; i += nt) {
     const double x = quad[2 * (size_t)i * stride + comp] - c;
-    out[i] = exp(-lambda * (x * x));
+    out[i] = scale * exp(-lambda * (x * x));
   }
 }
 
@@ -184,7 +181,8 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     else if (mi == d.ni && is_wall(blk.bc_type[GEAST])) wall = GEAST;
   }
 
-  double *fh = dyn, *fb = dyn + Nv, *sgh = dyn + 2 * Nv, *sgb = dyn + 3 * Nv;
+  // per velocity: (h, b) at the face and their slopes, kept for the later sweeps
+  double2 *fhb = reinterpret_cast<double2 *>(dyn), *sgb = fhb + Nv;
   const V2 n = ld2(blk.normal, faceidx(d, gi, gj, dir));
   const V2 mid = ld2(blk.mid_side, faceidx(d, gi, gj, dir));
   // stencil geometry for both upwind directions (iFace, clUGKS.c:148-176)
@@ -202,51 +200,55 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
   const long step = dir == SOUTH ? (long)Nv : (long)d.Nj * Nv;
   const size_t base = fidx(d, gi, gj, 0);
 
-  // ---- sweep 1: reconstruction (+ interior faces: moments W, WL, WR)
-  double m[12];
-#pragma unroll
-  for (int k = 0; k < 12; ++k) m[k] = 0.0;
+  // ---- sweep 1: reconstruction (+ interior faces: the face moments W of
+  // getFaceCons; the 1/2 of the energy moment is applied after the sum)
+  double m[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll 2
   for (int v = threadIdx.x; v < Nv; v += FT) {
     const V2 uv = face_velocity(d, v, n);
     const int delta = uv.x > 0.0 ? 1 : 0;
-    double ffh, ffb, sx, sy, lh, lb, rh, rb;
+    double ffh, ffb, sx, sy;
     reconstruct<T, FM>(blk.f, base + v, step, delta, inv_l1[delta], dist[delta], inv_dist[delta],
-                       ffh, ffb, sx, sy, lh, lb, rh, rb);
-    fh[v] = ffh;
-    fb[v] = ffb;
-    sgh[v] = sx;
-    sgb[v] = sy;
+                       ffh, ffb, sx, sy);
+    fhb[v] = make_double2(ffh, ffb);
+    sgb[v] = make_double2(sx, sy);
     if (wall < 0) {
-      const double uu = uv.x * uv.x + uv.y * uv.y;
-      m[0] += ffh; m[1] += uv.x * ffh; m[2] += uv.y * ffh; m[3] += 0.5 * (uu * ffh + ffb);
-      m[4] += lh; m[5] += uv.x * lh; m[6] += uv.y * lh; m[7] += 0.5 * (uu * lh + lb);
-      m[8] += rh; m[9] += uv.x * rh; m[10] += uv.y * rh; m[11] += 0.5 * (uu * rh + rb);
+      const double uu = fma(uv.x, uv.x, uv.y * uv.y);
+      m[0] += ffh;
+      m[1] = fma(uv.x, ffh, m[1]);
+      m[2] = fma(uv.y, ffh, m[2]);
+      m[3] += fma(uu, ffh, ffb);
     }
   }
   const double len = blk.side_length[faceidx(d, gi, gj, dir)];
 
   if (wall < 0) {
     // ---------------- interior face ----------------
-    block_sum<12>(m, sh.scratch);
-    const P4 W = p4(m[0], m[1], m[2], m[3]);
+    block_sum<4>(m, sh.scratch);
+    const P4 W = p4(m[0], m[1], m[2], 0.5 * m[3]);
     const P4 prim = to_primary(d, W);  // getPLR (clUGKS.c:421-422), every thread
     const int un = d.u_num, vn = d.v_num;
     const bool sep = un > 0 && un * vn == Nv && un + vn <= 512;
     double *Eu = dyn + 4 * Nv, *Ev = Eu + (sep ? un : 0);
     const V2 Ug = to_global(v2(prim.s1, prim.s2), n);  // face mean velocity, global frame
+    // Maxwellian prefactor rho lambda / pi (fM, clFunctions.c:49-58), times the
+    // face length: every per-velocity flux below carries the length
+    const double chl = (prim.s0 * (prim.s3 / d.PI)) * len;
     double q[2] = {0.0, 0.0};
     if (threadIdx.x < 32) {
       if (threadIdx.x == 0) {
-        // getPLR slopes (clUGKS.c:424-436) and initMacroFlux (446-518)
-        const V2 cl = ld2(blk.centre, gidx(d, gi - dir, gj - (1 - dir)));
-        const V2 cr = ld2(blk.centre, gidx(d, gi, gj));
+        // getPLR slopes (clUGKS.c:424-436) from the cell moments of the two
+        // cells beside the face (getAL / getAR), and initMacroFlux (446-518)
+        const size_t kl = gidx(d, gi - dir, gj - (1 - dir)), kr = gidx(d, gi, gj);
+        const P4 ml = ld4(blk.cell_mom, kl), mr = ld4(blk.cell_mom, kr);
+        const V2 ul = to_local(v2(ml.s1, ml.s2), n), ur = to_local(v2(mr.s1, mr.s2), n);
+        const V2 cl = ld2(blk.centre, kl), cr = ld2(blk.centre, kr);
         const double idl = 1.0 / sqrt((mid.x - cl.x) * (mid.x - cl.x) + (mid.y - cl.y) * (mid.y - cl.y));
         const double idr = 1.0 / sqrt((mid.x - cr.x) * (mid.x - cr.x) + (mid.y - cr.y) * (mid.y - cr.y));
-        const P4 aL = micro_slope(d, prim, p4((W.s0 - m[4]) * idl, (W.s1 - m[5]) * idl,
-                                              (W.s2 - m[6]) * idl, (W.s3 - m[7]) * idl));
-        const P4 aR = micro_slope(d, prim, p4((m[8] - W.s0) * idr, (m[9] - W.s1) * idr,
-                                              (m[10] - W.s2) * idr, (m[11] - W.s3) * idr));
+        const P4 aL = micro_slope(d, prim, p4((W.s0 - ml.s0) * idl, (W.s1 - ul.x) * idl,
+                                              (W.s2 - ul.y) * idl, (W.s3 - ml.s3) * idl));
+        const P4 aR = micro_slope(d, prim, p4((mr.s0 - W.s0) * idr, (ur.x - W.s1) * idr,
+                                              (ur.y - W.s2) * idr, (mr.s3 - W.s3) * idr));
         double Mu[MNUM], Mv[MTUM], Mxi[3], MuL[MNUM], MuR[MNUM], Mt[5];
         moments_u(d, prim, Mu, Mv, Mxi, MuL, MuR);
         const P4 aT = micro_slope(d, prim, scale(-prim.s0, add(moment_au(aL, MuL, Mv, Mxi, 1, 0),
@@ -257,13 +259,27 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
                                     scale(Mt[1], add(moment_au(aL, MuL, Mv, Mxi, 2, 0),
                                                      moment_au(aR, MuR, Mv, Mxi, 2, 0)))),
                                 scale(Mt[2], moment_au(aT, Mu, Mv, Mxi, 1, 0))));
+        // distFlux coefficients folded per face (derivation at sweep 3)
+        const double kb = d.K / (2.0 * prim.s3), xk = Mxi[2] - kb * kb;
         double *c = sh.bcast;
-        c[4] = aL.s0; c[5] = aL.s1; c[6] = aL.s2; c[7] = aL.s3;
-        c[8] = aR.s0; c[9] = aR.s1; c[10] = aR.s2; c[11] = aR.s3;
-        c[12] = aT.s0; c[13] = aT.s1; c[14] = aT.s2; c[15] = aT.s3;
-        c[16] = Mt[0]; c[17] = Mt[1]; c[18] = Mt[2]; c[19] = Mt[3]; c[20] = Mt[4];
-        c[21] = Mxi[2];
-        c[22] = g0.s0; c[23] = g0.s1; c[24] = g0.s2; c[25] = g0.s3;
+        const P4 as[2] = {aL, aR};
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          c[5 * k + 0] = Mt[1] * fma(0.5 * as[k].s3, kb, as[k].s0);
+          c[5 * k + 1] = Mt[1] * as[k].s1;
+          c[5 * k + 2] = Mt[1] * as[k].s2;
+          c[5 * k + 3] = Mt[1] * (0.5 * as[k].s3);
+          c[5 * k + 4] = Mt[1] * (0.5 * as[k].s3 * xk);
+        }
+        c[10] = Mt[2] * fma(0.5 * aT.s3, kb, aT.s0) + Mt[0];
+        c[11] = Mt[2] * aT.s1;
+        c[12] = Mt[2] * aT.s2;
+        c[13] = Mt[2] * (0.5 * aT.s3);
+        c[14] = Mt[2] * (0.5 * aT.s3 * xk);
+        c[15] = Mt[0];
+        c[16] = Mt[3] * len;
+        c[17] = Mt[4] * len;
+        c[18] = len * g0.s0; c[19] = len * g0.s1; c[20] = len * g0.s2; c[21] = len * g0.s3;
       }
     } else {
       // meanwhile: face heat flux (calcFaceQ, clUGKS.c:522-585) and the
@@ -273,35 +289,45 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
       for (int v = t; v < Nv; v += nt) {
         const V2 uv = face_velocity(d, v, n);
         const double cx = uv.x - prim.s1, cy = uv.y - prim.s2, c2 = cx * cx + cy * cy;
-        const double tq = c2 * fh[v] + fb[v] * Kinv;
+        const double2 fv = fhb[v];
+        const double tq = c2 * fv.x + fv.y * Kinv;
         q[0] += 0.5 * (cx * tq);
         q[1] += 0.5 * (cy * tq);
       }
       if (sep) {
-        axis_exp(Eu, d.quad, un, vn, 0, Ug.x, prim.s3, t, nt);
+        axis_exp(Eu, d.quad, un, vn, 0, Ug.x, prim.s3, t, nt, chl);
         axis_exp(Ev, d.quad, vn, 1, 1, Ug.y, prim.s3, t, nt);
       }
     }
     block_sum<2>(q, sh.scratch);
+    // ---- sweep 3: macroFlux (587-681) and distFlux (683-772).
+    // With h0 = weight * fM (times the face length), kb = K / (2 lambda),
+    // S = Mt0 s (c . Q) (the Shakhov factor of fS, clFunctions.c:64-77, times
+    // Mt0), P4 = 2 lambda c^2 - 4, the upwind slope a (aL for u > 0, else aR),
+    //   Ph = a0 + a1 u + a2 v + a3 (|u|^2 + kb) / 2, and Th likewise with aT,
+    //   Rh = Mt3 fh - Mt4 u sh,   Rb = Mt3 fb - Mt4 u sb,
+    //   Zh = u (S P4 h0 + Rh),    Zb = u (S (P4 + 2) kb h0 + Rb),
+    //   B  = Mt0 + Mt1 u Ph + Mt2 Th,
+    // distFlux's two components are
+    //   hx = Zh + u h0 B,
+    //   hy = Zb + u h0 (kb B + Mt1 u a3 X / 2 + Mt2 aT3 X / 2),  X = Mxi2 - kb^2,
+    // and macroFlux's discrete part sums (Zh, u Zh, v Zh, (|u|^2 Zh + Zb) / 2).
     const double *c = sh.bcast;
     const V2 Q = v2(q[0], q[1]);
-    const P4 aL = p4(c[4], c[5], c[6], c[7]), aR = p4(c[8], c[9], c[10], c[11]);
-    const P4 aT = p4(c[12], c[13], c[14], c[15]);
-    const double Mt0 = c[16], Mt1 = c[17], Mt2 = c[18], Mt3 = c[19], Mt4 = c[20], Mxi2 = c[21];
-    // per-face constants of the Maxwellian (fM, clFunctions.c:49-58) and the
-    // Shakhov factor (fS, clFunctions.c:64-77)
-    const double ch = prim.s0 * (prim.s3 / d.PI);
-    const double kb = d.K / (2.0 * prim.s3);
-    const double s0 = 0.8 * (1 - d.Pr) * (prim.s3 * prim.s3) / prim.s0;
-    // ---- sweep 3: macroFlux (587-681) and distFlux (683-772)
-    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    const double lam = prim.s3, Ux = prim.s1, Uy = prim.s2, lam2 = 2.0 * lam;
+    const double kb = d.K / (2.0 * lam);
+    const double s0 = 0.8 * (1 - d.Pr) * (lam * lam) / prim.s0;
+    const double Mt0 = c[15], Mt3 = c[16], Mt4 = c[17];
+    const double sx = (Mt0 * s0) * Q.x, sy = (Mt0 * s0) * Q.y;
+    const double T0 = c[10], T1 = c[11], T2 = c[12], T3 = c[13], CT = c[14];
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     void *flux = dir == SOUTH ? blk.flux_S : blk.flux_W;
     const int qs = sep ? FT / vn : 0, rs = sep ? FT % vn : 0;
     int iu = sep ? threadIdx.x / vn : 0, jv = sep ? threadIdx.x % vn : 0;
     for (int v = threadIdx.x; v < Nv; v += FT) {
       const V2 uv = face_velocity(d, v, n);
-      const double u = uv.x, vt = uv.y, uu = u * u + vt * vt;
-      const double cx = u - prim.s1, cy = vt - prim.s2;
+      const double u = uv.x, vt = uv.y, uu = fma(u, u, vt * vt);
+      const double cx = u - Ux, cy = vt - Uy, c2 = fma(cx, cx, cy * cy);
       double E;
       if (sep) {
         E = Eu[iu] * Ev[jv];
@@ -309,41 +335,41 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
         iu += qs;
         if (jv >= vn) { jv -= vn; ++iu; }
       } else {
-        E = exp(-prim.s3 * (cx * cx + cy * cy));
+        E = chl * exp(-lam * c2);
       }
-      const double h0 = d.weight[v] * ch * E, b0 = h0 * kb;
-      const double S = s0 * (cx * Q.x + cy * Q.y), part = 2 * prim.s3 * (cx * cx + cy * cy);
-      const double F0h = (S * (part - 4)) * h0, F0b = (S * (part - 2)) * b0;
-      const double fdh = fh[v], fdb = fb[v], fsh = sgh[v], fsb = sgb[v];
-      const double uu2 = u * u;
-      acc[0] += Mt0 * u * F0h + Mt3 * u * fdh - Mt4 * uu2 * fsh;
-      acc[1] += Mt0 * uu2 * F0h + Mt3 * uu2 * fdh - Mt4 * uu2 * u * fsh;
-      acc[2] += Mt0 * vt * u * F0h + Mt3 * vt * u * fdh - Mt4 * vt * uu2 * fsh;
-      acc[3] += Mt0 * 0.5 * (u * uu * F0h + u * F0b) + Mt3 * 0.5 * (u * uu * fdh + u * fdb) -
-                Mt4 * 0.5 * (uu2 * uu * fsh + uu2 * fsb);
-      const P4 a = u > 0.0 ? aL : aR;
-      const double pa = a.s0 + a.s1 * u + a.s2 * vt;
-      const double pt = aT.s0 + aT.s1 * u + aT.s2 * vt;
-      const double ph = h0 * (pa + 0.5 * a.s3 * (uu + kb));
-      const double pb = b0 * pa + 0.5 * a.s3 * (uu * b0 + Mxi2 * h0);
-      const double th = h0 * (pt + 0.5 * aT.s3 * (uu + kb));
-      const double tb = b0 * pt + 0.5 * aT.s3 * (uu * b0 + Mxi2 * h0);
-      const double hx = Mt0 * u * (h0 + F0h) + Mt1 * uu2 * ph + Mt2 * u * th + Mt3 * u * fdh - Mt4 * uu2 * fsh;
-      const double hy = Mt0 * u * (b0 + F0b) + Mt1 * uu2 * pb + Mt2 * u * tb + Mt3 * u * fdb - Mt4 * uu2 * fsb;
-      St::store(flux, base + v, v2(len * hx, len * hy));
+      const double h0 = d.weight[v] * E;
+      const double Sp = fma(cx, sx, cy * sy);
+      const double S4 = Sp * fma(lam2, c2, -4.0), S2 = fma(2.0, Sp, S4);
+      const double *A = c + (u > 0.0 ? 0 : 5);
+      const double MP = fma(A[3], uu, fma(A[2], vt, fma(A[1], u, A[0])));
+      const double Bk = fma(u, MP, fma(T3, uu, fma(T2, vt, fma(T1, u, T0))));
+      const double2 fd = fhb[v], fs = sgb[v];
+      const double mu = Mt4 * u;
+      const double Rh = fma(-mu, fs.x, Mt3 * fd.x), Rb = fma(-mu, fs.y, Mt3 * fd.y);
+      const double Zh = u * fma(S4, h0, Rh), Zb = u * fma(S2, h0 * kb, Rb);
+      const double uh = u * h0;
+      const double hx = fma(uh, Bk, Zh);
+      const double hy = fma(uh, fma(kb, Bk, fma(A[4], u, CT)), Zb);
+      acc[0] += Zh;
+      acc[1] = fma(u, Zh, acc[1]);
+      acc[2] = fma(vt, Zh, acc[2]);
+      acc[3] = fma(uu, Zh, acc[3]);
+      acc[4] += Zb;
+      St::store(flux, base + v, v2(hx, hy));
     }
-    block_sum<4>(acc, sh.scratch);
+    block_sum<5>(acc, sh.scratch);
     if (threadIdx.x == 0) {
-      P4 out = add(p4(acc[0], acc[1], acc[2], acc[3]), p4(c[22], c[23], c[24], c[25]));
+      P4 out = p4(acc[0] + c[18], acc[1] + c[19], acc[2] + c[20], 0.5 * (acc[3] + acc[4]) + c[21]);
       const V2 g = to_global(v2(out.s1, out.s2), n);
       out.s1 = g.x;
       out.s2 = g.y;
-      st4(dir == SOUTH ? blk.flux_macro_S : blk.flux_macro_W, gidx(d, gi, gj), scale(len, out));
+      st4(dir == SOUTH ? blk.flux_macro_S : blk.flux_macro_W, gidx(d, gi, gj), out);
     }
     return;
   }
 
   // ---------------- wall face ----------------
+  double *fw = reinterpret_cast<double *>(fhb);  // (h, b) per velocity
   const int rot = (wall == GNORTH || wall == GEAST) ? -1 : 1;
   const long ci = dir == SOUTH ? mi : mj;
   P4 wl = ld4(blk.wall_prop, ci * 4 + wall);
@@ -359,7 +385,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     for (int v = threadIdx.x; v < Nv; v += FT) {
       const V2 uv = face_velocity(d, v, n);
       const int delta = upwind_flag(uv.x, rot);
-      s[0] += uv.x * (1 - delta) * fh[v];
+      s[0] += uv.x * (1 - delta) * fw[2 * v];
       s[1] -= uv.x * delta * maxwellian(d, wl, uv, v).x;
     }
     block_sum<2>(s, sh.scratch);
@@ -368,8 +394,8 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
       const V2 uv = face_velocity(d, v, n);
       const int delta = upwind_flag(uv.x, rot);
       const V2 M = maxwellian(d, wl, uv, v);
-      fh[v] = ratio * delta * M.x + (1 - delta) * fh[v];
-      fb[v] = ratio * delta * M.y + (1 - delta) * fb[v];
+      fw[2 * v] = ratio * delta * M.x + (1 - delta) * fw[2 * v];
+      fw[2 * v + 1] = ratio * delta * M.y + (1 - delta) * fw[2 * v + 1];
     }
   } else {
     // adsorbingWall_P1 (clAdsorb.c:253-482)
@@ -384,7 +410,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
       const V2 uv = face_velocity(d, v, n);
       const int delta = upwind_flag(uv.x, rot);
       const double k = -rot * uv.x * (1 - delta);
-      const V2 total = v2(k * fh[v], k * fb[v]);
+      const V2 total = v2(k * fw[2 * v], k * fw[2 * v + 1]);
       const double beta = sticking(d, uv, Tw, wall);
       V2 ads = v2(beta * total.x * gf * (1.0 - theta), beta * total.y * gf * (1.0 - theta));
       const double fs = ocl_sign(total.x);
@@ -450,8 +476,8 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
         const V2 uv = face_velocity(d, v, n);
         const int delta = upwind_flag(uv.x, rot);
         const V2 dif = delta ? maxwellian(d, wl, uv, v) : v2(0.0, 0.0);
-        fh[v] = delta * dif.x + (1 - delta) * fh[v];
-        fb[v] = delta * dif.y + (1 - delta) * fb[v];
+        fw[2 * v] = delta * dif.x + (1 - delta) * fw[2 * v];
+        fw[2 * v + 1] = delta * dif.y + (1 - delta) * fw[2 * v + 1];
         r[0] += rot * uv.x * dif.x;
       }
       block_sum<1>(r, sh.scratch);
@@ -464,14 +490,14 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
       const V2 uv = face_velocity(d, v, n);
       const int delta = upwind_flag(uv.x, rot);
       const double sc = 1 - delta * (1 - ratio);
-      double x = fh[v] * sc, y = fb[v] * sc;
+      double x = fw[2 * v] * sc, y = fw[2 * v + 1] * sc;
       const V2 M = maxwellian(d, wd, uv, v);
       x += delta * M.x;
       y += delta * M.y;
       x -= account * delta * x;
       y -= account * delta * y;
-      fh[v] = x;
-      fb[v] = y;
+      fw[2 * v] = x;
+      fw[2 * v + 1] = y;
     }
   }
   // wallFlux (clUGKS.c:910-1011) and wallMassEnergyFluxes (1019-1147)
@@ -481,7 +507,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
   for (int k = 0; k < 12; ++k) s[k] = 0.0;
   for (int v = threadIdx.x; v < Nv; v += FT) {
     const V2 uv = face_velocity(d, v, n);
-    const double wh = fh[v], wb = fb[v];
+    const double wh = fw[2 * v], wb = fw[2 * v + 1];
     const double oh = uv.x * wh * len * dt, ob = uv.x * wb * len * dt;
     St::store(flux, base + v, v2(oh, ob));
     const double uu = uv.x * uv.x + uv.y * uv.y;
@@ -559,7 +585,7 @@ __device__ __forceinline__ double cfl_freq(const ugks_fused_block &blk, P4 m, lo
 template <typename T>
 __global__ void __launch_bounds__(FT, CELL_MIN_BLOCKS) cell_pass(const ugks_fused_block *__restrict__ B, int nb,
                                                    ugks_solve_state *__restrict__ solves) {
-  __shared__ double scratch[2 * (FT / 32)];
+  __shared__ double scratch[4 * (FT / 32)];
   __shared__ double bc[12];
   extern __shared__ double dyn[];  // axis factors: old (u, v), new (u, v)
   using St = Store<T>;
@@ -629,6 +655,7 @@ __global__ void __launch_bounds__(FT, CELL_MIN_BLOCKS) cell_pass(const ugks_fuse
   const int qs = sep ? FT / vn : 0, rs = sep ? FT % vn : 0;
   int iu = sep ? threadIdx.x / vn : 0, jv = sep ? threadIdx.x % vn : 0;
   bool nan = false;
+  double mom[4] = {0.0, 0.0, 0.0, 0.0};  // moments of f^{n+1} for the next face pass
 #pragma unroll 2
   for (int v = threadIdx.x; v < Nv; v += FT) {
     const V2 e = quad_at(d, v);
@@ -661,8 +688,15 @@ __global__ void __launch_bounds__(FT, CELL_MIN_BLOCKS) cell_pass(const ugks_fuse
     const V2 out = v2((f.x + flh + hdt * rh) * iden, (f.y + flb + hdt * rb) * iden);
     nan |= isnan(out.x) || isnan(out.y);
     St::store(blk.f, k, out);
+    const V2 o = St::as_stored(out);
+    mom[0] += o.x;
+    mom[1] = fma(e.x, o.x, mom[1]);
+    mom[2] = fma(e.y, o.x, mom[2]);
+    mom[3] += fma(fma(e.x, e.x, e.y * e.y), o.x, o.y);
   }
   if (nan) atomicExch(&sol.status, 1);
+  block_sum<4>(mom, scratch);
+  if (threadIdx.x == 0) st4(blk.cell_mom, gidx(d, gi, gj), p4(mom[0], mom[1], mom[2], 0.5 * mom[3]));
 }
 
 // ---------------------------------------------------------------------------
@@ -672,6 +706,7 @@ __global__ void __launch_bounds__(FT, CELL_MIN_BLOCKS) cell_pass(const ugks_fuse
 template <typename T>
 __global__ void __launch_bounds__(FT) ghost_pass(const ugks_fused_block *__restrict__ B, int nb,
                                                  const ugks_solve_state *__restrict__ solves) {
+  __shared__ double scratch[4 * (FT / 32)];
   using St = Store<T>;
   const int w = blockIdx.x;
   const int bi = find_block<2>(B, nb, w);
@@ -700,6 +735,18 @@ __global__ void __launch_bounds__(FT) ghost_pass(const ugks_fused_block *__restr
   }
   const size_t dst = fidx(d, gi, gj, 0);
   const int t = blk.bc_type[face];
+  // every branch writes the ghost cell through put(), which also sums the
+  // cell moments the next face pass reads
+  double mom[4] = {0.0, 0.0, 0.0, 0.0};
+  auto put = [&](int v, V2 x) {
+    St::store(blk.f, dst + v, x);
+    const V2 o = St::as_stored(x);
+    const V2 e = quad_at(d, v);
+    mom[0] += o.x;
+    mom[1] = fma(e.x, o.x, mom[1]);
+    mom[2] = fma(e.y, o.x, mom[2]);
+    mom[3] += fma(fma(e.x, e.x, e.y * e.y), o.x, o.y);
+  };
   if (t == BC_ADJACENT || t == BC_PERIODIC) {
     // edgeExchange (clGhostRoutines.c:407-538)
     const ugks_fused_block &ob = B[blk.bc_block[face]];
@@ -733,10 +780,7 @@ __global__ void __launch_bounds__(FT) ghost_pass(const ugks_fused_block *__restr
     const size_t src = ((size_t)iB * NJB + jB) * (size_t)Nv;
     const int flip = blk.bc_flip[face];
     const int32_t *perm = flip == FLIP_NS ? d.mirror_NS : (flip == FLIP_D ? d.mirror_D : d.mirror_EW);
-    using Vec = typename St::vec;
-    const Vec *s = reinterpret_cast<const Vec *>(ob.f) + src;
-    Vec *o = reinterpret_cast<Vec *>(blk.f) + dst;
-    for (int v = threadIdx.x; v < Nv; v += FT) o[v] = s[flip == NO_FLIP ? v : perm[v]];
+    for (int v = threadIdx.x; v < Nv; v += FT) put(v, St::load(ob.f, src + (flip == NO_FLIP ? v : perm[v])));
   } else if (t == BC_DIFFUSE || t == BC_ADSORBING) {
     // edgeConstGrad (clGhostRoutines.c:967-1048)
     long ei0, ej0, ei1, ej1;
@@ -750,8 +794,8 @@ __global__ void __launch_bounds__(FT) ghost_pass(const ugks_fused_block *__restr
     const size_t k0 = fidx(d, ei0, ej0, 0), k1 = fidx(d, ei1, ej1, 0);
     for (int v = threadIdx.x; v < Nv; v += FT) {
       const V2 f0 = St::load(blk.f, k0 + v), f1 = St::load(blk.f, k1 + v);
-      St::store(blk.f, dst + v, v2(__dadd_rn(f1.x, __dmul_rn(m, __dsub_rn(f1.x, f0.x))),
-                                   __dadd_rn(f1.y, __dmul_rn(m, __dsub_rn(f1.y, f0.y)))));
+      put(v, v2(__dadd_rn(f1.x, __dmul_rn(m, __dsub_rn(f1.x, f0.x))),
+                __dadd_rn(f1.y, __dmul_rn(m, __dsub_rn(f1.y, f0.y)))));
     }
   } else if (t == BC_EXTRAPOLATE_OUT || t == BC_REFLECT || t == BC_BOUNCE_BACK) {
     long si, sj;
@@ -772,10 +816,8 @@ __global__ void __launch_bounds__(FT) ghost_pass(const ugks_fused_block *__restr
       }
       if (t == BC_BOUNCE_BACK) perm = d.mirror_D;
     }
-    using Vec = typename St::vec;
-    Vec *F = reinterpret_cast<Vec *>(blk.f);
     const size_t src = fidx(d, si, sj, 0);
-    for (int v = threadIdx.x; v < Nv; v += FT) F[dst + v] = F[src + (perm ? perm[v] : v)];
+    for (int v = threadIdx.x; v < Nv; v += FT) put(v, St::load(blk.f, src + (perm ? perm[v] : v)));
   } else if (t == BC_CONSTANT || t == BC_INFLOW || t == BC_OUTFLOW) {
     const long ci = (face == GNORTH || face == GSOUTH) ? a : b;
     const P4 wp = ld4(blk.wall_prop, ci * 4 + face);
@@ -803,8 +845,10 @@ __global__ void __launch_bounds__(FT) ghost_pass(const ugks_fused_block *__restr
         prim.s3 = wp.s3;
       }
     }
-    for (int v = threadIdx.x; v < Nv; v += FT) St::store(blk.f, dst + v, shakhov_eq(d, prim, Q, quad_at(d, v), v));
+    for (int v = threadIdx.x; v < Nv; v += FT) put(v, shakhov_eq(d, prim, Q, quad_at(d, v), v));
   }
+  block_sum<4>(mom, scratch);
+  if (threadIdx.x == 0) st4(blk.cell_mom, gidx(d, gi, gj), p4(mom[0], mom[1], mom[2], 0.5 * mom[3]));
 }
 
 // ---------------------------------------------------------------------------
@@ -874,7 +918,8 @@ __global__ void __launch_bounds__(FT) init_cells(const ugks_fused_block *__restr
   }
   // calcMacro
   block_sum<4>(m, scratch);
-  prim = to_primary(d, p4(m[0], m[1], m[2], m[3]));
+  const P4 mom = p4(m[0], m[1], m[2], m[3]);
+  prim = to_primary(d, mom);
   // calcQ
   double q[2] = {0.0, 0.0};
   for (int v = threadIdx.x; v < d.Nv; v += FT) {
@@ -888,6 +933,7 @@ __global__ void __launch_bounds__(FT) init_cells(const ugks_fused_block *__restr
   block_sum<2>(q, scratch);
   if (threadIdx.x == 0) {
     st4(blk.macro, midx(d, mi, mj), prim);
+    st4(blk.cell_mom, gidx(d, mi + d.ghost, mj + d.ghost), mom);
     st2(blk.Q, midx(d, mi, mj), v2(q[0], q[1]));
     const double fq = cfl_freq(blk, prim, mi, mj);
     atomicMax(&sol.max_freq, (unsigned long long)__double_as_longlong(fq));

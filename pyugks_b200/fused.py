@@ -139,6 +139,7 @@ class FusedSolver:
         blk.wall_cover = self._dev(cover)
         blk.wall_fluxes = z(wl, 4, 8)
         blk.wall_dist = z(wl, Nv, 2)
+        blk.cell_mom = z(Ni, Nj, 4)
         x = _lib.FusedBlock()
         d = x.d
         d.ni, d.nj, d.Ni, d.Nj, d.ghost, d.Nv = ni, nj, Ni, Nj, G, Nv
@@ -173,7 +174,7 @@ class FusedSolver:
         x.solve = s
         for name in ("f", "flux_S", "flux_W", "flux_macro_S", "flux_macro_W", "macro", "Q", "prim_old",
                      "area", "centre", "mid_side", "normal", "side_length", "xy", "wall_prop",
-                     "wall_cover", "wall_fluxes", "wall_dist"):
+                     "wall_cover", "wall_fluxes", "wall_dist", "cell_mom"):
             setattr(x, name, getattr(blk, name).data_ptr())
         blk.struct = x
         return blk
