@@ -242,6 +242,9 @@ typedef struct ugks_fused_block {
                                   (u^2+v^2)/2 | 1/2) per cell, global frame;
                                   written by the init, cell and ghost passes,
                                   read by the face pass (getAL/getAR)       */
+  double *Q_next;              /* [ni][nj] x 2: calcQ of f^{n+1} with the macro of
+                                  step n+1, accumulated by the cell pass of step n
+                                  and moved to Q by the cell pass of step n+1 */
 } ugks_fused_block;
 
 typedef struct ugks_solve_state {
@@ -265,6 +268,8 @@ typedef struct ugks_solve_state {
                                   (ugks_block.py:1319-1327, ugks_sim.py:463-468) */
 } ugks_solve_state;
 
+#define UGKS_MAX_FACE_SEGMENTS 16
+
 /* Work sizes of a block table, computed on the host by ugks_fused_layout. */
 typedef struct ugks_fused_sizes {
   int32_t n_faces;        /* face work items (2 per cell corner of every block) */
@@ -273,6 +278,16 @@ typedef struct ugks_fused_sizes {
   int32_t max_nv;         /* largest Nv (sizes the face pass's shared memory)  */
   int32_t face_begin[4];  /* first face work item of the blocks of flux_method k */
   int32_t face_count[4];  /* their number (0 when no block uses method k)      */
+  int32_t max_axes;       /* largest u_num + v_num of a tensor velocity grid   */
+  /* face-pass launches: runs of consecutive blocks with one flux method and
+     one Nv (merged within a method when there are more than
+     UGKS_MAX_FACE_SEGMENTS), each launched with shared memory for its own Nv */
+  int32_t n_segments;
+  int32_t seg_begin[UGKS_MAX_FACE_SEGMENTS];
+  int32_t seg_count[UGKS_MAX_FACE_SEGMENTS];
+  int32_t seg_method[UGKS_MAX_FACE_SEGMENTS];
+  int32_t seg_max_nv[UGKS_MAX_FACE_SEGMENTS];
+  int32_t seg_max_axes[UGKS_MAX_FACE_SEGMENTS];
 } ugks_fused_sizes;
 
 /* Fills face_begin/cell_begin/ghost_begin of the host copy `blocks` and the
@@ -345,7 +360,8 @@ int ugks_getDT_noalloc(const ugks_block_desc *d, const double *xy, const double 
 const char *ugks_version(void);
 /* sizeof(ugks_block_desc), sizeof(ugks_fused_block), sizeof(ugks_solve_state),
    offsetof(ugks_fused_block, f), offsetof(ugks_solve_state, residual),
-   offsetof(ugks_block_desc, wall_D): the first n into out; returns 6.  Lets a
+   offsetof(ugks_block_desc, wall_D), sizeof(ugks_fused_sizes): the first n
+   into out; returns 7.  Lets a
    binding check its struct layout against the library's. */
 int ugks_abi_sizes(int64_t *out, int n);
 

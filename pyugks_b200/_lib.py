@@ -44,7 +44,7 @@ class FusedBlock(C.Structure):
         ("macro", vp), ("Q", vp), ("prim_old", vp),
         ("area", vp), ("centre", vp), ("mid_side", vp), ("normal", vp), ("side_length", vp),
         ("xy", vp), ("wall_prop", vp), ("wall_cover", vp), ("wall_fluxes", vp), ("wall_dist", vp),
-        ("cell_mom", vp),
+        ("cell_mom", vp), ("Q_next", vp),
     ]
 
 
@@ -62,7 +62,9 @@ class SolveState(C.Structure):
 class FusedSizes(C.Structure):
     """ugks_fused_sizes"""
     _fields_ = [("n_faces", i32), ("n_cells", i32), ("n_ghost", i32), ("max_nv", i32),
-                ("face_begin", i32 * 4), ("face_count", i32 * 4)]
+                ("face_begin", i32 * 4), ("face_count", i32 * 4), ("max_axes", i32),
+                ("n_segments", i32), ("seg_begin", i32 * 16), ("seg_count", i32 * 16),
+                ("seg_method", i32 * 16), ("seg_max_nv", i32 * 16), ("seg_max_axes", i32 * 16)]
 
 
 # argument kinds of the drop-in kernels in reference order (p pointer, i int,
@@ -124,10 +126,11 @@ def lib():
     L.ugks_version.restype = C.c_char_p
     L.ugks_abi_sizes.restype = C.c_int
     L.ugks_abi_sizes.argtypes = [C.POINTER(C.c_int64), C.c_int]
-    sizes = (C.c_int64 * 6)()
-    L.ugks_abi_sizes(sizes, 6)
+    sizes = (C.c_int64 * 7)()
+    L.ugks_abi_sizes(sizes, 7)
     want = [C.sizeof(BlockDesc), C.sizeof(FusedBlock), C.sizeof(SolveState),
-            FusedBlock.f.offset, SolveState.residual.offset, BlockDesc.wall_D.offset]
+            FusedBlock.f.offset, SolveState.residual.offset, BlockDesc.wall_D.offset,
+            C.sizeof(FusedSizes)]
     if list(sizes) != want:
         raise NativeLibraryMissing("struct layout mismatch with libugks_b200.so: %s vs %s"
                                    % (list(sizes), want))

@@ -22,6 +22,9 @@
 #include <cuda_runtime.h>
 #include <float.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "ugks_device.cuh"
 
 using namespace ugks;
@@ -29,11 +32,18 @@ using namespace ugks;
 namespace {
 
 constexpr int FT = 128;  // threads per face / cell / ghost CTA
+// face kernels come in two register budgets: FACE_MIN_BLOCKS CTAs per SM
+// (fits while 32 B x Nv of shared memory per face allows that many) and
+// FACE_MIN_BLOCKS_WIDE for larger velocity grids
 #ifndef FACE_MIN_BLOCKS
-#define FACE_MIN_BLOCKS 4
+#define FACE_MIN_BLOCKS 6
 #endif
+#ifndef FACE_MIN_BLOCKS_WIDE
+#define FACE_MIN_BLOCKS_WIDE 4
+#endif
+constexpr int FACE_NARROW_MAX_NV = 1100;  // 6 x (32 B x 1100 + 2.5 KB) <= 228 KB
 #ifndef CELL_MIN_BLOCKS
-#define CELL_MIN_BLOCKS 8
+#define CELL_MIN_BLOCKS 2  // CTAs of 8 cell warps (128 registers: the update loop does not spill)
 #endif
 
 inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
@@ -68,6 +78,90 @@ __device__ __forceinline__ double limited_dt(double dt_old, double dt_new, doubl
 // ---------------------------------------------------------------------------
 // face pass
 // ---------------------------------------------------------------------------
+// The per-face and per-cell coefficient helpers below restate getPrimary,
+// microSlope, momentU, relaxTime and the time weights (clUGKS.c:16-80,
+// 497-503, clFunctions.c:8-32) with every division by rho, lambda, tau or a
+// constant replaced by one Newton-Raphson reciprocal (nr_rcp) and products:
+// branch-free, so the independent chains of a face overlap.  Results differ
+// from the dividing forms by a few ulp.
+struct Rcp {
+  double rho, lam;  // 1/rho, 1/lambda
+};
+
+__device__ __forceinline__ P4 to_primary_rcp(const ugks_block_desc &d, P4 w, Rcp &r) {
+  const double r0 = nr_rcp(w.s0);
+  P4 p = w;
+  p.s1 = w.s1 * r0;
+  p.s2 = w.s2 * r0;
+  const double e = w.s3 - 0.5 * (w.s1 * w.s1 + w.s2 * w.s2) * r0;
+  p.s3 = (0.5 * w.s0) * nr_rcp((d.gam - 1.0) * e);
+  r.rho = r0;
+  r.lam = nr_rcp(p.s3);
+  return p;
+}
+
+__device__ __forceinline__ P4 micro_slope_rcp(double K, P4 prim, Rcp r, P4 sw) {
+  const double k2 = 0.5 * (K + 2.0) * r.lam;  // (K + 2) / (2 lambda)
+  const double c3 = 4.0 * (prim.s3 * prim.s3) * nr_rcp(K + 2.0) * r.rho;
+  const double cl = 2.0 * prim.s3 * r.rho;
+  const double uv2 = prim.s1 * prim.s1 + prim.s2 * prim.s2;
+  P4 a;
+  a.s3 = c3 * (2.0 * sw.s3 - 2.0 * prim.s1 * sw.s1 - 2.0 * prim.s2 * sw.s2 + sw.s0 * (uv2 - k2));
+  a.s2 = cl * (sw.s2 - prim.s2 * sw.s0) - prim.s2 * a.s3;
+  a.s1 = cl * (sw.s1 - prim.s1 * sw.s0) - prim.s1 * a.s3;
+  a.s0 = sw.s0 * r.rho - prim.s1 * a.s1 - prim.s2 * a.s2 - 0.5 * (uv2 + k2) * a.s3;
+  return a;
+}
+
+__device__ __forceinline__ void moments_u_rcp(double PI, double K, P4 prim, Rcp r, double Mu[MNUM],
+                                              double Mv[MTUM], double Mxi[3], double MuL[MNUM],
+                                              double MuR[MNUM]) {
+  const double sl = sqrt(prim.s3);
+  const double g = 0.5 * exp(-prim.s3 * (prim.s1 * prim.s1)) * nr_rcp(sqrt(PI * prim.s3));
+  const double hl = 0.5 * r.lam;
+  MuL[0] = 0.5 * erfc(-sl * prim.s1);
+  MuL[1] = prim.s1 * MuL[0] + g;
+  MuR[0] = 0.5 * erfc(sl * prim.s1);
+  MuR[1] = prim.s1 * MuR[0] - g;
+#pragma unroll
+  for (int i = 2; i < MNUM; ++i) {
+    MuL[i] = prim.s1 * MuL[i - 1] + ((i - 1) * hl) * MuL[i - 2];
+    MuR[i] = prim.s1 * MuR[i - 1] + ((i - 1) * hl) * MuR[i - 2];
+  }
+#pragma unroll
+  for (int i = 0; i < MNUM; ++i) Mu[i] = MuL[i] + MuR[i];
+  Mv[0] = 1.0;
+  Mv[1] = prim.s2;
+#pragma unroll
+  for (int i = 2; i < MTUM; ++i) Mv[i] = prim.s2 * Mv[i - 1] + ((i - 1) * hl) * Mv[i - 2];
+  Mxi[0] = 1.0;
+  Mxi[1] = K * hl;
+  Mxi[2] = (K * K + 2.0 * K) * (hl * hl);
+}
+
+// 1 / relaxTime
+__device__ __forceinline__ double inv_relax_time_rcp(const ugks_block_desc &d, P4 prim, Rcp r) {
+  const double p = pow(prim.s3, 1.0 - d.omega);
+  double c = 1.0;
+  switch (d.relax_type) {
+    case 0: c = 0.79788456080286541; break;
+    case 1: c = (5. / 8.) * sqrt(d.PI); break;
+    case 3: c = 2.2567583341910251; break;
+    default: break;
+  }
+  return nr_rcp((d.Kn_eff * r.rho) * c * p);
+}
+
+__device__ __forceinline__ void time_weights_rcp(double inv_tau, double dt, double Mt[5]) {
+  const double tau = nr_rcp(inv_tau);
+  const double e = exp(-dt * inv_tau);
+  Mt[3] = tau * (1.0 - e);
+  Mt[4] = -tau * dt * e + tau * Mt[3];
+  Mt[0] = dt - Mt[3];
+  Mt[1] = -tau * Mt[0] + Mt[4];
+  Mt[2] = 0.5 * (dt * dt) - tau * Mt[0];
+}
+
 struct FaceShared {
   double scratch[16 * (FT / 32)];
   double bcast[48];
@@ -98,18 +192,20 @@ __device__ __forceinline__ void weno5_part(const double (&S)[5], double &num, do
 
 // iFace (clUGKS.c:148-194) for one velocity: face value and slope of (h, b).
 // The two components share one reciprocal: 1/x = y * 1/(x y).
+// The stencil runs upwind to downwind: cells MID+1 .. 1 before the face and
+// 0 .. L-MID-2 after it for u > 0, mirrored for u <= 0; `p` points at stencil
+// cell 0 and `st` is the signed cell stride in (h, b) pairs.
 template <typename T, int FM>
-__device__ __forceinline__ void reconstruct(const void *f, size_t kv, long step, int delta,
-                                            double inv_l, double ds, double inv_ds, double &fh,
-                                            double &fb, double &sh, double &sb) {
+__device__ __forceinline__ void reconstruct(const typename Store<T>::vec *p, long st, double inv_l,
+                                            double ds, double inv_ds, double &fh, double &fb,
+                                            double &sh, double &sb) {
   constexpr int L = FM == 1 ? 5 : 3, MID = FM == 1 ? 2 : 1;
   double Sh[L], Sb[L];
 #pragma unroll
   for (int s = 0; s < L; ++s) {
-    const long off = delta ? (long)(-MID - 1 + s) : (long)(MID - s);
-    const V2 x = Store<T>::load(f, (size_t)((long)kv + off * step));
-    Sh[s] = x.x;
-    Sb[s] = x.y;
+    const auto x = p[s * st];
+    Sh[s] = (double)x.x;
+    Sb[s] = (double)x.y;
   }
   if constexpr (FM == 0) {
     // vanLeer (clFunctions.c:255-261)
@@ -185,20 +281,27 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
   double2 *fhb = reinterpret_cast<double2 *>(dyn), *sgb = fhb + Nv;
   const V2 n = ld2(blk.normal, faceidx(d, gi, gj, dir));
   const V2 mid = ld2(blk.mid_side, faceidx(d, gi, gj, dir));
-  // stencil geometry for both upwind directions (iFace, clUGKS.c:148-176)
-  double dist[2], inv_dist[2], inv_l1[2];
-#pragma unroll
-  for (int dl = 0; dl < 2; ++dl) {
-    const long c0 = dl ? -1 : 0, c1 = dl ? -2 : 1;  // cells MID and MID-1 relative to the face
-    const long c0i = dir == SOUTH ? gi : gi + c0, c0j = dir == SOUTH ? gj + c0 : gj;
-    const long c1i = dir == SOUTH ? gi : gi + c1, c1j = dir == SOUTH ? gj + c1 : gj;
-    const V2 a = ld2(blk.centre, gidx(d, c0i, c0j)), b = ld2(blk.centre, gidx(d, c1i, c1j));
-    dist[dl] = sqrt((mid.x - a.x) * (mid.x - a.x) + (mid.y - a.y) * (mid.y - a.y));
-    inv_dist[dl] = 1.0 / dist[dl];
-    inv_l1[dl] = 1.0 / sqrt((a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y));
+  // stencil geometry for both upwind directions (iFace, clUGKS.c:148-176):
+  // index 1 for u > 0 (upwind cell before the face), 0 otherwise
+  double dist0, dist1, idist0, idist1, il0, il1;
+  {
+    auto geo = [&](long c0, long c1, double &ds, double &ids, double &il) {
+      const long c0i = dir == SOUTH ? gi : gi + c0, c0j = dir == SOUTH ? gj + c0 : gj;
+      const long c1i = dir == SOUTH ? gi : gi + c1, c1j = dir == SOUTH ? gj + c1 : gj;
+      const V2 a = ld2(blk.centre, gidx(d, c0i, c0j)), b = ld2(blk.centre, gidx(d, c1i, c1j));
+      ds = sqrt((mid.x - a.x) * (mid.x - a.x) + (mid.y - a.y) * (mid.y - a.y));
+      ids = 1.0 / ds;
+      il = 1.0 / sqrt((a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y));
+    };
+    geo(0, 1, dist0, idist0, il0);     // cells MID and MID-1 relative to the face, u <= 0
+    geo(-1, -2, dist1, idist1, il1);   // u > 0
   }
   const long step = dir == SOUTH ? (long)Nv : (long)d.Nj * Nv;
   const size_t base = fidx(d, gi, gj, 0);
+  constexpr int MID = FM == 1 ? 2 : 1;
+  using Vec = typename St::vec;
+  const Vec *fcell = reinterpret_cast<const Vec *>(blk.f) + base;  // cell (gi, gj), velocity 0
+  const Vec *up1 = fcell - (MID + 1) * step, *up0 = fcell + MID * step;
 
   // ---- sweep 1: reconstruction (+ interior faces: the face moments W of
   // getFaceCons; the 1/2 of the energy moment is applied after the sum)
@@ -206,10 +309,10 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
 #pragma unroll 2
   for (int v = threadIdx.x; v < Nv; v += FT) {
     const V2 uv = face_velocity(d, v, n);
-    const int delta = uv.x > 0.0 ? 1 : 0;
+    const bool up = uv.x > 0.0;
     double ffh, ffb, sx, sy;
-    reconstruct<T, FM>(blk.f, base + v, step, delta, inv_l1[delta], dist[delta], inv_dist[delta],
-                       ffh, ffb, sx, sy);
+    reconstruct<T, FM>((up ? up1 : up0) + v, up ? step : -step, up ? il1 : il0, up ? dist1 : dist0,
+                       up ? idist1 : idist0, ffh, ffb, sx, sy);
     fhb[v] = make_double2(ffh, ffb);
     sgb[v] = make_double2(sx, sy);
     if (wall < 0) {
@@ -226,7 +329,8 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     // ---------------- interior face ----------------
     block_sum<4>(m, sh.scratch);
     const P4 W = p4(m[0], m[1], m[2], 0.5 * m[3]);
-    const P4 prim = to_primary(d, W);  // getPLR (clUGKS.c:421-422), every thread
+    Rcp rc;
+    const P4 prim = to_primary_rcp(d, W, rc);  // getPLR (clUGKS.c:421-422), every thread
     const int un = d.u_num, vn = d.v_num;
     const bool sep = un > 0 && un * vn == Nv && un + vn <= 512;
     double *Eu = dyn + 4 * Nv, *Ev = Eu + (sep ? un : 0);
@@ -243,24 +347,25 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
         const P4 ml = ld4(blk.cell_mom, kl), mr = ld4(blk.cell_mom, kr);
         const V2 ul = to_local(v2(ml.s1, ml.s2), n), ur = to_local(v2(mr.s1, mr.s2), n);
         const V2 cl = ld2(blk.centre, kl), cr = ld2(blk.centre, kr);
-        const double idl = 1.0 / sqrt((mid.x - cl.x) * (mid.x - cl.x) + (mid.y - cl.y) * (mid.y - cl.y));
-        const double idr = 1.0 / sqrt((mid.x - cr.x) * (mid.x - cr.x) + (mid.y - cr.y) * (mid.y - cr.y));
-        const P4 aL = micro_slope(d, prim, p4((W.s0 - ml.s0) * idl, (W.s1 - ul.x) * idl,
-                                              (W.s2 - ul.y) * idl, (W.s3 - ml.s3) * idl));
-        const P4 aR = micro_slope(d, prim, p4((mr.s0 - W.s0) * idr, (ur.x - W.s1) * idr,
-                                              (ur.y - W.s2) * idr, (mr.s3 - W.s3) * idr));
+        const double idl = nr_rcp(sqrt((mid.x - cl.x) * (mid.x - cl.x) + (mid.y - cl.y) * (mid.y - cl.y)));
+        const double idr = nr_rcp(sqrt((mid.x - cr.x) * (mid.x - cr.x) + (mid.y - cr.y) * (mid.y - cr.y)));
+        const P4 aL = micro_slope_rcp(d.K, prim, rc, p4((W.s0 - ml.s0) * idl, (W.s1 - ul.x) * idl,
+                                                        (W.s2 - ul.y) * idl, (W.s3 - ml.s3) * idl));
+        const P4 aR = micro_slope_rcp(d.K, prim, rc, p4((mr.s0 - W.s0) * idr, (ur.x - W.s1) * idr,
+                                                        (ur.y - W.s2) * idr, (mr.s3 - W.s3) * idr));
         double Mu[MNUM], Mv[MTUM], Mxi[3], MuL[MNUM], MuR[MNUM], Mt[5];
-        moments_u(d, prim, Mu, Mv, Mxi, MuL, MuR);
-        const P4 aT = micro_slope(d, prim, scale(-prim.s0, add(moment_au(aL, MuL, Mv, Mxi, 1, 0),
-                                                               moment_au(aR, MuR, Mv, Mxi, 1, 0))));
-        time_weights(relax_time(d, prim), dt, Mt);
+        moments_u_rcp(d.PI, d.K, prim, rc, Mu, Mv, Mxi, MuL, MuR);
+        const P4 aT = micro_slope_rcp(d.K, prim, rc,
+                                      scale(-prim.s0, add(moment_au(aL, MuL, Mv, Mxi, 1, 0),
+                                                          moment_au(aR, MuR, Mv, Mxi, 1, 0))));
+        time_weights_rcp(inv_relax_time_rcp(d, prim, rc), dt, Mt);
         const P4 g0 = scale(prim.s0,
                             add(add(scale(Mt[0], moment_uv(Mu, Mv, Mxi, 1, 0, 0)),
                                     scale(Mt[1], add(moment_au(aL, MuL, Mv, Mxi, 2, 0),
                                                      moment_au(aR, MuR, Mv, Mxi, 2, 0)))),
                                 scale(Mt[2], moment_au(aT, Mu, Mv, Mxi, 1, 0))));
         // distFlux coefficients folded per face (derivation at sweep 3)
-        const double kb = d.K / (2.0 * prim.s3), xk = Mxi[2] - kb * kb;
+        const double kb = (0.5 * d.K) * rc.lam, xk = Mxi[2] - kb * kb;
         double *c = sh.bcast;
         const P4 as[2] = {aL, aR};
 #pragma unroll
@@ -315,8 +420,8 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     const double *c = sh.bcast;
     const V2 Q = v2(q[0], q[1]);
     const double lam = prim.s3, Ux = prim.s1, Uy = prim.s2, lam2 = 2.0 * lam;
-    const double kb = d.K / (2.0 * lam);
-    const double s0 = 0.8 * (1 - d.Pr) * (lam * lam) / prim.s0;
+    const double kb = (0.5 * d.K) * rc.lam;
+    const double s0 = 0.8 * (1 - d.Pr) * (lam * lam) * rc.rho;
     const double Mt0 = c[15], Mt3 = c[16], Mt4 = c[17];
     const double sx = (Mt0 * s0) * Q.x, sy = (Mt0 * s0) * Q.y;
     const double T0 = c[10], T1 = c[11], T2 = c[12], T3 = c[13], CT = c[14];
@@ -532,8 +637,8 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
 }
 
 // main face pass: one CTA per face work item of the blocks of one flux method
-template <typename T, int FM>
-__global__ void __launch_bounds__(FT, FACE_MIN_BLOCKS) face_pass(const ugks_fused_block *__restrict__ B, int nb,
+template <typename T, int FM, int MINB>
+__global__ void __launch_bounds__(FT, MINB) face_pass(const ugks_fused_block *__restrict__ B, int nb,
                                                                  ugks_solve_state *__restrict__ solves,
                                                                  int first) {
   face_item<T, FM>(B, nb, solves, first + (int)blockIdx.x, 0);
@@ -542,8 +647,8 @@ __global__ void __launch_bounds__(FT, FACE_MIN_BLOCKS) face_pass(const ugks_fuse
 // the flux pass redone after a dt change (ugks_sim.py:432-441): RETRY_CTAS
 // CTAs per solve; a solve whose retry flag is clear costs one early exit each
 constexpr int RETRY_CTAS = 148;
-template <typename T, int FM>
-__global__ void __launch_bounds__(FT, FACE_MIN_BLOCKS) face_retry(const ugks_fused_block *__restrict__ B, int nb,
+template <typename T, int FM, int MINB>
+__global__ void __launch_bounds__(FT, MINB) face_retry(const ugks_fused_block *__restrict__ B, int nb,
                                                                   ugks_solve_state *__restrict__ solves,
                                                                   int ns) {
   const int s = blockIdx.x / RETRY_CTAS, r = blockIdx.x % RETRY_CTAS;
@@ -582,40 +687,51 @@ __device__ __forceinline__ double cfl_freq(const ugks_fused_block &blk, P4 m, lo
   return (dx * u + dy * v) / blk.area[gidx(d, mi + G, mj + G)];
 }
 
+// one warp per cell, CW cells per CTA: no block-wide barrier, so the serial
+// per-cell coefficients of one cell (lane 0) stall only that cell's warp
+constexpr int CW = 8;
+// per-warp shared memory: the axis tables of the old and new state
+// (2 (u_num + v_num) doubles) and CELL_COEF coefficient slots
+constexpr int CELL_COEF = 16;
+
+template <int N>
+__device__ __forceinline__ void warp_sum(double (&x)[N]) {
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x[k] += __shfl_xor_sync(0xffffffffu, x[k], o);
+  }
+}
+
 template <typename T>
-__global__ void __launch_bounds__(FT, CELL_MIN_BLOCKS) cell_pass(const ugks_fused_block *__restrict__ B, int nb,
-                                                   ugks_solve_state *__restrict__ solves) {
-  __shared__ double scratch[4 * (FT / 32)];
-  __shared__ double bc[12];
-  extern __shared__ double dyn[];  // axis factors: old (u, v), new (u, v)
+__global__ void __launch_bounds__(CW * 32, CELL_MIN_BLOCKS) cell_pass(const ugks_fused_block *__restrict__ B, int nb,
+                                                        ugks_solve_state *__restrict__ solves, int n_cells,
+                                                        int wstride) {
+  extern __shared__ double dyn[];
   using St = Store<T>;
-  const int w = blockIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int w = blockIdx.x * CW + warp;
+  if (w >= n_cells) return;
   const int bi = find_block<1>(B, nb, w);
   const ugks_fused_block &blk = B[bi];
   const ugks_block_desc &d = blk.d;
   ugks_solve_state &sol = solves[blk.solve];
   if (!sol.active) return;
-  const double dt = sol.dt;
   const int lc = w - blk.cell_begin;
   const long mi = lc / d.nj, mj = lc % d.nj;
   const long gi = mi + d.ghost, gj = mj + d.ghost;
   const int Nv = d.Nv, un = d.u_num, vn = d.v_num;
   const bool sep = un > 0 && un * vn == Nv && un + vn <= 512;
-  double *Eou = dyn, *Eov = Eou + un, *Enu = Eov + vn, *Env = Enu + un;
+  double *Eou = dyn + (size_t)warp * wstride, *Eov = Eou + un, *Enu = Eov + vn, *Env = Enu + un;
+  double *bc = dyn + (size_t)warp * wstride + (wstride - CELL_COEF);
   const size_t base = fidx(d, gi, gj, 0);
+  const size_t sj = (size_t)Nv, si = (size_t)d.Nj * Nv;
+  const double dt = sol.dt;
   const P4 old = ld4(blk.macro, midx(d, mi, mj));
-  // calcQ on f^n with the macro of f^n
-  double q[2] = {0.0, 0.0};
-  const double Kinv = 1.0 / d.K;
-  for (int v = threadIdx.x; v < Nv; v += FT) {
-    const V2 f = St::load(blk.f, base + v);
-    const V2 e = quad_at(d, v);
-    const double cx = e.x - old.s1, cy = e.y - old.s2, c2 = cx * cx + cy * cy;
-    const double t = c2 * f.x + f.y * Kinv;
-    q[0] += 0.5 * (cx * t);
-    q[1] += 0.5 * (cy * t);
-  }
-  if (threadIdx.x == 0) {
+  // calcQ of f^n with the macro of f^n: accumulated by the previous cell pass
+  // (or the initialisation) in Q_next
+  const V2 Q = ld2(blk.Q_next, midx(d, mi, mj));
+  if (lane == 0) {
     // updateMacro
     const P4 wc = to_conserved(d, old);
     const double iA = 1.0 / blk.area[gidx(d, gi, gj)];
@@ -623,45 +739,59 @@ __global__ void __launch_bounds__(FT, CELL_MIN_BLOCKS) cell_pass(const ugks_fuse
     const P4 w0 = ld4(blk.flux_macro_W, gidx(d, gi, gj)), w1 = ld4(blk.flux_macro_W, gidx(d, gi + 1, gj));
     const P4 nw = p4(wc.s0 + (s0.s0 - s1.s0 + w0.s0 - w1.s0) * iA, wc.s1 + (s0.s1 - s1.s1 + w0.s1 - w1.s1) * iA,
                      wc.s2 + (s0.s2 - s1.s2 + w0.s2 - w1.s2) * iA, wc.s3 + (s0.s3 - s1.s3 + w0.s3 - w1.s3) * iA);
-    const P4 prim = to_primary(d, nw);
+    Rcp rn, ro;
+    const P4 prim = to_primary_rcp(d, nw, rn);
+    ro.rho = nr_rcp(old.s0);
+    ro.lam = nr_rcp(old.s3);
     st4(blk.macro, midx(d, mi, mj), prim);
     st4(blk.prim_old, midx(d, mi, mj), old);
-    bc[0] = prim.s0; bc[1] = prim.s1; bc[2] = prim.s2; bc[3] = prim.s3;
-    bc[4] = 1.0 / relax_time(d, old);
-    bc[5] = 1.0 / relax_time(d, prim);
-    bc[6] = iA;
+    st2(blk.Q, midx(d, mi, mj), Q);
+    // UGKS_update (clUGKS.c:1189-1257) per velocity, regrouped:
+    //   f' = f a1 + (sum of face fluxes) a2 + fEQ(new) a3 + fEQ(old) a4,
+    //   a1 = (1 - dt/2 /tau_old) / D, a2 = 1 / (A D), a3 = dt/2 / (tau D),
+    //   a4 = dt/2 / (tau_old D), D = 1 + dt/2 / tau;
+    // a3 and a4 go into the Maxwellian prefactors rho lambda / pi of fEQ
+    const double itau_old = inv_relax_time_rcp(d, old, ro), itau = inv_relax_time_rcp(d, prim, rn);
+    const double hdt = 0.5 * dt, iden = nr_rcp(1.0 + hdt * itau);
+    const double ipi = nr_rcp(d.PI);
+    bc[0] = prim.s1;
+    bc[1] = prim.s2;
+    bc[2] = prim.s3;
+    bc[3] = (1.0 - hdt * itau_old) * iden;                         // a1
+    bc[4] = iden * iA;                                             // a2
+    bc[5] = prim.s0 * (prim.s3 * ipi) * (hdt * itau * iden);       // new prefactor x a3
+    bc[6] = old.s0 * (old.s3 * ipi) * (hdt * itau_old * iden);     // old prefactor x a4
+    bc[7] = (0.5 * d.K) * rn.lam;                                  // K / (2 lambda) new
+    bc[8] = 0.8 * (1 - d.Pr) * (prim.s3 * prim.s3) * rn.rho;       // Shakhov factor new
     const double fq = cfl_freq(blk, prim, mi, mj);
     atomicMax(&sol.max_freq, (unsigned long long)__double_as_longlong(fq));
-  } else if (sep && threadIdx.x >= 32) {
-    axis_exp(Eou, d.quad, un, vn, 0, old.s1, old.s3, threadIdx.x - 32, FT - 32);
-    axis_exp(Eov, d.quad, vn, 1, 1, old.s2, old.s3, threadIdx.x - 32, FT - 32);
+  } else if (sep) {
+    axis_exp(Eou, d.quad, un, vn, 0, old.s1, old.s3, lane - 1, 31);
+    axis_exp(Eov, d.quad, vn, 1, 1, old.s2, old.s3, lane - 1, 31);
   }
-  block_sum<2>(q, scratch);
-  if (threadIdx.x == 0) st2(blk.Q, midx(d, mi, mj), v2(q[0], q[1]));
-  const P4 prim = p4(bc[0], bc[1], bc[2], bc[3]);
-  const double itau_old = bc[4], itau = bc[5], iA = bc[6];
+  __syncwarp();
+  const double nU = bc[0], nV = bc[1], nl = bc[2];
   if (sep) {
-    axis_exp(Enu, d.quad, un, vn, 0, prim.s1, prim.s3, threadIdx.x, FT);
-    axis_exp(Env, d.quad, vn, 1, 1, prim.s2, prim.s3, threadIdx.x, FT);
-    __syncthreads();
+    axis_exp(Enu, d.quad, un, vn, 0, nU, nl, lane, 32);
+    axis_exp(Env, d.quad, vn, 1, 1, nV, nl, lane, 32);
+    __syncwarp();
   }
-  const V2 Q = v2(q[0], q[1]);
-  const double co = old.s0 * (old.s3 / d.PI), cn = prim.s0 * (prim.s3 / d.PI);
-  const double ko = d.K / (2.0 * old.s3), kn = d.K / (2.0 * prim.s3);
-  const double so = 0.8 * (1 - d.Pr) * (old.s3 * old.s3) / old.s0;
-  const double sn = 0.8 * (1 - d.Pr) * (prim.s3 * prim.s3) / prim.s0;
-  const double hdt = 0.5 * dt, iden = 1.0 / (1.0 + 0.5 * dt * itau);
-  const size_t sj = (size_t)Nv, si = (size_t)d.Nj * Nv;
-  const int qs = sep ? FT / vn : 0, rs = sep ? FT % vn : 0;
-  int iu = sep ? threadIdx.x / vn : 0, jv = sep ? threadIdx.x % vn : 0;
+  const double a1 = bc[3], a2 = bc[4], cn = bc[5], co = bc[6], kn = bc[7], sn = bc[8];
+  const double ko = (0.5 * d.K) * nr_rcp(old.s3);
+  const double so = 0.8 * (1 - d.Pr) * (old.s3 * old.s3) * nr_rcp(old.s0);
+  const int qs = sep ? 32 / vn : 0, rs = sep ? 32 % vn : 0;
+  int iu = sep ? lane / vn : 0, jv = sep ? lane % vn : 0;
   bool nan = false;
-  double mom[4] = {0.0, 0.0, 0.0, 0.0};  // moments of f^{n+1} for the next face pass
 #pragma unroll 2
-  for (int v = threadIdx.x; v < Nv; v += FT) {
+  for (int v = lane; v < Nv; v += 32) {
+    const size_t k = base + v;
+    const V2 f = St::load(blk.f, k);
+    const V2 s0 = St::load(blk.flux_S, k), s1 = St::load(blk.flux_S, k + sj);
+    const V2 w0 = St::load(blk.flux_W, k), w1 = St::load(blk.flux_W, k + si);
     const V2 e = quad_at(d, v);
     const double wv = d.weight[v];
-    const double ox = e.x - old.s1, oy = e.y - old.s2, o2 = ox * ox + oy * oy;
-    const double nx = e.x - prim.s1, ny = e.y - prim.s2, n2 = nx * nx + ny * ny;
+    const double ox = e.x - old.s1, oy = e.y - old.s2, o2 = fma(ox, ox, oy * oy);
+    const double nx = e.x - nU, ny = e.y - nV, n2 = fma(nx, nx, ny * ny);
     double Eo, En;
     if (sep) {
       Eo = Eou[iu] * Eov[jv];
@@ -671,32 +801,43 @@ __global__ void __launch_bounds__(FT, CELL_MIN_BLOCKS) cell_pass(const ugks_fuse
       if (jv >= vn) { jv -= vn; ++iu; }
     } else {
       Eo = exp(-old.s3 * o2);
-      En = exp(-prim.s3 * n2);
+      En = exp(-nl * n2);
     }
-    // fEQ (clFunctions.c:79-86) at the old and the new macro state
-    const double ho = wv * co * Eo, bo = ho * ko, hn = wv * cn * En, bn = hn * kn;
-    const double So = so * (ox * Q.x + oy * Q.y), po = 2 * old.s3 * o2;
-    const double Sn = sn * (nx * Q.x + ny * Q.y), pn = 2 * prim.s3 * n2;
-    const double foh = ho + (So * (po - 4)) * ho, fob = bo + (So * (po - 2)) * bo;
-    const double fnh = hn + (Sn * (pn - 4)) * hn, fnb = bn + (Sn * (pn - 2)) * bn;
-    const size_t k = base + v;
-    const V2 f = St::load(blk.f, k);
-    const V2 a0 = St::load(blk.flux_S, k), a1 = St::load(blk.flux_S, k + sj);
-    const V2 b0 = St::load(blk.flux_W, k), b1 = St::load(blk.flux_W, k + si);
-    const double flh = (a0.x - a1.x + b0.x - b1.x) * iA, flb = (a0.y - a1.y + b0.y - b1.y) * iA;
-    const double rh = fnh * itau + (foh - f.x) * itau_old, rb = fnb * itau + (fob - f.y) * itau_old;
-    const V2 out = v2((f.x + flh + hdt * rh) * iden, (f.y + flb + hdt * rb) * iden);
+    // fEQ (clFunctions.c:79-86) at the old and the new macro state, scaled
+    const double ho = wv * co * Eo, hn = wv * cn * En;
+    const double So = so * fma(ox, Q.x, oy * Q.y), Sn = sn * fma(nx, Q.x, ny * Q.y);
+    const double po = fma(2.0 * old.s3, o2, -4.0), pn = fma(2.0 * nl, n2, -4.0);
+    const double eh = fma(So * po, ho, ho) + fma(Sn * pn, hn, hn);
+    const double eb = ko * fma(So * (po + 2.0), ho, ho) + kn * fma(Sn * (pn + 2.0), hn, hn);
+    const double flh = (s0.x - s1.x) + (w0.x - w1.x), flb = (s0.y - s1.y) + (w0.y - w1.y);
+    const V2 out = v2(fma(f.x, a1, fma(flh, a2, eh)), fma(f.y, a1, fma(flb, a2, eb)));
     nan |= isnan(out.x) || isnan(out.y);
     St::store(blk.f, k, out);
-    const V2 o = St::as_stored(out);
+  }
+  if (nan) atomicExch(&sol.status, 1);
+  // moments of f^{n+1} for the next face pass, and calcQ (clKernel.c:480-543)
+  // of f^{n+1} with the new macro for the next cell pass: a second sweep over
+  // the values this lane just stored (L2-resident), which keeps the update
+  // loop's registers free
+  const double Kinv = nr_rcp(d.K);
+  double mom[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int v = lane; v < Nv; v += 32) {
+    const V2 o = St::load(blk.f, base + v);
+    const V2 e = quad_at(d, v);
+    const double nx = e.x - nU, ny = e.y - nV, n2 = fma(nx, nx, ny * ny);
     mom[0] += o.x;
     mom[1] = fma(e.x, o.x, mom[1]);
     mom[2] = fma(e.y, o.x, mom[2]);
     mom[3] += fma(fma(e.x, e.x, e.y * e.y), o.x, o.y);
+    const double t = fma(n2, o.x, o.y * Kinv);
+    mom[4] = fma(nx, t, mom[4]);
+    mom[5] = fma(ny, t, mom[5]);
   }
-  if (nan) atomicExch(&sol.status, 1);
-  block_sum<4>(mom, scratch);
-  if (threadIdx.x == 0) st4(blk.cell_mom, gidx(d, gi, gj), p4(mom[0], mom[1], mom[2], 0.5 * mom[3]));
+  warp_sum<6>(mom);
+  if (lane == 0) {
+    st4(blk.cell_mom, gidx(d, gi, gj), p4(mom[0], mom[1], mom[2], 0.5 * mom[3]));
+    st2(blk.Q_next, midx(d, mi, mj), v2(0.5 * mom[4], 0.5 * mom[5]));
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -935,6 +1076,7 @@ __global__ void __launch_bounds__(FT) init_cells(const ugks_fused_block *__restr
     st4(blk.macro, midx(d, mi, mj), prim);
     st4(blk.cell_mom, gidx(d, mi + d.ghost, mj + d.ghost), mom);
     st2(blk.Q, midx(d, mi, mj), v2(q[0], q[1]));
+    st2(blk.Q_next, midx(d, mi, mj), v2(q[0], q[1]));
     const double fq = cfl_freq(blk, prim, mi, mj);
     atomicMax(&sol.max_freq, (unsigned long long)__double_as_longlong(fq));
   }
@@ -977,46 +1119,84 @@ int init_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
   return launch_status();
 }
 
-template <typename T, int FM>
+template <typename T, int FM, int MINB>
 void set_face_attributes() {
-  cudaFuncSetAttribute(face_pass<T, FM>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(face_retry<T, FM>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(face_pass<T, FM, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(face_retry<T, FM, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(face_pass<T, FM, MINB>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       cudaSharedmemCarveoutMaxShared);
+}
+
+// shared memory of a face CTA: (h, b) and slopes per velocity + axis tables
+inline size_t face_smem(int max_nv, int max_axes) {
+  return (size_t)4 * sizeof(double) * (size_t)max_nv + sizeof(double) * (size_t)max_axes;
+}
+
+// the main face pass of one segment (one flux method, one register budget)
+template <typename T, int MINB>
+void launch_segment(const ugks_fused_block *B, int nb, ugks_solve_state *solves, int method, int first,
+                    int count, size_t smem, cudaStream_t st) {
+  switch (method) {
+    case 0: face_pass<T, 0, MINB><<<count, FT, smem, st>>>(B, nb, solves, first); break;
+    case 1: face_pass<T, 1, MINB><<<count, FT, smem, st>>>(B, nb, solves, first); break;
+    case 3: face_pass<T, 3, MINB><<<count, FT, smem, st>>>(B, nb, solves, first); break;
+    default: break;
+  }
+}
+
+// the retry pass of every flux method (per solve; rare)
+template <typename T, int MINB>
+void launch_retry(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks_solve_state *solves,
+                  int ns, size_t smem, cudaStream_t st) {
+  const unsigned rg = (unsigned)ns * RETRY_CTAS;
+  if (z->face_count[0]) face_retry<T, 0, MINB><<<rg, FT, smem, st>>>(B, nb, solves, ns);
+  if (z->face_count[1]) face_retry<T, 1, MINB><<<rg, FT, smem, st>>>(B, nb, solves, ns);
+  if (z->face_count[3]) face_retry<T, 3, MINB><<<rg, FT, smem, st>>>(B, nb, solves, ns);
 }
 
 template <typename T>
 int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks_solve_state *solves,
               int ns, void *stream, void *const *events = nullptr) {
   cudaStream_t st = S(stream);
-  // face pass: (h, b) and slopes per velocity + the two axis factor tables
-  const size_t smem = (size_t)4 * sizeof(double) * (size_t)z->max_nv + 2 * sizeof(double) * 512;
-  const size_t csmem = 4 * sizeof(double) * 512;
+  // face pass: (h, b) and slopes per velocity + the two axis factor tables;
+  // cell pass: the axis factor tables of the old and new macro state
+  const size_t smem = face_smem(z->max_nv, z->max_axes);
+  const int cstride = 2 * z->max_axes + CELL_COEF;  // doubles of shared memory per cell warp
+  const size_t csmem = (size_t)CW * cstride * sizeof(double);
   static bool attr_set = false;  // one flag per instantiation
   if (!attr_set) {
-    set_face_attributes<T, 0>();
-    set_face_attributes<T, 1>();
-    set_face_attributes<T, 3>();
+    set_face_attributes<T, 0, FACE_MIN_BLOCKS>();
+    set_face_attributes<T, 1, FACE_MIN_BLOCKS>();
+    set_face_attributes<T, 3, FACE_MIN_BLOCKS>();
+    set_face_attributes<T, 0, FACE_MIN_BLOCKS_WIDE>();
+    set_face_attributes<T, 1, FACE_MIN_BLOCKS_WIDE>();
+    set_face_attributes<T, 3, FACE_MIN_BLOCKS_WIDE>();
     attr_set = true;
   }
   if (smem > 200 * 1024) return -(int)cudaErrorInvalidValue;
   const unsigned sg = (unsigned)((ns + 127) / 128);
-  const unsigned rg = (unsigned)ns * RETRY_CTAS;
   auto mark = [&](int k) {
     if (events) cudaEventRecord(reinterpret_cast<cudaEvent_t>(events[k]), st);
   };
   mark(0);
-  if (z->face_count[0]) face_pass<T, 0><<<z->face_count[0], FT, smem, st>>>(B, nb, solves, z->face_begin[0]);
-  if (z->face_count[1]) face_pass<T, 1><<<z->face_count[1], FT, smem, st>>>(B, nb, solves, z->face_begin[1]);
-  if (z->face_count[3]) face_pass<T, 3><<<z->face_count[3], FT, smem, st>>>(B, nb, solves, z->face_begin[3]);
+  for (int k = 0; k < z->n_segments && k < UGKS_MAX_FACE_SEGMENTS; ++k) {
+    if (z->seg_count[k] <= 0) continue;
+    const size_t sm = face_smem(z->seg_max_nv[k], z->seg_max_axes[k]);
+    if (z->seg_max_nv[k] <= FACE_NARROW_MAX_NV)
+      launch_segment<T, FACE_MIN_BLOCKS>(B, nb, solves, z->seg_method[k], z->seg_begin[k], z->seg_count[k], sm, st);
+    else
+      launch_segment<T, FACE_MIN_BLOCKS_WIDE>(B, nb, solves, z->seg_method[k], z->seg_begin[k], z->seg_count[k], sm, st);
+  }
+  const bool narrow = z->max_nv <= FACE_NARROW_MAX_NV;
   mark(1);
   dt_check<<<sg, 128, 0, st>>>(solves, ns, 0);
   mark(2);
-  if (z->face_count[0]) face_retry<T, 0><<<rg, FT, smem, st>>>(B, nb, solves, ns);
-  if (z->face_count[1]) face_retry<T, 1><<<rg, FT, smem, st>>>(B, nb, solves, ns);
-  if (z->face_count[3]) face_retry<T, 3><<<rg, FT, smem, st>>>(B, nb, solves, ns);
+  if (narrow) launch_retry<T, FACE_MIN_BLOCKS>(B, nb, z, solves, ns, smem, st);
+  else launch_retry<T, FACE_MIN_BLOCKS_WIDE>(B, nb, z, solves, ns, smem, st);
   mark(3);
   dt_check<<<sg, 128, 0, st>>>(solves, ns, 1);
   mark(4);
-  if (z->n_cells) cell_pass<T><<<z->n_cells, FT, csmem, st>>>(B, nb, solves);
+  if (z->n_cells) cell_pass<T><<<(z->n_cells + CW - 1) / CW, CW * 32, csmem, st>>>(B, nb, solves, z->n_cells, cstride);
   mark(5);
   dt_update<<<sg, 128, 0, st>>>(solves, ns);
   mark(6);
@@ -1087,8 +1267,13 @@ int ugks_residual(const ugks_fused_block *blocks_dev, int nblocks, ugks_solve_st
 
 int ugks_fused_layout(ugks_fused_block *blocks, int nblocks, ugks_fused_sizes *z) {
   int64_t f = 0, c = 0, g = 0;
-  int32_t max_nv = 0;
+  int32_t max_nv = 0, max_axes = 0;
   int64_t fb[4] = {0, 0, 0, 0}, fc[4] = {0, 0, 0, 0};
+  struct Run {
+    int method, nv, max_nv, axes;
+    int64_t begin, count;
+  };
+  std::vector<Run> runs;
   int last_method = -1, seen = 0, last_solve = -1;
   for (int b = 0; b < nblocks; ++b) {
     ugks_fused_block &x = blocks[b];
@@ -1108,17 +1293,51 @@ int ugks_fused_layout(ugks_fused_block *blocks, int nblocks, ugks_fused_sizes *z
     x.cell_begin = (int32_t)c;
     x.ghost_begin = (int32_t)g;
     const int64_t nf = 2ll * (x.d.ni + 1) * (x.d.nj + 1);
+    const int axes_b = (x.d.u_num > 0 && x.d.u_num * x.d.v_num == x.d.Nv && x.d.u_num + x.d.v_num <= 512)
+                           ? x.d.u_num + x.d.v_num : 0;
+    if (runs.empty() || runs.back().method != m || runs.back().nv != x.d.Nv)
+      runs.push_back(Run{m, x.d.Nv, x.d.Nv, axes_b, f, 0});
+    runs.back().count += nf;
+    runs.back().axes = std::max(runs.back().axes, axes_b);
     f += nf;
     fc[m] += nf;
     c += (int64_t)x.d.ni * x.d.nj;
     g += 2ll * x.d.ghost * (x.d.ni + x.d.nj);
     if (x.d.Nv > max_nv) max_nv = x.d.Nv;
+    const int axes = x.d.u_num + x.d.v_num;
+    if (x.d.u_num > 0 && x.d.u_num * x.d.v_num == x.d.Nv && axes <= 512 && axes > max_axes) max_axes = axes;
   }
   if (f > INT32_MAX || c > INT32_MAX || g > INT32_MAX) return -1;
   z->n_faces = (int32_t)f;
   z->n_cells = (int32_t)c;
   z->n_ghost = (int32_t)g;
   z->max_nv = max_nv;
+  z->max_axes = max_axes;
+  // at most UGKS_MAX_FACE_SEGMENTS launches: merge the adjacent pair of one
+  // method whose merged Nv is smallest (methods are contiguous, so this ends
+  // at one run per method at worst)
+  while ((int)runs.size() > UGKS_MAX_FACE_SEGMENTS) {
+    int best = -1;
+    for (int k = 0; k + 1 < (int)runs.size(); ++k)
+      if (runs[k].method == runs[k + 1].method &&
+          (best < 0 || std::max(runs[k].max_nv, runs[k + 1].max_nv) <
+                           std::max(runs[best].max_nv, runs[best + 1].max_nv)))
+        best = k;
+    if (best < 0) return -2;
+    runs[best].max_nv = std::max(runs[best].max_nv, runs[best + 1].max_nv);
+    runs[best].axes = std::max(runs[best].axes, runs[best + 1].axes);
+    runs[best].count += runs[best + 1].count;
+    runs.erase(runs.begin() + best + 1);
+  }
+  z->n_segments = (int32_t)runs.size();
+  for (int k = 0; k < UGKS_MAX_FACE_SEGMENTS; ++k) {
+    const bool on = k < (int)runs.size();
+    z->seg_begin[k] = on ? (int32_t)runs[k].begin : 0;
+    z->seg_count[k] = on ? (int32_t)runs[k].count : 0;
+    z->seg_method[k] = on ? runs[k].method : 0;
+    z->seg_max_nv[k] = on ? runs[k].max_nv : 0;
+    z->seg_max_axes[k] = on ? runs[k].axes : 0;
+  }
   for (int m = 0; m < 4; ++m) {
     z->face_begin[m] = (int32_t)fb[m];
     z->face_count[m] = (int32_t)fc[m];

@@ -935,12 +935,12 @@ extern "C" {
 const char *ugks_version(void) { return "ugks_b200 0.1 (sm_100a)"; }
 
 int ugks_abi_sizes(int64_t *out, int n) {
-  const int64_t v[6] = {(int64_t)sizeof(ugks_block_desc), (int64_t)sizeof(ugks_fused_block),
+  const int64_t v[7] = {(int64_t)sizeof(ugks_block_desc), (int64_t)sizeof(ugks_fused_block),
                         (int64_t)sizeof(ugks_solve_state), (int64_t)offsetof(ugks_fused_block, f),
                         (int64_t)offsetof(ugks_solve_state, residual),
-                        (int64_t)offsetof(ugks_block_desc, wall_D)};
-  for (int i = 0; i < n && i < 6; ++i) out[i] = v[i];
-  return 6;
+                        (int64_t)offsetof(ugks_block_desc, wall_D), (int64_t)sizeof(ugks_fused_sizes)};
+  for (int i = 0; i < n && i < 7; ++i) out[i] = v[i];
+  return 7;
 }
 
 int ugks_iFace(const ugks_block_desc *d, size_t g0, size_t g1, const double *Fin, double *iface_f,

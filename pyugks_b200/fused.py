@@ -22,7 +22,7 @@ import numpy as np
 
 from . import _lib
 from . import defs as D
-from .problem import Constants, fill_arrays, geometry, wall_values
+from .problem import Constants, VelocityGrid, fill_arrays, geometry, wall_values
 
 
 def _torch():
@@ -48,10 +48,12 @@ class FusedSolver:
         if isinstance(cases, dict):
             cases = [cases]
         cases = list(cases)
-        # solves are stored grouped by flux method (one face-pass launch per
-        # method covers a contiguous range); order[k] is the internal index
-        # of the caller's solve k
-        perm = sorted(range(len(cases)), key=lambda k: D.FLUX_METHODS[cases[k]["flux_method"]])
+        # solves are stored grouped by flux method, then by velocity-grid size
+        # (a face-pass launch covers a contiguous run of one method and one Nv,
+        # with shared memory sized for it); order[k] is the internal index of
+        # the caller's solve k
+        nvs = [VelocityGrid(c["quad"]).Nv for c in cases]
+        perm = sorted(range(len(cases)), key=lambda k: (D.FLUX_METHODS[cases[k]["flux_method"]], nvs[k], k))
         self.order = [0] * len(cases)
         for internal, k in enumerate(perm):
             self.order[k] = internal
@@ -140,6 +142,7 @@ class FusedSolver:
         blk.wall_fluxes = z(wl, 4, 8)
         blk.wall_dist = z(wl, Nv, 2)
         blk.cell_mom = z(Ni, Nj, 4)
+        blk.Q_next = z(ni, nj, 2)
         x = _lib.FusedBlock()
         d = x.d
         d.ni, d.nj, d.Ni, d.Nj, d.ghost, d.Nv = ni, nj, Ni, Nj, G, Nv
@@ -174,7 +177,7 @@ class FusedSolver:
         x.solve = s
         for name in ("f", "flux_S", "flux_W", "flux_macro_S", "flux_macro_W", "macro", "Q", "prim_old",
                      "area", "centre", "mid_side", "normal", "side_length", "xy", "wall_prop",
-                     "wall_cover", "wall_fluxes", "wall_dist", "cell_mom"):
+                     "wall_cover", "wall_fluxes", "wall_dist", "cell_mom", "Q_next"):
             setattr(x, name, getattr(blk, name).data_ptr())
         blk.struct = x
         return blk

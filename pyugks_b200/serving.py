@@ -44,7 +44,7 @@ def footprint_bytes(case: dict, precision: str) -> int:
     for b in case["blocks"]:
         Ni, Nj = b["ni"] + 2 * G, b["nj"] + 2 * G
         total += 3 * Ni * Nj * nv * 2 * es
-        total += Ni * Nj * 8 * (4 * 3 + 2 + 2 * 2 + 1 + 2 + 2 * 2 + 2)
+        total += Ni * Nj * 8 * (4 * 3 + 2 * 2 + 2 * 2 + 1 + 2 + 2 * 2 + 2)
         total += max(b["ni"], b["nj"]) * 4 * 8 * (4 + 4 + 8) + max(b["ni"], b["nj"]) * nv * 16
     return total
 
@@ -104,8 +104,10 @@ class SolvePool:
     def _rebuild(self):
         import torch
         self._sync_records()
-        # group by limiter, then admission order (ugks_fused_layout's rule)
-        order = sorted(self.solves, key=lambda sid: (D.FLUX_METHODS[self.solves[sid].case["flux_method"]], sid))
+        # group by limiter (ugks_fused_layout's rule), then by Nv (one face-pass
+        # launch per run), then admission order
+        order = sorted(self.solves, key=lambda sid: (D.FLUX_METHODS[self.solves[sid].case["flux_method"]],
+                                                     self.solves[sid].nv, sid))
         structs, records = [], []
         for k, sid in enumerate(order):
             s = self.solves[sid]
