@@ -262,7 +262,7 @@ def run_ours(args, rank, world, dist):
                      "step_frac": bpu * units / (t_max / args.steps / 1e3) / 1e9 / peak},
         "e2e": {"value": job_throughput(units, args.steps, world, e2e_ms), "unit": UNIT,
                 "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]},
-        "gpu_launches": 7 * args.steps,
+        "gpu_launches": solver.launches_per_step() * args.steps,
         "clocks": clocks,
     }
     if world == 1 and not args.no_cpu_baseline:

@@ -188,6 +188,14 @@ class FusedSolver:
         return s.cuda_stream
 
     # ---------------------------------------------------------------- stepping
+    def launches_per_step(self) -> int:
+        """Kernel launches of one ugks_step_* call: one face pass per
+        (limiter, Nv) segment, one retry pass per limiter present, two dt
+        checks, the cell pass, the dt update and the ghost pass."""
+        z = self.sizes
+        methods = sum(1 for m in range(4) if z.face_count[m] > 0)
+        return z.n_segments + methods + 2 + (1 if z.n_cells else 0) + 1 + (1 if z.n_ghost else 0)
+
     def step(self, n: int = 1):
         """Advance every active solve by n steps (asynchronous)."""
         for _ in range(n):
