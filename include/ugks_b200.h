@@ -305,6 +305,18 @@ int ugks_init_fp64(const ugks_fused_block *blocks_dev, int nblocks, const ugks_f
 int ugks_init_mixed(const ugks_fused_block *blocks_dev, int nblocks, const ugks_fused_sizes *sizes,
                     ugks_solve_state *solves_dev, int nsolves, UGKS_STREAM);
 
+/* Restart with saved distributions (UGKSBlock.initFunctions with a restart
+   file that holds f, ugks_block.py:274-300, 347-349, then ugks_sim.py:85-92):
+   f, macro and Q are the caller's (loaded into the block arrays beforehand);
+   wall_prop from the wall values, the fused path's per-cell moments and next
+   heat flux from f, ghosts filled, dt := CFL / max frequency of the loaded
+   macro.  `time` and `steps` of each solve record are left as the caller set
+   them.  (A restart without saved f is ugks_init_*: f := fEQ(macro, Q).) */
+int ugks_restart_fp64(const ugks_fused_block *blocks_dev, int nblocks, const ugks_fused_sizes *sizes,
+                      ugks_solve_state *solves_dev, int nsolves, UGKS_STREAM);
+int ugks_restart_mixed(const ugks_fused_block *blocks_dev, int nblocks, const ugks_fused_sizes *sizes,
+                       ugks_solve_state *solves_dev, int nsolves, UGKS_STREAM);
+
 /* One UGKSim.one_step (ugks_sim.py:407-501) of every active solve: flux
    pass, dt check with the reference's single retry, cell update, new dt,
    time advance, ghost update. */

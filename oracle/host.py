@@ -74,6 +74,31 @@ class OracleBlock:
         self.prg.calcQ(g, self.f, self.macro, self.Q)
         self.prg.paraBC((self.wall_len, 1), self.para, self.wall_prop, float(self.sim.time))
 
+    # ugks_block.py:274-300, 347-349, 411-432: macro and Q as saved (Q is the
+    # external heat flux the file holds, loaded without conversion); f as
+    # saved, or fEQ(macro, Q) with macro and Q then re-taken from f
+    def init_functions_restart(self, data):
+        self.sim.time = float(data["time"])
+        self.macro[:] = data["macro"]
+        self.Q[:] = data["Q"]
+        if data["f"] is not None:
+            self.f[:] = data["f"]
+        else:
+            g = (self.ni, self.nj)
+            self.prg.initFunctions(g, self.f, self.macro, self.Q)
+            self.prg.calcMacro(g, self.f, self.macro)
+            self.prg.calcQ(g, self.f, self.macro, self.Q)
+        self.prg.paraBC((self.wall_len, 1), self.para, self.wall_prop, float(self.sim.time))
+
+    # the datasets save_hdf writes (ugks_block.py:1441-1595), with Q from
+    # updateHost: calcQ of the current f and macro, in place, then times
+    # (4 + K) / 5 (ugks_block.py:1376-1386)
+    def save_data(self, with_f=True):
+        self.prg.calcQ((self.ni, self.nj), self.f, self.macro, self.Q)
+        return dict(macro=self.macro.copy(), Q_ext=self.Q * ((4.0 + self.sim.const.K) / 5.0),
+                    wall_prop=self.wall_prop.copy(), wall_cover=self.wall_cover.copy(),
+                    wall_fluxes=self.wall_fluxes.copy(), f=self.f.copy() if with_f else None)
+
     # ugks_block.py:621-665
     def update_bc(self):
         for face, bc in enumerate(self.bc_list):
@@ -206,12 +231,16 @@ class OracleBlock:
 class OracleSim:
     """``UGKSim`` restated for the time-step path."""
 
-    def __init__(self, case: dict, backend: str = "port", threads: int | None = None):
+    def __init__(self, case: dict, backend: str = "port", threads: int | None = None,
+                 restart: dict | None = None):
+        """restart: a loaded checkpoint ({'final_step', 'blocks': [dt, time,
+        macro, Q, f or None]}); UGKSim.restart (ugks_sim.py:824-840) sets the
+        step, UGKSBlock.initFunctions (ugks_block.py:274-300) the fields."""
         self.case = case
         self.const = us.Constants(case)
         self.time = 0.0
         self.dt = 0.0
-        self.step = 0
+        self.step = 0 if restart is None else int(restart["final_step"])
         self.force_time = False
         geoms = us.block_geometry(case, self.const.ghost)
         self.blocks = []
@@ -225,8 +254,11 @@ class OracleSim:
             self.blocks.append(OracleBlock(self, bid, b, g, prog))
         self.is_open = any(bc["type"] in (us.EXTRAPOLATE_OUT, us.INFLOW, us.OUTFLOW, us.CONSTANT)
                            for b in case["blocks"] for bc in b["bc"])
-        for blk in self.blocks:
-            blk.init_functions()
+        for k, blk in enumerate(self.blocks):
+            if restart is None:
+                blk.init_functions()
+            else:
+                blk.init_functions_restart(restart["blocks"][k])
         self.update_all_bc()
         self.calc_time_step()
         self.update_time_step(limit=False)

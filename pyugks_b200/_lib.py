@@ -113,7 +113,8 @@ def lib():
     L.ugks_array_max.argtypes = [vp, C.c_size_t, vp, vp]
     L.ugks_fused_layout.restype = C.c_int
     L.ugks_fused_layout.argtypes = [C.POINTER(FusedBlock), C.c_int, C.POINTER(FusedSizes)]
-    for nm in ("ugks_init_fp64", "ugks_init_mixed", "ugks_step_fp64", "ugks_step_mixed"):
+    for nm in ("ugks_init_fp64", "ugks_init_mixed", "ugks_restart_fp64", "ugks_restart_mixed",
+               "ugks_step_fp64", "ugks_step_mixed"):
         fn = getattr(L, nm)
         fn.restype = C.c_int
         fn.argtypes = [vp, C.c_int, C.POINTER(FusedSizes), vp, C.c_int, vp]

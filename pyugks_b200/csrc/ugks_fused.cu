@@ -1082,6 +1082,49 @@ __global__ void __launch_bounds__(FT) init_cells(const ugks_fused_block *__restr
   }
 }
 
+// restart from saved f, macro and Q (initFunctions with a restart file and
+// f present, ugks_block.py:274-300, 347-349): f and macro stay as loaded; the
+// fused path's own per-cell state is rebuilt from them (the moments of f for
+// the face pass, calcQ of f with the macro for the next cell pass) and the CFL
+// frequency of every cell is taken as at start-up (calcTimeStep)
+template <typename T>
+__global__ void __launch_bounds__(FT) restart_cells(const ugks_fused_block *__restrict__ B, int nb,
+                                                    ugks_solve_state *__restrict__ solves) {
+  __shared__ double scratch[6 * (FT / 32)];
+  using St = Store<T>;
+  const int w = blockIdx.x;
+  const int bi = find_block<1>(B, nb, w);
+  const ugks_fused_block &blk = B[bi];
+  const ugks_block_desc &d = blk.d;
+  ugks_solve_state &sol = solves[blk.solve];
+  if (!sol.active) return;
+  const int lc = w - blk.cell_begin;
+  const long mi = lc / d.nj, mj = lc % d.nj;
+  const size_t base = fidx(d, mi + d.ghost, mj + d.ghost, 0);
+  const P4 prim = ld4(blk.macro, midx(d, mi, mj));
+  const double Kinv = 1.0 / d.K;
+  double m[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+  for (int v = threadIdx.x; v < d.Nv; v += FT) {
+    const V2 f = St::load(blk.f, base + v);
+    const V2 e = quad_at(d, v);
+    m[0] += f.x;
+    m[1] = fma(e.x, f.x, m[1]);
+    m[2] = fma(e.y, f.x, m[2]);
+    m[3] += fma(fma(e.x, e.x, e.y * e.y), f.x, f.y);
+    const double cx = e.x - prim.s1, cy = e.y - prim.s2;
+    const double t = fma(fma(cx, cx, cy * cy), f.x, f.y * Kinv);
+    m[4] = fma(cx, t, m[4]);
+    m[5] = fma(cy, t, m[5]);
+  }
+  block_sum<6>(m, scratch);
+  if (threadIdx.x == 0) {
+    st4(blk.cell_mom, gidx(d, mi + d.ghost, mj + d.ghost), p4(m[0], m[1], m[2], 0.5 * m[3]));
+    st2(blk.Q_next, midx(d, mi, mj), v2(0.5 * m[4], 0.5 * m[5]));
+    const double fq = cfl_freq(blk, prim, mi, mj);
+    atomicMax(&sol.max_freq, (unsigned long long)__double_as_longlong(fq));
+  }
+}
+
 // paraBC (clKernel.c:141-218) for constant wall values, every block
 __global__ void init_walls(const ugks_fused_block *B, int nb) {
   const ugks_fused_block &blk = B[blockIdx.x];
@@ -1114,6 +1157,17 @@ int init_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
   cudaStream_t st = S(stream);
   init_walls<<<nb, 128, 0, st>>>(B, nb);
   if (z->n_cells) init_cells<T><<<z->n_cells, FT, 0, st>>>(B, nb, solves);
+  dt_init<<<(ns + 127) / 128, 128, 0, st>>>(solves, ns);
+  if (z->n_ghost) ghost_pass<T><<<z->n_ghost, FT, 0, st>>>(B, nb, solves);
+  return launch_status();
+}
+
+template <typename T>
+int restart_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks_solve_state *solves,
+                 int ns, void *stream) {
+  cudaStream_t st = S(stream);
+  init_walls<<<nb, 128, 0, st>>>(B, nb);
+  if (z->n_cells) restart_cells<T><<<z->n_cells, FT, 0, st>>>(B, nb, solves);
   dt_init<<<(ns + 127) / 128, 128, 0, st>>>(solves, ns);
   if (z->n_ghost) ghost_pass<T><<<z->n_ghost, FT, 0, st>>>(B, nb, solves);
   return launch_status();
@@ -1352,6 +1406,14 @@ int ugks_init_fp64(const ugks_fused_block *blocks_dev, int nblocks, const ugks_f
 int ugks_init_mixed(const ugks_fused_block *blocks_dev, int nblocks, const ugks_fused_sizes *sizes,
                     ugks_solve_state *solves_dev, int nsolves, void *stream) {
   return init_impl<float>(blocks_dev, nblocks, sizes, solves_dev, nsolves, stream);
+}
+int ugks_restart_fp64(const ugks_fused_block *blocks_dev, int nblocks, const ugks_fused_sizes *sizes,
+                      ugks_solve_state *solves_dev, int nsolves, void *stream) {
+  return restart_impl<double>(blocks_dev, nblocks, sizes, solves_dev, nsolves, stream);
+}
+int ugks_restart_mixed(const ugks_fused_block *blocks_dev, int nblocks, const ugks_fused_sizes *sizes,
+                       ugks_solve_state *solves_dev, int nsolves, void *stream) {
+  return restart_impl<float>(blocks_dev, nblocks, sizes, solves_dev, nsolves, stream);
 }
 
 }  // extern "C"

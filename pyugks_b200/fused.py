@@ -21,6 +21,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
+from . import checkpoint
 from . import defs as D
 from .problem import Constants, VelocityGrid, fill_arrays, geometry, wall_values
 
@@ -35,7 +36,11 @@ class _Block:
 
 
 class FusedSolver:
-    def __init__(self, cases, precision: str = "fp64", device="cuda", stream=None):
+    def __init__(self, cases, precision: str = "fp64", device="cuda", stream=None, restart=None):
+        """restart: {caller's solve index: checkpoint path or the dict of
+        checkpoint.read}; those solves resume from the saved state (the
+        reference's restart, ugks_sim.py:824-840, ugks_block.py:274-300)
+        instead of starting from their fill condition."""
         torch = _torch()
         if precision not in ("fp64", "mixed"):
             raise ValueError(precision)
@@ -95,12 +100,42 @@ class FusedSolver:
             st[s].active = 1
             st[s].nblocks = len(self.solve_blocks[s])
             st[s].first_block = self.solve_blocks[s][0]
+        # restarts: load the saved state into the block arrays
+        with_f = set()
+        for k, ck in (restart or {}).items():
+            s = self.order[k]
+            data = ck if isinstance(ck, dict) else checkpoint.read(ck)
+            if len(data["blocks"]) != len(self.solve_blocks[s]):
+                raise ValueError("checkpoint has %d blocks, solve %d has %d"
+                                 % (len(data["blocks"]), k, len(self.solve_blocks[s])))
+            for bi, bd in zip(self.solve_blocks[s], data["blocks"]):
+                blk = self.blocks[bi]
+                if bd["macro"].shape != tuple(blk.macro.shape):
+                    raise ValueError("checkpoint block shape %s != %s" % (bd["macro"].shape, tuple(blk.macro.shape)))
+                blk.macro.copy_(self._dev(bd["macro"]))
+                blk.Q.copy_(self._dev(bd["Q"]))
+                if bd["f"] is not None:
+                    blk.f.copy_(self._dev(bd["f"], self.sdtype))
+                    with_f.add(s)
+            st[s].time = data["blocks"][0]["time"]
+            st[s].steps = int(data["final_step"])
         self.solves = torch.from_numpy(np.frombuffer(bytes(st), dtype=np.uint8).copy()).to(self.device)
         self.nsolves = len(self.cases)
         self._stream = stream
         init = self.lib.ugks_init_fp64 if precision == "fp64" else self.lib.ugks_init_mixed
-        _lib.check(init(self.table.data_ptr(), self.nblocks, C.byref(self.sizes),
-                        self.solves.data_ptr(), self.nsolves, self._sptr()), "ugks_init")
+        rst = self.lib.ugks_restart_fp64 if precision == "fp64" else self.lib.ugks_restart_mixed
+        args = lambda: (self.table.data_ptr(), self.nblocks, C.byref(self.sizes), self.solves.data_ptr(),
+                        self.nsolves, self._sptr())
+        if not with_f:
+            _lib.check(init(*args()), "ugks_init")
+        else:
+            # solves restarted with saved f skip the equilibrium start-up
+            self._set_active_internal([s not in with_f for s in range(self.nsolves)])
+            if len(with_f) < self.nsolves:
+                _lib.check(init(*args()), "ugks_init")
+            self._set_active_internal([s in with_f for s in range(self.nsolves)])
+            _lib.check(rst(*args()), "ugks_restart")
+            self._set_active_internal([True] * self.nsolves)
         self._step_fn = self.lib.ugks_step_fp64 if precision == "fp64" else self.lib.ugks_step_mixed
         self.graph = None
 
@@ -238,11 +273,35 @@ class FusedSolver:
 
     def set_active(self, flags):
         """Switch solves on/off for the next steps (device-side flag)."""
+        self._set_active_internal([flags[k] for k in sorted(range(self.nsolves), key=lambda k: self.order[k])])
+
+    def _set_active_internal(self, flags):
         torch = _torch()
+        torch.cuda.synchronize(self.device)  # the solve records may be written on another stream
         st = (_lib.SolveState * self.nsolves).from_buffer_copy(self.solves.cpu().numpy().tobytes())
-        for k, a in enumerate(flags):
-            st[self.order[k]].active = 1 if a else 0
+        for s, a in enumerate(flags):
+            st[s].active = 1 if a else 0
         self.solves.copy_(torch.from_numpy(np.frombuffer(bytes(st), dtype=np.uint8).copy()))
+
+    def save_checkpoint(self, path: str, solve: int = 0, save_f: bool = True):
+        """Write one solve's state as a checkpoint (checkpoint.py; the
+        reference's saveHDF5 + close_HDF5, ugks_sim.py:1022-1096)."""
+        s = self.order[solve]
+        state = self.solve_state()[solve]
+        const = Constants(self.cases[s])
+        blocks = []
+        for k, bi in enumerate(self.solve_blocks[s]):
+            b = self.blocks[bi]
+            m = b.macro.cpu().numpy()
+            f_full = b.f.cpu().numpy()
+            q = self._heat_flux(b, f_full[b.G:-b.G, b.G:-b.G].astype(np.float64), m)
+            blocks.append(checkpoint.block_datasets(
+                k, state["dt"], state["time"], m, checkpoint.external_heat_flux(q, const.K),
+                b.wall_prop.cpu().numpy(), b.wall_cover.cpu().numpy(), b.wall_fluxes.cpu().numpy(),
+                f_full if save_f else None))
+        meta = dict(Nv=const.Nv, K=const.K, CFL=float(self.cases[s]["CFL"]), quad=const.vgrid.quad,
+                    weight=const.vgrid.weight)
+        checkpoint.write(path, state["steps"], blocks, meta)
 
     def fields(self, solve: int = 0):
         """Per block interior fields of one solve (caller's index) as numpy:

@@ -91,12 +91,30 @@ class UGKSBlock:
         self.face_lengths = [Ls[G:-G, -G, 0], Ls[-G, G:-G, 1], Ls[G:-G, G, 0], Ls[G, G:-G, 1]]
 
     # ------------------------------------------------------------------ init
-    def initFunctions(self):
+    def initFunctions(self, restart=None):
+        """ugks_block.py:258-432.  restart: this block's entry of a loaded
+        checkpoint (macro, Q as saved, f or None): macro and Q are taken as
+        saved (Q without conversion, as the reference loads it), and f too
+        when present; otherwise f := fEQ(macro, Q) and macro, Q re-taken from
+        f."""
         gs, ws = _m_tuple((self.ni, self.nj, 1), (1, 1, 1))
-        self.prg.initFunctions(self.queue, gs, ws, self.f_D, self.macro_D, self.Q_D)
-        self.prg.calcMacro(self.queue, gs, ws, self.f_D, self.macro_D)
-        self.prg.calcQ(self.queue, gs, ws, self.f_D, self.macro_D, self.Q_D)
+        init_f = True
+        if restart is not None:
+            self.sim.time = float(restart["time"])
+            self.macro_D.copy_(self._t(restart["macro"]))
+            self.Q_D.copy_(self._t(restart["Q"]))
+            if restart["f"] is not None:
+                self.f_D.copy_(self._t(restart["f"]))
+                init_f = False
+        if init_f:
+            self.prg.initFunctions(self.queue, gs, ws, self.f_D, self.macro_D, self.Q_D)
+            self.prg.calcMacro(self.queue, gs, ws, self.f_D, self.macro_D)
+            self.prg.calcQ(self.queue, gs, ws, self.f_D, self.macro_D, self.Q_D)
         self.parametricBC(force=True)
+
+    def _t(self, a):
+        import torch
+        return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(self.f_D.device)
 
     def parametricBC(self, force=False):
         if force:

@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import numpy as np
 
+from . import checkpoint
 from . import defs as D
 from .desc import VelocityTables
 from .problem import Constants, geometry
@@ -20,7 +21,10 @@ from .ugks_block import UGKSBlock
 
 
 class UGKSim:
-    def __init__(self, case: dict, device="cuda", queue=None):
+    def __init__(self, case: dict, device="cuda", queue=None, restart=None):
+        """restart: checkpoint path (or the dict of checkpoint.read) to resume
+        from, as the reference's ``gdata.restart`` (``restart``,
+        ugks_sim.py:824-840)."""
         import torch
         self.case = case
         self.const = Constants(case)
@@ -31,7 +35,9 @@ class UGKSim:
         self.Kn_eff = float(case["Kn_eff"])
         self.dt = 0.0
         self.time = 0.0
-        self.step = 0
+        if restart is not None and not isinstance(restart, dict):
+            restart = checkpoint.read(restart)
+        self.step = 0 if restart is None else int(restart["final_step"])
         self.force_time = False
         self.tabs = VelocityTables(self.const, self.device)
         geoms = geometry(case, self.const.ghost)
@@ -39,8 +45,8 @@ class UGKSim:
                        for k, (b, g) in enumerate(zip(case["blocks"], geoms))]
         self.is_open = any(bc["type"] in (D.EXTRAPOLATE_OUT, D.INFLOW, D.OUTFLOW, D.CONSTANT)
                            for b in case["blocks"] for bc in b["bc"])
-        for b in self.blocks:
-            b.initFunctions()
+        for k, b in enumerate(self.blocks):
+            b.initFunctions(None if restart is None else restart["blocks"][k])
         self.updateAllBC()
         self.calcTimeStep()
         self.updateTimeStep(limit=False)
@@ -133,6 +139,23 @@ class UGKSim:
             out.append(dict(rho=m[:, :, 0], U=m[:, :, 1], V=m[:, :, 2], T=1.0 / m[:, :, 3],
                             qx=q[:, :, 0], qy=q[:, :, 1]))
         return out
+
+    def save_checkpoint(self, path: str, save_f: bool = True):
+        """saveHDF5 + close_HDF5 (ugks_sim.py:1022-1096) into one .npz:
+        per block the fields with Q re-taken from f as updateHost does
+        (ugks_block.py:1376-1386), wall data and optionally f."""
+        import torch
+        blocks = []
+        for k, b in enumerate(self.blocks):
+            b.prg.calcQ(self.queue, (b.ni, b.nj, 1), None, b.f_D, b.macro_D, b.Q_D)
+            q = b.Q_D.cpu().numpy()
+            blocks.append(checkpoint.block_datasets(
+                k, self.dt, self.time, b.macro_D.cpu().numpy(), checkpoint.external_heat_flux(q, self.const.K),
+                b.wall_prop_D.cpu().numpy(), b.wall_cover_D.cpu().numpy(), b.wall_fluxes_D.cpu().numpy(),
+                b.f_D.cpu().numpy() if save_f else None))
+        meta = dict(Nv=self.const.Nv, K=self.const.K, CFL=self.CFL, quad=self.const.vgrid.quad,
+                    weight=self.const.vgrid.weight)
+        checkpoint.write(path, self.step, blocks, meta)
 
     def interior_f(self):
         return [b.f_D[b.ghost:-b.ghost, b.ghost:-b.ghost].cpu().numpy() for b in self.blocks]
