@@ -368,6 +368,10 @@ int ugks_residual(const ugks_fused_block *blocks_dev, int nblocks, ugks_solve_st
 int ugks_getDT_noalloc(const ugks_block_desc *d, const double *xy, const double *area,
                        const double *macro, double Kn, double *max_freq, UGKS_STREAM);
 
+/* Kernel launches one ugks_step_fp64 (mixed = 0) or ugks_step_mixed
+   (mixed = 1) call makes for a block table of these sizes. */
+int ugks_step_launches(const ugks_fused_sizes *sizes, int mixed);
+
 /* Library identification: returns a static version string. */
 const char *ugks_version(void);
 /* sizeof(ugks_block_desc), sizeof(ugks_fused_block), sizeof(ugks_solve_state),

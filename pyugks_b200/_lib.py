@@ -120,6 +120,8 @@ def lib():
         fn.argtypes = [vp, C.c_int, C.POINTER(FusedSizes), vp, C.c_int, vp]
     L.ugks_step_profiled.restype = C.c_int
     L.ugks_step_profiled.argtypes = [C.c_int, vp, C.c_int, C.POINTER(FusedSizes), vp, C.c_int, vp, vp]
+    L.ugks_step_launches.restype = C.c_int
+    L.ugks_step_launches.argtypes = [C.POINTER(FusedSizes), C.c_int]
     L.ugks_residual.restype = C.c_int
     L.ugks_residual.argtypes = [vp, C.c_int, vp, C.c_int, vp]
     L.ugks_getDT_noalloc.restype = C.c_int

@@ -1312,6 +1312,18 @@ int ugks_step_profiled(int mixed, const ugks_fused_block *blocks_dev, int nblock
   return mixed ? step_impl<float>(blocks_dev, nblocks, sizes, solves_dev, nsolves, stream, events)
                : step_impl<double>(blocks_dev, nblocks, sizes, solves_dev, nsolves, stream, events);
 }
+int ugks_step_launches(const ugks_fused_sizes *z, int mixed) {
+  (void)mixed;  // the same kernels run in both precisions
+  int n = 0;
+  for (int k = 0; k < z->n_segments && k < UGKS_MAX_FACE_SEGMENTS; ++k) n += z->seg_count[k] > 0 ? 1 : 0;
+  for (int m = 0; m < 4; ++m) n += z->face_count[m] > 0 ? 1 : 0;  // retry passes
+  n += 2;                                                          // dt checks
+  n += z->n_cells ? 1 : 0;
+  n += 1;                                                          // dt update
+  n += z->n_ghost ? 1 : 0;
+  return n;
+}
+
 int ugks_residual(const ugks_fused_block *blocks_dev, int nblocks, ugks_solve_state *solves_dev,
                   int nsolves, void *stream) {
   if (nsolves <= 0) return 0;

@@ -224,12 +224,11 @@ class FusedSolver:
 
     # ---------------------------------------------------------------- stepping
     def launches_per_step(self) -> int:
-        """Kernel launches of one ugks_step_* call: one face pass per
-        (limiter, Nv) segment, one retry pass per limiter present, two dt
-        checks, the cell pass, the dt update and the ghost pass."""
-        z = self.sizes
-        methods = sum(1 for m in range(4) if z.face_count[m] > 0)
-        return z.n_segments + methods + 2 + (1 if z.n_cells else 0) + 1 + (1 if z.n_ghost else 0)
+        """Kernel launches of one ugks_step_* call (ugks_step_launches): one
+        face pass per (limiter, Nv) segment, one retry pass per limiter
+        present, two dt checks, the cell pass, the dt update and the ghost
+        pass."""
+        return self.lib.ugks_step_launches(C.byref(self.sizes), 0 if self.precision == "fp64" else 1)
 
     def step(self, n: int = 1):
         """Advance every active solve by n steps (asynchronous)."""
