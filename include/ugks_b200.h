@@ -64,7 +64,16 @@ typedef struct ugks_block_desc {
      (ugks_data.py:287-292); u_num * v_num == Nv lets the fused kernels
      factor the Maxwellian exponential; 0 for an unstructured set */
   int32_t u_num, v_num;
+  /* adsorbing-wall re-emission per face: UGKS_REFLECT_SPECULAR (the
+     reference's default 'S'), _DIFFUSE ('D') or _CL (Cercignani-Lampis with
+     accommodation ALPHA_N, ALPHA_T; ugks_CL.py:134-148, 255-273) */
+  double alpha_n[4], alpha_t[4];
+  int32_t reflect[4];
 } ugks_block_desc;
+
+#define UGKS_REFLECT_SPECULAR 0
+#define UGKS_REFLECT_DIFFUSE 1
+#define UGKS_REFLECT_CL 2
 
 /* ------------------------------------------------------------------------
  * 1. Drop-in kernels (reference: source/clUGKS.c, clKernel.c,
@@ -197,6 +206,16 @@ int ugks_adsorbingWallD_P2(const ugks_block_desc *d, size_t g0, size_t g1, const
                            int face, const double *wall_prop, const double *wall_cover,
                            const double *wall_dist, double *flux_f, const double *macro,
                            double dt, UGKS_STREAM);
+/* clAdsorb.c:656-816: specular re-emission of the reflected flux */
+int ugks_adsorbingWallS_P2(const ugks_block_desc *d, size_t g0, size_t g1, const double *normal,
+                           int face, const double *wall_prop, const double *wall_cover,
+                           const double *wall_dist, double *flux_f, const double *macro,
+                           double dt, UGKS_STREAM);
+/* clAdsorb.c:488-651: Cercignani-Lampis re-emission of the reflected flux */
+int ugks_adsorbingWallCL_P2(const ugks_block_desc *d, size_t g0, size_t g1, const double *normal,
+                            int face, const double *wall_prop, const double *wall_cover,
+                            const double *wall_dist, double *flux_f, const double *macro,
+                            double dt, UGKS_STREAM);
 
 /* ------------------------------------------------------------------------
  * 2. Fused step.

@@ -133,10 +133,11 @@ class OracleBlock:
                                       self.wall_dist, flux, self.macro, dt, self.flag)
             if self.flag[0] == 4.0:
                 return True
-            if bc.get("reflect_type", "S") != "D":
-                raise NotImplementedError("only diffuse re-emission is restated")
-            self.prg.adsorbingWallD_P2(gsize, self.normal, wall, self.wall_prop, self.wall_cover,
-                                       self.wall_dist, flux, self.macro, dt)
+            # re-emission by reflect_type (ugks_block.py:952-969; 'S' unless 'CL' or 'D')
+            rtype = bc.get("reflect_type", "S")
+            p2 = (self.prg.adsorbingWallCL_P2 if rtype == "CL" else
+                  self.prg.adsorbingWallD_P2 if rtype == "D" else self.prg.adsorbingWallS_P2)
+            p2(gsize, self.normal, wall, self.wall_prop, self.wall_cover, self.wall_dist, flux, self.macro, dt)
         self.prg.wallFlux(gsize, self.normal, self.length, wall, flux, flux_macro, dt)
         self.prg.wallMassEnergyFluxes(gsize, self.normal, self.length, self.area, wall, flux,
                                       self.wall_fluxes, dt)

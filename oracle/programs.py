@@ -37,6 +37,7 @@ SIGNATURES = {
     "edgeConstant": "pip", "edgeInflow": "pipppp", "edgeOutflow": "pipppp",
     "edgeMirror": "pi", "edgeBounceBack": "pi", "edgeConstGrad": "pi",
     "adsorbingWall_P1": "pipppppdp", "adsorbingWallD_P2": "pipppppd",
+    "adsorbingWallS_P2": "pipppppd", "adsorbingWallCL_P2": "pipppppd",
 }
 _CT = {"p": C.c_void_p, "i": C.c_int, "d": C.c_double}
 
@@ -143,6 +144,7 @@ class _PortParams(C.Structure):
         ("beta_n", C.c_double * 4), ("beta_t", C.c_double * 4), ("gamma_f", C.c_double * 4),
         ("alpha_p", C.c_double * 4), ("dynamic", C.c_int * 4), ("constant_adsorb", C.c_int * 4),
         ("adsorb", C.c_double * 4), ("k_des", C.c_double * 4),
+        ("alpha_n", C.c_double * 4), ("alpha_t", C.c_double * 4),
     ]
 
 
@@ -181,8 +183,11 @@ class PortProgram(_Program):
                 p.constant_adsorb[f] = 1 if np.ndim(bc["adsorb"]) == 0 else 0
                 p.adsorb[f] = float("%g" % bc["adsorb"]) if np.ndim(bc["adsorb"]) == 0 else 0.0
                 p.k_des[f] = float(bc.get("k_des", 0.0))
+                p.alpha_n[f] = us.e15(bc.get("alpha_n", 0.0))
+                p.alpha_t[f] = us.e15(bc.get("alpha_t", 0.0))
             else:
                 p.beta_n[f] = p.beta_t[f] = p.gamma_f[f] = p.alpha_p[f] = -1.0
+                p.alpha_n[f] = p.alpha_t[f] = -1.0
                 p.dynamic[f] = -1
         self._params = p
         super().__init__(PortProgram._lib, "port_", bind=(C.cast(C.pointer(p), C.c_void_p),))

@@ -1112,6 +1112,161 @@ void port_adsorbingWall_P1(PP, size_t g0, size_t g1, const double *normal, int f
     }
 }
 
+/* the second half of adsorbingWall{S,CL,D}_P2 (clAdsorb.c:601-649, 766-814,
+   931-973): scale the re-emitted half by `ratio` and add the desorbed
+   particles as a wall Maxwellian of density 2 des sqrt(pi lambda_w) */
+static void add_desorbed(PP, double *flux_f, size_t gi, size_t gj, d2 n, int rot, d4 wall, const double *cover,
+                         double ratio) {
+  double refl = cover[1], des = cover[3], ads = cover[2];
+  size_t account = ((des == 0.0) && (ads > 0.0) && (refl == 0.0)) ? 1 : 0;
+  wall.s0 = 2 * des * sqrt(P->PI * wall.s3);
+  for (size_t v = 0; v < (size_t)P->Nv; ++v) {
+    d2 uv = face_velocity(P, v, n);
+    int delta = (int)((ocl_sign(uv.x) * rot + 1) / 2);
+    d2 fd = ld2(flux_f, FIDX(gi, gj, v));
+    double sc = 1 - delta * (1 - ratio);
+    fd.x *= sc;
+    fd.y *= sc;
+    d2 M = maxwellian(P, wall, uv, v);
+    fd.x += delta * M.x;
+    fd.y += delta * M.y;
+    fd.x -= account * delta * fd.x;
+    fd.y -= account * delta * fd.y;
+    st2(flux_f, FIDX(gi, gj, v), fd);
+  }
+}
+
+/* adsorbingWallS_P2 (clAdsorb.c:656-816): the reflected part of the
+   incoming flux is re-emitted specularly, through the velocity mirrored
+   about the wall (mirror_EW on WEST/EAST faces, mirror_NS on SOUTH/NORTH;
+   axis-aligned walls only, as in the reference) */
+void port_adsorbingWallS_P2(PP, size_t g0, size_t g1, const double *normal, int face,
+                            const double *wall_prop, const double *wall_cover, const double *wall_dist,
+                            double *flux_f, const double *macro, double dt) {
+  (void)macro; (void)dt;
+  for (size_t a = 0; a < g0; ++a)
+    for (size_t b = 0; b < g1; ++b) {
+      size_t gi = a, gj = b, ci;
+      int rot, fid;
+      wall_face(P, face, &gi, &gj, &ci, &rot, &fid);
+      if (!wall_in_range(P, fid, gi, gj)) continue;
+      d2 n = ld2(normal, FACEIDX(gi, gj, fid));
+      d4 wall = ld4(wall_prop, ci * 4 + face);
+      d2 wv = {wall.s1, wall.s2};
+      wv = to_local(wv, n);
+      wall.s1 = wv.x;
+      wall.s2 = wv.y;
+      const double *cover = wall_cover + 4 * (ci * 4 + face);
+      double refl = cover[1];
+      double ratio = 1.0;
+      if (refl > 0.0) {
+        double s = 0.0;
+        for (size_t v = 0; v < (size_t)P->Nv; ++v) {
+          d2 uv = face_velocity(P, v, n);
+          int delta = (int)((ocl_sign(uv.x) * rot + 1) / 2);
+          d2 spec = {0.0, 0.0};
+          if (delta) {
+            size_t mv = (size_t)(fid == WEST ? P->mirror_EW[v] : P->mirror_NS[v]);
+            spec = ld2(wall_dist, ci * P->Nv + mv);
+          }
+          d2 fd = ld2(flux_f, FIDX(gi, gj, v));
+          d2 out = {delta * spec.x + (1 - delta) * fd.x, delta * spec.y + (1 - delta) * fd.y};
+          st2(flux_f, FIDX(gi, gj, v), out);
+          s += rot * uv.x * spec.x;
+        }
+        ratio = refl / s;
+      }
+      add_desorbed(P, flux_f, gi, gj, n, rot, wall, cover, ratio);
+    }
+}
+
+/* modified Bessel function I0 by its power series sum_k ((x/2)^2)^k / (k!)^2
+   (all terms positive; the reference evaluates I0 by Blair's rational
+   Chebyshev approximation, clFunctions.c:88-145, which agrees to rounding) */
+static double bessel_i0(double x) {
+  const double y = 0.25 * x * x;
+  double term = 1.0, sum = 1.0;
+  for (int k = 1; k < 1000; ++k) {
+    term *= y / ((double)k * (double)k);
+    sum += term;
+    if (term < 1e-17 * sum) break;
+  }
+  return sum;
+}
+
+/* scatterNormal, scatterTangential, CercignaniLampis (clFunctions.c:146-185) */
+static double scatter_normal(PP, double c_in, double c_out, double an, double Tw) {
+  (void)P;
+  return (2.0 / (an * Tw)) * fabs(c_out) * bessel_i0(((2 * sqrt(1 - an)) / (an * Tw)) * c_in * c_out) *
+         exp(-(c_out * c_out + (1 - an) * c_in * c_in) / (an * Tw));
+}
+static double scatter_tangential(PP, double c_in, double c_out, double at, double Tw) {
+  double a = c_out - (1 - at) * c_in;
+  return (1.0 / sqrt(P->PI * at * (2 - at) * Tw)) * exp(-(a * a) / (at * (2 - at) * Tw));
+}
+static d2 cercignani_lampis(PP, d2 uv_in, d2 uv_out, d2 f_in, double an, double at, double Tw) {
+  double k = fabs(uv_in.x / uv_out.x) * scatter_normal(P, uv_in.x, uv_out.x, an, Tw) *
+             scatter_tangential(P, uv_in.y, uv_out.y, at, Tw);
+  d2 r = {k * f_in.x, k * f_in.y};
+  r.y *= (1 - at) * (1 - at);
+  return r;
+}
+
+/* adsorbingWallCL_P2 (clAdsorb.c:488-651): the reflected part of the
+   incoming flux is re-emitted through the Cercignani-Lampis kernel, an
+   O(Nv^2) sum over incoming velocities per outgoing velocity */
+void port_adsorbingWallCL_P2(PP, size_t g0, size_t g1, const double *normal, int face,
+                             const double *wall_prop, const double *wall_cover, const double *wall_dist,
+                             double *flux_f, const double *macro, double dt) {
+  (void)macro; (void)dt;
+  for (size_t a = 0; a < g0; ++a)
+    for (size_t b = 0; b < g1; ++b) {
+      size_t gi = a, gj = b, ci;
+      int rot, fid;
+      wall_face(P, face, &gi, &gj, &ci, &rot, &fid);
+      if (!wall_in_range(P, fid, gi, gj)) continue;
+      d2 n = ld2(normal, FACEIDX(gi, gj, fid));
+      d4 wall = ld4(wall_prop, ci * 4 + face);
+      d2 wv = {wall.s1, wall.s2};
+      wv = to_local(wv, n);
+      wall.s1 = wv.x;
+      wall.s2 = wv.y;
+      const double *cover = wall_cover + 4 * (ci * 4 + face);
+      double refl = cover[1];
+      double ratio = 1.0;
+      const double an = P->alpha_n[face], at = P->alpha_t[face];
+      if (refl > 0.0) {
+        double s = 0.0;
+        for (size_t v = 0; v < (size_t)P->Nv; ++v) {
+          d2 uv_out = face_velocity(P, v, n);
+          int delta = (int)((ocl_sign(uv_out.x) * rot + 1) / 2);
+          d2 cl_v = {0.0, 0.0};
+          if (delta) {
+            for (size_t va = 0; va < (size_t)P->Nv; ++va) {
+              d2 uv_in = face_velocity(P, va, n);
+              int delta_in = (int)((ocl_sign(uv_in.x) * rot + 1) / 2);
+              if ((!delta_in) && (uv_in.x != 0.0)) {
+                d2 cl = cercignani_lampis(P, uv_in, uv_out, ld2(wall_dist, ci * P->Nv + va), an, at,
+                                          1.0 / wall.s3);
+                cl.y += 0.5 * at * (2 - at) / wall.s3 * cl.x;
+                cl_v.x += cl.x;
+                cl_v.y += cl.y;
+              }
+            }
+            cl_v.x *= P->weight[v];
+            cl_v.y *= P->weight[v];
+          }
+          d2 fd = ld2(flux_f, FIDX(gi, gj, v));
+          d2 out = {delta * cl_v.x + (1 - delta) * fd.x, delta * cl_v.y + (1 - delta) * fd.y};
+          st2(flux_f, FIDX(gi, gj, v), out);
+          s += rot * uv_out.x * cl_v.x;
+        }
+        ratio = refl / s;
+      }
+      add_desorbed(P, flux_f, gi, gj, n, rot, wall, cover, ratio);
+    }
+}
+
 /* adsorbingWallD_P2 (clAdsorb.c:821-975): diffuse re-emission of the
    reflected flux plus the desorbed particles */
 void port_adsorbingWallD_P2(PP, size_t g0, size_t g1, const double *normal, int face,

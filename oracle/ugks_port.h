@@ -34,6 +34,8 @@ typedef struct {
   /* first-order desorption rate per face; 0 selects the reference's
      Langmuir-driven desorption (clAdsorb.c:436-438) */
   double k_des[4];
+  /* Cercignani-Lampis accommodation (ALPHA_N, ALPHA_T, ugks_CL.py:134-148) */
+  double alpha_n[4], alpha_t[4];
 } ugks_port_params;
 
 #endif

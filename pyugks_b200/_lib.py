@@ -30,6 +30,7 @@ class BlockDesc(C.Structure):
         ("adsorb", f64 * 4), ("k_des", f64 * 4),
         ("dynamic", i32 * 4), ("constant_adsorb", i32 * 4),
         ("u_num", i32), ("v_num", i32),
+        ("alpha_n", f64 * 4), ("alpha_t", f64 * 4), ("reflect", i32 * 4),
     ]
 
 
@@ -80,6 +81,7 @@ KERNEL_SIGNATURES = {
     "edgeConstant": "pip", "edgeInflow": "pipppp", "edgeOutflow": "pipppp",
     "edgeMirror": "pi", "edgeBounceBack": "pi", "edgeConstGrad": "pi",
     "adsorbingWall_P1": "pipppppdp", "adsorbingWallD_P2": "pipppppd",
+    "adsorbingWallS_P2": "pipppppd", "adsorbingWallCL_P2": "pipppppd",
 }
 _CT = {"p": vp, "i": C.c_int, "d": f64}
 

@@ -63,15 +63,19 @@ def reflect():
 
 
 def adsorbing(T=1.0, gamma_f=0.5, k_des=0.01, adsorb=0.5, S_T=1.0, reflect_type="D",
-              cover_initial=0.0, beta_n=0.0, beta_t=0.0):
+              cover_initial=0.0, beta_n=0.0, beta_t=0.0, alpha_n=1.0, alpha_t=1.0):
     """``AdsorbingBC`` (``geom/geom_bc_defs.py:355-414``) with the extra
     first-order desorption rate ``k_des`` (per unit time; 0 restores the
     reference's Langmuir-driven desorption, which needs ``adsorb``).  With
     reference values of 1, ``alpha_p = 1/S_T`` and ``gamma_f = S_T k_f``
-    (``ugks_data.py:516-518``)."""
+    (``ugks_data.py:516-518``).  ``reflect_type`` re-emits the reflected flux
+    specularly ('S', the reference's default), diffusely ('D') or through
+    the Cercignani-Lampis kernel ('CL', accommodation ``alpha_n``,
+    ``alpha_t``)."""
     return dict(type=D.ADSORBING, D=1.0, T=T, U=0.0, V=0.0, gamma_f=gamma_f, alpha_p=1.0 / S_T,
                 S_T=S_T, beta_n=beta_n, beta_t=beta_t, adsorb=adsorb, dynamic=1,
-                reflect_type=reflect_type, cover_initial=cover_initial, k_des=k_des)
+                reflect_type=reflect_type, cover_initial=cover_initial, k_des=k_des,
+                alpha_n=alpha_n, alpha_t=alpha_t)
 
 
 def base_case(flux_method, Kn, m, vlim, CFL=0.8):
@@ -130,7 +134,7 @@ def cavity_multiblock(nb=2, n=64, m=32, vlim=5.0, flux_method="WENO5", Kn=0.01, 
 
 def channel(nblocks=4, n=64, m=32, vlim=5.0, flux_method="WENO5", Kn=0.05, rho_in=1.2,
             rho_out=1.0, length=4.0, height=1.0, gamma_f=0.5, k_des=0.01, CFL=0.3, nj=None,
-            adsorb=0.5):
+            adsorb=0.5, reflect_type="D", alpha_n=1.0, alpha_t=1.0):
     """Pressure-driven channel: nblocks blocks of n x nj cells along x,
     equilibrium inlet/outlet ghosts, diffuse upper wall, adsorbing lower wall."""
     nj = n if nj is None else nj
@@ -139,7 +143,8 @@ def channel(nblocks=4, n=64, m=32, vlim=5.0, flux_method="WENO5", Kn=0.05, rho_i
         x, y = uniform_grid(n, nj, length * b / nblocks, length * (b + 1) / nblocks, 0.0, height)
         bc = [None] * 4
         bc[D.NORTH] = diffuse(1.0)
-        bc[D.SOUTH] = adsorbing(1.0, gamma_f=gamma_f, k_des=k_des, adsorb=adsorb)
+        bc[D.SOUTH] = adsorbing(1.0, gamma_f=gamma_f, k_des=k_des, adsorb=adsorb, reflect_type=reflect_type,
+                                alpha_n=alpha_n, alpha_t=alpha_t)
         bc[D.WEST] = adjacent(b - 1, D.EAST) if b > 0 else inflow(rho_in, 1.0)
         bc[D.EAST] = adjacent(b + 1, D.WEST) if b + 1 < nblocks else inflow(rho_out, 1.0)
         # linear initial density between inlet and outlet

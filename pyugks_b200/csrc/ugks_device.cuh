@@ -261,6 +261,29 @@ __device__ __forceinline__ double sticking(const ugks_block_desc &d, V2 uv, doub
   return nrm * tan_;
 }
 
+// Cercignani-Lampis scattering (scatterNormal, scatterTangential,
+// CercignaniLampis: clFunctions.c:146-185), I0 from the CUDA math library
+__device__ __forceinline__ double scatter_normal(double c_in, double c_out, double an, double Tw) {
+  return (2.0 / (an * Tw)) * fabs(c_out) * cyl_bessel_i0(((2 * sqrt(1 - an)) / (an * Tw)) * c_in * c_out) *
+         exp(-(c_out * c_out + (1 - an) * c_in * c_in) / (an * Tw));
+}
+__device__ __forceinline__ double scatter_tangential(double PI, double c_in, double c_out, double at,
+                                                     double Tw) {
+  const double a = c_out - (1 - at) * c_in;
+  return (1.0 / sqrt(PI * at * (2 - at) * Tw)) * exp(-(a * a) / (at * (2 - at) * Tw));
+}
+// contribution of incoming velocity uv_in (distribution f_in) to outgoing
+// uv_out, with the (h, b) closure term added (clAdsorb.c:568-569)
+__device__ __forceinline__ V2 cercignani_lampis(double PI, V2 uv_in, V2 uv_out, V2 f_in, double an, double at,
+                                                double Tw, double lam_w) {
+  const double k = fabs(uv_in.x / uv_out.x) * scatter_normal(uv_in.x, uv_out.x, an, Tw) *
+                   scatter_tangential(PI, uv_in.y, uv_out.y, at, Tw);
+  V2 r = v2(k * f_in.x, k * f_in.y);
+  r.y *= (1 - at) * (1 - at);
+  r.y += 0.5 * at * (2 - at) / lam_w * r.x;
+  return r;
+}
+
 // ---------------------------------------------------------------------------
 // block-wide sums: every thread passes N partial sums and receives the totals.
 // `scratch` is shared memory of at least N * (blockDim.x / 32) doubles.

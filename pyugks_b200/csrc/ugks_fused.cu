@@ -572,18 +572,52 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
         st2(blk.wall_dist, k, v2(x.x * corr, x.y * corr));
       }
     if (!ok) return;  // the reference skips the rest of this wall (ugks_block.py:949-950)
-    // adsorbingWallD_P2 (clAdsorb.c:821-975)
+    // re-emission of the reflected flux: adsorbingWallD_P2 (clAdsorb.c:821-975,
+    // diffuse), adsorbingWallS_P2 (656-816, specular) or adsorbingWallCL_P2
+    // (488-651, Cercignani-Lampis)
     const double refl = cover[1], des = cover[3], ads = cover[2];
+    const int kind = d.reflect[wall];
     double ratio = 1.0;
     if (refl > 0.0) {
+      // the reflected incoming distribution (wall_dist) of every velocity,
+      // staged in the slope buffer, which wall faces do not use
+      double2 *rin = sgb;
+      __syncthreads();
+      if (kind != UGKS_REFLECT_DIFFUSE)
+        for (int v = threadIdx.x; v < Nv; v += FT) {
+          const V2 x = ld2(blk.wall_dist, (size_t)ci * Nv + v);
+          rin[v] = make_double2(x.x, x.y);
+        }
+      __syncthreads();
+      const double an = d.alpha_n[wall], at = d.alpha_t[wall], Tw = 1.0 / wl.s3;
       double r[1] = {0.0};
       for (int v = threadIdx.x; v < Nv; v += FT) {
         const V2 uv = face_velocity(d, v, n);
         const int delta = upwind_flag(uv.x, rot);
-        const V2 dif = delta ? maxwellian(d, wl, uv, v) : v2(0.0, 0.0);
-        fw[2 * v] = delta * dif.x + (1 - delta) * fw[2 * v];
-        fw[2 * v + 1] = delta * dif.y + (1 - delta) * fw[2 * v + 1];
-        r[0] += rot * uv.x * dif.x;
+        V2 out = v2(0.0, 0.0);
+        if (delta) {
+          if (kind == UGKS_REFLECT_DIFFUSE) {
+            out = maxwellian(d, wl, uv, v);
+          } else if (kind == UGKS_REFLECT_CL) {
+            for (int va = 0; va < Nv; ++va) {
+              const V2 uv_in = face_velocity(d, va, n);
+              if (!upwind_flag(uv_in.x, rot) && uv_in.x != 0.0) {
+                const double2 fi = rin[va];
+                const V2 c = cercignani_lampis(d.PI, uv_in, uv, v2(fi.x, fi.y), an, at, Tw, wl.s3);
+                out.x += c.x;
+                out.y += c.y;
+              }
+            }
+            out.x *= d.weight[v];
+            out.y *= d.weight[v];
+          } else {
+            const double2 x = rin[dir == WEST ? d.mirror_EW[v] : d.mirror_NS[v]];
+            out = v2(x.x, x.y);
+          }
+        }
+        fw[2 * v] = delta * out.x + (1 - delta) * fw[2 * v];
+        fw[2 * v + 1] = delta * out.y + (1 - delta) * fw[2 * v + 1];
+        r[0] += rot * uv.x * out.x;
       }
       block_sum<1>(r, sh.scratch);
       ratio = refl / r[0];

@@ -857,6 +857,88 @@ __global__ void __launch_bounds__(VT) k_adsorbingWall_P1(ugks_block_desc d, size
     }
 }
 
+// adsorbingWallS_P2 (clAdsorb.c:656-816) and adsorbingWallCL_P2
+// (clAdsorb.c:488-651): the reflected part of the incoming flux (wall_dist,
+// per incoming velocity, from adsorbingWall_P1) is re-emitted specularly,
+// through the velocity mirrored about the wall, or through the
+// Cercignani-Lampis kernel (an O(Nv^2) sum over incoming velocities); then,
+// as for diffuse re-emission, scaled to the reflected flux and the desorbed
+// particles added
+template <int KIND>
+__global__ void __launch_bounds__(VT) k_adsorbingWallSCL_P2(ugks_block_desc d, size_t g1,
+                                                            const double *normal, int face,
+                                                            const double *wall_prop,
+                                                            const double *wall_cover,
+                                                            const double *wall_dist, double *flux_f) {
+  __shared__ double scratch[VT / 32];
+  size_t a, b;
+  work_group(g1, a, b);
+  long gi = a, gj = b, ci;
+  int rot, fid;
+  wall_face(d, face, gi, gj, ci, rot, fid);
+  if (!wall_range(d, fid, gi, gj)) return;
+  V2 n = ld2(normal, faceidx(d, gi, gj, fid));
+  P4 wall = ld4(wall_prop, ci * 4 + face);
+  V2 wl = to_local(v2(wall.s1, wall.s2), n);
+  wall.s1 = wl.x;
+  wall.s2 = wl.y;
+  const double *cover = wall_cover + 4 * (ci * 4 + face);
+  const double refl = cover[1];
+  double ratio = 1.0;
+  if (refl > 0.0) {
+    double s[1] = {0.0};
+    const double an = d.alpha_n[face], at = d.alpha_t[face], Tw = 1.0 / wall.s3;
+    for (int v = threadIdx.x; v < d.Nv; v += blockDim.x) {
+      V2 uv = face_velocity(d, v, n);
+      int delta = upwind_flag(uv.x, rot);
+      V2 out = v2(0.0, 0.0);
+      if (delta) {
+        if (KIND == UGKS_REFLECT_SPECULAR) {
+          const int mv = fid == WEST ? d.mirror_EW[v] : d.mirror_NS[v];
+          out = ld2(wall_dist, (size_t)ci * d.Nv + mv);
+        } else {
+          for (int va = 0; va < d.Nv; ++va) {
+            const V2 uv_in = face_velocity(d, va, n);
+            if (!upwind_flag(uv_in.x, rot) && uv_in.x != 0.0) {
+              const V2 c = cercignani_lampis(d.PI, uv_in, uv, ld2(wall_dist, (size_t)ci * d.Nv + va), an, at, Tw,
+                                             wall.s3);
+              out.x += c.x;
+              out.y += c.y;
+            }
+          }
+          out.x *= d.weight[v];
+          out.y *= d.weight[v];
+        }
+      }
+      size_t kv = fidx(d, gi, gj, v);
+      V2 fd = ld2(flux_f, kv);
+      st2(flux_f, kv, v2(delta * out.x + (1 - delta) * fd.x, delta * out.y + (1 - delta) * fd.y));
+      s[0] += rot * uv.x * out.x;
+    }
+    block_sum<1>(s, scratch);
+    ratio = refl / s[0];
+  }
+  const double des = cover[3], ads = cover[2];
+  const int account = ((des == 0.0) && (ads > 0.0) && (refl == 0.0)) ? 1 : 0;
+  P4 wd = wall;
+  wd.s0 = 2 * des * sqrt(d.PI * wall.s3);
+  for (int v = threadIdx.x; v < d.Nv; v += blockDim.x) {
+    V2 uv = face_velocity(d, v, n);
+    int delta = upwind_flag(uv.x, rot);
+    size_t kv = fidx(d, gi, gj, v);
+    V2 fd = ld2(flux_f, kv);
+    double sc = 1 - delta * (1 - ratio);
+    fd.x *= sc;
+    fd.y *= sc;
+    V2 M = maxwellian(d, wd, uv, v);
+    fd.x += delta * M.x;
+    fd.y += delta * M.y;
+    fd.x -= account * delta * fd.x;
+    fd.y -= account * delta * fd.y;
+    st2(flux_f, kv, fd);
+  }
+}
+
 __global__ void __launch_bounds__(VT) k_adsorbingWallD_P2(ugks_block_desc d, size_t g1,
                                                           const double *normal, int face,
                                                           const double *wall_prop,
@@ -1109,6 +1191,20 @@ int ugks_adsorbingWallD_P2(const ugks_block_desc *d, size_t g0, size_t g1, const
                            double dt, void *stream) {
   (void)wall_dist; (void)macro; (void)dt;
   VEL_LAUNCH(k_adsorbingWallD_P2, normal, face, wall_prop, wall_cover, flux_f);
+}
+int ugks_adsorbingWallS_P2(const ugks_block_desc *d, size_t g0, size_t g1, const double *normal,
+                           int face, const double *wall_prop, const double *wall_cover,
+                           const double *wall_dist, double *flux_f, const double *macro,
+                           double dt, void *stream) {
+  (void)macro; (void)dt;
+  VEL_LAUNCH(k_adsorbingWallSCL_P2<UGKS_REFLECT_SPECULAR>, normal, face, wall_prop, wall_cover, wall_dist, flux_f);
+}
+int ugks_adsorbingWallCL_P2(const ugks_block_desc *d, size_t g0, size_t g1, const double *normal,
+                            int face, const double *wall_prop, const double *wall_cover,
+                            const double *wall_dist, double *flux_f, const double *macro,
+                            double dt, void *stream) {
+  (void)macro; (void)dt;
+  VEL_LAUNCH(k_adsorbingWallSCL_P2<UGKS_REFLECT_CL>, normal, face, wall_prop, wall_cover, wall_dist, flux_f);
 }
 
 }  // extern "C"

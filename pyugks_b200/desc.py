@@ -39,6 +39,16 @@ def block_desc(const: Constants, block: dict, tabs: VelocityTables) -> "_lib.Blo
     d.quad, d.weight = tabs.quad.data_ptr(), tabs.weight.data_ptr()
     d.mirror_NS, d.mirror_EW, d.mirror_D = (tabs.mirror_NS.data_ptr(), tabs.mirror_EW.data_ptr(),
                                             tabs.mirror_D.data_ptr())
+    fill_walls(d, block)
+    return d
+
+
+REFLECT_CODES = {"S": 0, "D": 1, "CL": 2}
+
+
+def fill_walls(d, block: dict):
+    """Wall values and the adsorbing-wall tables of ugks_block_desc, printed
+    as the reference's generated header prints them (ugks_CL.py:102-185)."""
     for f, bc in enumerate(block["bc"]):
         d.wall_D[f], d.wall_U[f], d.wall_V[f], d.wall_T[f], d.wall_P[f] = wall_values(bc)
         if bc["type"] == D.ADSORBING:
@@ -46,12 +56,17 @@ def block_desc(const: Constants, block: dict, tabs: VelocityTables) -> "_lib.Blo
             d.beta_t[f] = float("%0.15e" % bc.get("beta_t", 0.0))
             d.gamma_f[f] = float("%0.15e" % bc["gamma_f"])
             d.alpha_p[f] = float("%0.15e" % bc["alpha_p"])
+            d.alpha_n[f] = float("%0.15e" % bc.get("alpha_n", 1.0))
+            d.alpha_t[f] = float("%0.15e" % bc.get("alpha_t", 1.0))
             d.dynamic[f] = int(bc.get("dynamic", 1))
             scalar = np.ndim(bc["adsorb"]) == 0
             d.constant_adsorb[f] = 1 if scalar else 0
             d.adsorb[f] = float("%g" % bc["adsorb"]) if scalar else 0.0
             d.k_des[f] = float(bc.get("k_des", 0.0))
+            rt = bc.get("reflect_type", "S")
+            d.reflect[f] = REFLECT_CODES.get(rt, 0)
         else:
             d.beta_n[f] = d.beta_t[f] = d.gamma_f[f] = d.alpha_p[f] = -1.0
+            d.alpha_n[f] = d.alpha_t[f] = -1.0
             d.dynamic[f] = -1
-    return d
+            d.reflect[f] = -1

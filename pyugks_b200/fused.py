@@ -23,7 +23,8 @@ import numpy as np
 from . import _lib
 from . import checkpoint
 from . import defs as D
-from .problem import Constants, VelocityGrid, fill_arrays, geometry, wall_values
+from .desc import fill_walls
+from .problem import Constants, VelocityGrid, fill_arrays, geometry
 
 
 def _torch():
@@ -188,27 +189,14 @@ class FusedSolver:
         d.quad, d.weight = tabs["quad"].data_ptr(), tabs["weight"].data_ptr()
         d.mirror_NS, d.mirror_EW, d.mirror_D = (tabs["mNS"].data_ptr(), tabs["mEW"].data_ptr(),
                                                 tabs["mD"].data_ptr())
+        fill_walls(d, b)
         for f, bc in enumerate(b["bc"]):
-            d.wall_D[f], d.wall_U[f], d.wall_V[f], d.wall_T[f], d.wall_P[f] = wall_values(bc)
             x.bc_type[f] = bc["type"]
             if bc["type"] == D.ADJACENT:
                 x.bc_block[f] = first + bc["other_block"]
                 x.bc_face[f] = bc["other_face"]
                 x.bc_ori[f] = bc.get("orientation", 1)
                 x.bc_flip[f] = bc.get("flip", D.NO_FLIP)
-            if bc["type"] == D.ADSORBING:
-                d.beta_n[f] = float("%0.15e" % bc.get("beta_n", 0.0))
-                d.beta_t[f] = float("%0.15e" % bc.get("beta_t", 0.0))
-                d.gamma_f[f] = float("%0.15e" % bc["gamma_f"])
-                d.alpha_p[f] = float("%0.15e" % bc["alpha_p"])
-                d.dynamic[f] = int(bc.get("dynamic", 1))
-                scalar = np.ndim(bc["adsorb"]) == 0
-                d.constant_adsorb[f] = 1 if scalar else 0
-                d.adsorb[f] = float("%g" % bc["adsorb"]) if scalar else 0.0
-                d.k_des[f] = float(bc.get("k_des", 0.0))
-            else:
-                d.beta_n[f] = d.beta_t[f] = d.gamma_f[f] = d.alpha_p[f] = -1.0
-                d.dynamic[f] = -1
         x.solve = s
         for name in ("f", "flux_S", "flux_W", "flux_macro_S", "flux_macro_W", "macro", "Q", "prim_old",
                      "area", "centre", "mid_side", "normal", "side_length", "xy", "wall_prop",

@@ -178,10 +178,12 @@ class UGKSBlock:
                                       self.flag_D)
             if self.get_flag():
                 return True
-            if bc.get("reflect_type", "S") != "D":
-                raise NotImplementedError("adsorbing walls re-emit diffusely ('D') here")
-            self.prg.adsorbingWallD_P2(q, gsize, None, self.normal_D, wall, self.wall_prop_D,
-                                       self.wall_cover_D, self.wall_dist_D, flux, self.macro_D, dt)
+            # re-emission by reflect_type (ugks_block.py:952-969; 'S' unless 'CL' or 'D')
+            rtype = bc.get("reflect_type", "S")
+            p2 = (self.prg.adsorbingWallCL_P2 if rtype == "CL" else
+                  self.prg.adsorbingWallD_P2 if rtype == "D" else self.prg.adsorbingWallS_P2)
+            p2(q, gsize, None, self.normal_D, wall, self.wall_prop_D, self.wall_cover_D, self.wall_dist_D,
+               flux, self.macro_D, dt)
         self.prg.wallFlux(q, gsize, None, self.normal_D, self.length_D, wall, flux, flux_macro, dt)
         self.prg.wallMassEnergyFluxes(q, gsize, None, self.normal_D, self.length_D, self.area_D, wall,
                                       flux, self.wall_fluxes_D, dt)

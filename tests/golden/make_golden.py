@@ -15,6 +15,9 @@ Cases:
                (f, steps 1/10/30)
   channel8     2-block adsorbing channel 8x8, Langmuir desorption, CFL 0.3
                (f + coverage, 1/10/30)
+  channel8_specular / channel8_cl
+               channel8 with specular (adsorbingWallS_P2) or Cercignani-Lampis
+               (adsorbingWallCL_P2, alpha_n 0.5, alpha_t 0.7) re-emission
   cavity32     the 32x32 cavity, 25x25 velocities on [-4,4]^2, vanLeer, Kn 0.075,
                CFL 0.8, lid 0.15 (fields at steps 1/10/100/1000)
   cavity32_perturbed
@@ -41,6 +44,10 @@ CASES = {
     "multiblock8": (lambda: configs.cavity_multiblock(nb=2, n=8, m=8), (1, 10, 30), True),
     "channel8": (lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0), (1, 10, 30), True),
     "cavity32": (lambda: configs.cavity(n=32, m=24, vlim=4.0), (1, 10, 100, 1000), False),
+    "channel8_specular": (lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0, reflect_type="S"),
+                          (1, 10, 30), True),
+    "channel8_cl": (lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0, reflect_type="CL", alpha_n=0.5,
+                                            alpha_t=0.7), (1, 10, 30), True),
 }
 
 

@@ -120,6 +120,9 @@ CASES = {
     "multiblock_weno5": lambda: configs.cavity_multiblock(nb=2, n=8, m=8),
     "channel_langmuir": lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0),
     "channel_first_order": lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.01),
+    "channel_specular": lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0, reflect_type="S"),
+    "channel_cl": lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.01, reflect_type="CL", alpha_n=0.5,
+                                          alpha_t=0.7),
 }
 
 
@@ -134,7 +137,8 @@ def test_every_kernel_matches_oracle(cuda, name):
     assert not bad, (bad, sim.where)
 
 
-@pytest.mark.parametrize("name", ["cavity_vanleer", "multiblock_weno5", "channel_first_order"])
+@pytest.mark.parametrize("name", ["cavity_vanleer", "multiblock_weno5", "channel_first_order",
+                                  "channel_specular", "channel_cl"])
 def test_dropin_driver_matches_oracle(cuda, name):
     case = CASES[name]()
     ora = host.OracleSim(case, "port")

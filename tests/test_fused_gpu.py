@@ -46,8 +46,10 @@ def test_cavity_multiblock_weno5_fp64(cuda):
         assert rel_err(a, b) < FP64_TOL
 
 
-def test_channel_adsorbing_fp64(cuda):
-    case = configs.channel(nblocks=2, n=8, m=8, k_des=0.01)
+@pytest.mark.parametrize("reflect,k_des", [("D", 0.01), ("S", 0.0), ("S", 0.01), ("CL", 0.01)])
+def test_channel_adsorbing_fp64(cuda, reflect, k_des):
+    """Adsorbing lower wall with each re-emission model (adsorbingWall{D,S,CL}_P2)."""
+    case = configs.channel(nblocks=2, n=8, m=8, k_des=k_des, reflect_type=reflect, alpha_n=0.5, alpha_t=0.7)
     ora, gpu = run_both(case, 20)
     assert fields_err(gpu.fields(), ora.fields()) < FP64_TOL
     for bi, ob in zip(gpu.solve_block_ids(0), ora.blocks):

@@ -20,7 +20,13 @@ CASES = {
     "multiblock8": (lambda: configs.cavity_multiblock(nb=2, n=8, m=8), (1, 10, 30)),
     "channel8": (lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0), (1, 10, 30)),
     "cavity32": (lambda: configs.cavity(n=32, m=24, vlim=4.0), (1, 10)),
+    "channel8_specular": (lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0, reflect_type="S"), (1, 10, 30)),
+    "channel8_cl": (lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0, reflect_type="CL", alpha_n=0.5,
+                                            alpha_t=0.7), (1, 10, 30)),
 }
+# the Cercignani-Lampis kernel's Bessel I0: a power series in the port, a
+# rational approximation in the reference
+CASE_TOL = {"channel8_cl": 1e-12}
 
 
 @pytest.mark.parametrize("name", sorted(CASES))
@@ -38,12 +44,12 @@ def test_port_matches_reference_golden(name):
         for k, fl in enumerate(sim.fields()):
             gold = {key: g["s%d_b%d_%s" % (s, k, key)] for key in fl}
             errs = field_errors(fl, gold)
-            assert max(errs.values()) <= TOL, (name, s, k, errs)
+            assert max(errs.values()) <= CASE_TOL.get(name, TOL), (name, s, k, errs)
         key = "s%d_b0_f" % s
         if key in g:
             for k, f in enumerate(sim.interior_f()):
-                assert rel_err(f, g["s%d_b%d_f" % (s, k)]) <= TOL
-                assert rel_err(sim.blocks[k].wall_cover, g["s%d_b%d_cover" % (s, k)]) <= TOL
+                assert rel_err(f, g["s%d_b%d_f" % (s, k)]) <= CASE_TOL.get(name, TOL)
+                assert rel_err(sim.blocks[k].wall_cover, g["s%d_b%d_cover" % (s, k)]) <= CASE_TOL.get(name, TOL)
 
 
 def test_reference_build_matches_port_when_sources_present():
