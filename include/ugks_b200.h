@@ -69,6 +69,14 @@ typedef struct ugks_block_desc {
      accommodation ALPHA_N, ALPHA_T; ugks_CL.py:134-148, 255-273) */
   double alpha_n[4], alpha_t[4];
   int32_t reflect[4];
+  /* tabulated isotherms (constant_adsorb[f] == 0; ISO_, TRI_, NBR_<face>,
+     N_TRI, ugks_CL.py:158-252): device [n][4] points (P, T, theta, 0), the
+     [n_tri][4] Delaunay triangles of (P, T) and their [n_tri][4] neighbours
+     (-1: none) */
+  const double *iso[4];
+  const int32_t *tri[4];
+  const int32_t *nbr[4];
+  int32_t n_tri[4];
 } ugks_block_desc;
 
 #define UGKS_REFLECT_SPECULAR 0

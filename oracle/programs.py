@@ -145,6 +145,7 @@ class _PortParams(C.Structure):
         ("alpha_p", C.c_double * 4), ("dynamic", C.c_int * 4), ("constant_adsorb", C.c_int * 4),
         ("adsorb", C.c_double * 4), ("k_des", C.c_double * 4),
         ("alpha_n", C.c_double * 4), ("alpha_t", C.c_double * 4),
+        ("iso", C.c_void_p * 4), ("tri", C.c_void_p * 4), ("nbr", C.c_void_p * 4), ("n_tri", C.c_int * 4),
     ]
 
 
@@ -185,6 +186,11 @@ class PortProgram(_Program):
                 p.k_des[f] = float(bc.get("k_des", 0.0))
                 p.alpha_n[f] = us.e15(bc.get("alpha_n", 0.0))
                 p.alpha_t[f] = us.e15(bc.get("alpha_t", 0.0))
+                if np.ndim(bc["adsorb"]) != 0:
+                    pts, tri, nbr = us.isotherm_tables(bc["adsorb"])
+                    self._tables += [pts, tri, nbr]
+                    p.iso[f], p.tri[f], p.nbr[f] = pts.ctypes.data, tri.ctypes.data, nbr.ctypes.data
+                    p.n_tri[f] = tri.shape[0]
             else:
                 p.beta_n[f] = p.beta_t[f] = p.gamma_f[f] = p.alpha_p[f] = -1.0
                 p.alpha_n[f] = p.alpha_t[f] = -1.0

@@ -124,12 +124,23 @@ def gen_header(const: us.Constants, block: dict, block_id: int) -> str:
     a("const double ALPHA_T[4] = {%s};\n" % per_face("alpha_t", "%0.15e"))
     a("const int DYNAMIC_VARTHETA[4] = {%s};\n" % ", ".join(
         "%i" % bc.get("dynamic", 1) if bc["type"] == us.ADSORBING else "-1" for bc in bcs))
+    n_tri = [0, 0, 0, 0]
     for bci, bc in enumerate(bcs):
         fn = FACE_NAMES[bci]
+        if bc["type"] == us.ADSORBING and np.ndim(bc["adsorb"]) != 0:
+            pts, tri, nbr = us.isotherm_tables(bc["adsorb"])
+            a("#define CONSTANT_ADSORB_%s 0\n" % fn)
+            a("#define ADSORB_%s 0.0\n" % fn)
+            a("const double4 ISO_%s[%d] = {%s};\n" % (fn, len(pts), ", ".join(
+                "make_double4(%0.15e, %0.15e, %0.15e, 0)" % tuple(r[:3]) for r in pts)))
+            a("const int4 TRI_%s[%d] = {%s};\n" % (fn, len(tri), ", ".join(
+                "make_int4(%d, %d, %d, 0)" % tuple(r[:3]) for r in tri)))
+            a("const int4 NBR_%s[%d] = {%s};\n" % (fn, len(nbr), ", ".join(
+                "make_int4(%d, %d, %d, 0)" % tuple(r[:3]) for r in nbr)))
+            n_tri[bci] = len(tri)
+            continue
         if bc["type"] == us.ADSORBING:
             ads = bc["adsorb"]
-            if np.ndim(ads) != 0:
-                raise NotImplementedError("tabulated adsorption isotherms are not restated")
             if ads > 1.0 or ads <= 0.0:
                 raise RuntimeError("Boundary condition equilibrium adsorption out of bounds")
             a("#define CONSTANT_ADSORB_%s 1\n" % fn)
@@ -138,11 +149,9 @@ def gen_header(const: us.Constants, block: dict, block_id: int) -> str:
             a("#define CONSTANT_ADSORB_%s 0\n" % fn)
             a("#define ADSORB_%s 0.0\n" % fn)
         a("const double4 ISO_%s[1] = {make_double4(-1,-1,-1,-1)};\n" % fn)
-    for bci in range(4):
-        fn = FACE_NAMES[bci]
         a("const int4 TRI_%s[1] = {make_int4(-1,-1,-1,-1)};\n" % fn)
         a("const int4 NBR_%s[1] = {make_int4(-1,-1,-1,-1)};\n" % fn)
-    a("const int N_TRI[4] = {0, 0, 0, 0};\n")
+    a("const int N_TRI[4] = {%d, %d, %d, %d};\n" % tuple(n_tri))
     has = {"D": False, "CL": False, "S": False, "DA": False}
     for bc in bcs:
         if bc["type"] == us.DIFFUSE:

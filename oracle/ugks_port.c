@@ -505,6 +505,81 @@ void port_distFlux(PP, size_t g0, size_t g1, double *flux_f, const double *fsigm
     }
 }
 
+/* distance_from_segment, intersect, get_tri, interpolate, vartheta_langmuir
+   (clAdsorb.c:18-247): equilibrium coverage from a tabulated isotherm by a
+   walk through its Delaunay triangulation; intersect works in single
+   precision as the reference does */
+static double distance_from_segment(d2 a, d2 b, d2 c) {
+  double r_num = (c.x - a.x) * (b.x - a.x) + (c.y - a.y) * (b.y - a.y);
+  double r_den = (b.x - a.x) * (b.x - a.x) + (b.y - a.y) * (b.y - a.y);
+  double r = r_num / r_den;
+  double s = ((a.y - c.y) * (b.x - a.x) - (a.x - c.x) * (b.y - a.y)) / r_den;
+  double line = fabs(s) * sqrt(r_den);
+  if ((r >= 0) && (r <= 1)) return line;
+  double d1 = (c.x - a.x) * (c.x - a.x) + (c.y - a.y) * (c.y - a.y);
+  double d2v = (c.x - b.x) * (c.x - b.x) + (c.y - b.y) * (c.y - b.y);
+  return d1 < d2v ? sqrt(d1) : sqrt(d2v);
+}
+static int intersect(d2 a, d2 b, d2 c, d2 d) {
+  float den = (float)((d.y - c.y) * (b.x - a.x) - (d.x - c.x) * (b.y - a.y));
+  float num1 = (float)((d.x - c.x) * (a.y - c.y) - (d.y - c.y) * (a.x - c.x));
+  float num2 = (float)((b.x - a.x) * (a.y - c.y) - (b.y - a.y) * (a.x - c.x));
+  float u1 = num1 / den;
+  float u2 = num2 / den;
+  if (den == 0 && num1 == 0 && num2 == 0) return 0;
+  if (den == 0) return 0;
+  if (u1 < 0 || u1 > 1 || u2 < 0 || u2 > 1) return 0;
+  return 1;
+}
+static d2 iso_pt(const double *iso, int k) { d2 r = {iso[4 * k], iso[4 * k + 1]}; return r; }
+static void get_tri(d2 xy, const double *pts, const int32_t *tris, int size_tri, const int32_t *nbrs, int id,
+                    int *out_id, int *out_outside) {
+  const double tol = 1e-12;
+  int outside = 0;
+  for (int counter = 0; counter < size_tri; ++counter) {
+    const int32_t *t = tris + 4 * id;
+    d2 a = iso_pt(pts, t[0]), b = iso_pt(pts, t[1]), c = iso_pt(pts, t[2]);
+    d2 start = {(1.0 / 3.0) * (a.x + b.x + c.x), (1.0 / 3.0) * (a.y + b.y + c.y)};
+    int hz = intersect(a, b, start, xy), hx = intersect(b, c, start, xy), hy = intersect(c, a, start, xy);
+    if ((hx + hy + hz) == 0) break;
+    const int32_t *nb = nbrs + 4 * id;
+    if (hx) {
+      if (nb[0] == -1) { outside = 1; break; }
+      else if (distance_from_segment(b, c, xy) < tol) break;
+      else id = nb[0];
+    } else if (hy) {
+      if (nb[1] == -1) { outside = 1; break; }
+      else if (distance_from_segment(c, a, xy) < tol) break;
+      else id = nb[1];
+    } else if (hz) {
+      if (nb[2] == -1) { outside = 1; break; }
+      else if (distance_from_segment(a, b, xy) < tol) break;
+      else id = nb[2];
+    }
+  }
+  *out_id = id;
+  *out_outside = outside;
+}
+static double iso_interpolate(d2 pt, const double *a, const double *b, const double *c) {
+  double L1 = ((b[1] - c[1]) * (pt.x - c[0]) + (c[0] - b[0]) * (pt.y - c[1])) /
+              ((b[1] - c[1]) * (a[0] - c[0]) + (c[0] - b[0]) * (a[1] - c[1]));
+  double L2 = ((c[1] - a[1]) * (pt.x - c[0]) + (a[0] - c[0]) * (pt.y - c[1])) /
+              ((b[1] - c[1]) * (a[0] - c[0]) + (c[0] - b[0]) * (a[1] - c[1]));
+  double L3 = 1 - L1 - L2;
+  return L1 * a[2] + L2 * b[2] + L3 * c[2];
+}
+static d2 vartheta_langmuir(PP, double D, double T, int face) {
+  d2 v;
+  if (P->constant_adsorb[face]) { v.x = P->adsorb[face]; v.y = 0.0; return v; }
+  d2 pt = {0.5 * D * T, T};
+  int id, outside;
+  get_tri(pt, P->iso[face], P->tri[face], P->n_tri[face], P->nbr[face], 0, &id, &outside);
+  const int32_t *t = P->tri[face] + 4 * id;
+  v.x = iso_interpolate(pt, P->iso[face] + 4 * t[0], P->iso[face] + 4 * t[1], P->iso[face] + 4 * t[2]);
+  v.y = (double)outside;
+  return v;
+}
+
 /* wall-face addressing shared by the wall kernels (clUGKS.c:795-824) */
 static void wall_face(PP, int face, size_t *gi, size_t *gj, size_t *ci, int *rot, int *face_id) {
   switch (face) {
@@ -1080,15 +1155,17 @@ void port_adsorbingWall_P1(PP, size_t g0, size_t g1, const double *normal, int f
           dvt = 0.0;
           ads_final = ads_sum;
         }
-        if (!P->constant_adsorb[face]) {
-          flag[0] = ERR_CLAMPING_ADSORB_ISOTHERM;
-          continue;
-        }
         if (P->k_des[face] > 0.0) {
           /* first-order desorption: rate k_des * coverage (no reference counterpart) */
           des = P->k_des[face] * vartheta / P->alpha_p[face];
         } else {
-          double gamma_b = P->gamma_f[face] * (1.0 / P->adsorb[face] - 1.0) * adj_sum;
+          d2 veq = vartheta_langmuir(P, D, T, face);
+          if (veq.y == 1) {
+            /* outside the tabulated isotherm (clAdsorb.c:430-434) */
+            flag[0] = ERR_CLAMPING_ADSORB_ISOTHERM;
+            continue;
+          }
+          double gamma_b = P->gamma_f[face] * (1.0 / veq.x - 1.0) * adj_sum;
           des = gamma_b * vartheta;
         }
         if (P->dynamic[face] == 1) {

@@ -36,6 +36,11 @@ typedef struct {
   double k_des[4];
   /* Cercignani-Lampis accommodation (ALPHA_N, ALPHA_T, ugks_CL.py:134-148) */
   double alpha_n[4], alpha_t[4];
+  /* tabulated isotherms (ISO_, TRI_, NBR_<face>, N_TRI; ugks_CL.py:158-252):
+     points (P, T, theta, 0), Delaunay triangles and their neighbours */
+  const double *iso[4];
+  const int32_t *tri[4], *nbr[4];
+  int n_tri[4];
 } ugks_port_params;
 
 #endif

@@ -143,6 +143,25 @@ class Constants:
         self.delta_dt = float(case.get("delta_dt", 1.0))
 
 
+def isotherm_tables(adsorb):
+    """Tabulated isotherm of an adsorbing face (ugks_CL.py:158-252): points
+    (P, T, theta) as printed with %0.15e, padded to (n, 4); the Delaunay
+    triangles of (P, T) (scipy.spatial.Delaunay, as the reference) and
+    their neighbours, padded to (n_tri, 4) with 0."""
+    from scipy.spatial import Delaunay
+    a = np.asarray(adsorb, dtype=np.float64)
+    if a.ndim != 2 or a.shape[1] != 3:
+        raise RuntimeError("Passed in array for isotherm values is not an n*3 array")
+    pts = np.zeros((a.shape[0], 4))
+    pts[:, :3] = [[e15(x) for x in row] for row in a]
+    dl = Delaunay(a[:, 0:2])
+    tri = np.zeros((dl.simplices.shape[0], 4), dtype=np.int32)
+    nbr = np.zeros((dl.neighbors.shape[0], 4), dtype=np.int32)
+    tri[:, :3] = dl.simplices
+    nbr[:, :3] = dl.neighbors
+    return pts, tri, nbr
+
+
 def wall_text(bc: dict):
     """WALL_<f>_{D,U,V,T,P} macro bodies for one face (``ugks_CL.py:277-310``)."""
     t = bc["type"]

@@ -31,6 +31,7 @@ class BlockDesc(C.Structure):
         ("dynamic", i32 * 4), ("constant_adsorb", i32 * 4),
         ("u_num", i32), ("v_num", i32),
         ("alpha_n", f64 * 4), ("alpha_t", f64 * 4), ("reflect", i32 * 4),
+        ("iso", vp * 4), ("tri", vp * 4), ("nbr", vp * 4), ("n_tri", i32 * 4),
     ]
 
 

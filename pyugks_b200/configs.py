@@ -78,6 +78,21 @@ def adsorbing(T=1.0, gamma_f=0.5, k_des=0.01, adsorb=0.5, S_T=1.0, reflect_type=
                 alpha_n=alpha_n, alpha_t=alpha_t)
 
 
+def langmuir_table(K0=2.0, E=0.5, n_p=7, n_t=5, p_range=(0.05, 2.5), t_range=(0.5, 2.0), seed=3):
+    """A tabulated isotherm for ``adsorbing(adsorb=...)``: points (P, T,
+    theta) of the Langmuir form theta = K P / (1 + K P), K = K0 exp(E / T), on
+    a slightly jittered P x T grid (jitter keeps the Delaunay triangulation
+    of the points unique)."""
+    rng = np.random.default_rng(seed)
+    P, T = np.meshgrid(np.linspace(*p_range, n_p), np.linspace(*t_range, n_t), indexing="ij")
+    dp = (p_range[1] - p_range[0]) / (n_p - 1)
+    dt = (t_range[1] - t_range[0]) / (n_t - 1)
+    P = P + 0.05 * dp * rng.standard_normal(P.shape)
+    T = T + 0.05 * dt * rng.standard_normal(T.shape)
+    K = K0 * np.exp(E / T)
+    return np.stack([P.ravel(), T.ravel(), (K * P / (1.0 + K * P)).ravel()], axis=1)
+
+
 def base_case(flux_method, Kn, m, vlim, CFL=0.8):
     return dict(flux_method=flux_method, CFL=CFL, Pr=2.0 / 3.0, gamma=5.0 / 3.0, omega=0.81,
                 Kn_eff=Kn, relax_type=2, delta_dt=1.0,

@@ -261,6 +261,69 @@ __device__ __forceinline__ double sticking(const ugks_block_desc &d, V2 uv, doub
   return nrm * tan_;
 }
 
+// distance_from_segment, intersect, get_tri, interpolate, vartheta_langmuir
+// (clAdsorb.c:18-247): equilibrium coverage at (P = rho T / 2, T) from a
+// tabulated isotherm by a walk through its Delaunay triangulation, starting at
+// triangle 0; intersect works in single precision as the reference does.
+// Returns (theta, 1 when the point lies outside the table).
+__device__ __forceinline__ double iso_segment_distance(V2 a, V2 b, V2 c) {
+  const double r_num = (c.x - a.x) * (b.x - a.x) + (c.y - a.y) * (b.y - a.y);
+  const double r_den = (b.x - a.x) * (b.x - a.x) + (b.y - a.y) * (b.y - a.y);
+  const double r = r_num / r_den;
+  const double s = ((a.y - c.y) * (b.x - a.x) - (a.x - c.x) * (b.y - a.y)) / r_den;
+  const double line = fabs(s) * sqrt(r_den);
+  if ((r >= 0) && (r <= 1)) return line;
+  const double d1 = (c.x - a.x) * (c.x - a.x) + (c.y - a.y) * (c.y - a.y);
+  const double d2 = (c.x - b.x) * (c.x - b.x) + (c.y - b.y) * (c.y - b.y);
+  return d1 < d2 ? sqrt(d1) : sqrt(d2);
+}
+__device__ __forceinline__ int iso_intersect(V2 a, V2 b, V2 c, V2 d) {
+  const float den = (float)((d.y - c.y) * (b.x - a.x) - (d.x - c.x) * (b.y - a.y));
+  const float num1 = (float)((d.x - c.x) * (a.y - c.y) - (d.y - c.y) * (a.x - c.x));
+  const float num2 = (float)((b.x - a.x) * (a.y - c.y) - (b.y - a.y) * (a.x - c.x));
+  const float u1 = __fdiv_rn(num1, den), u2 = __fdiv_rn(num2, den);
+  if (den == 0.0f) return 0;
+  if (u1 < 0 || u1 > 1 || u2 < 0 || u2 > 1) return 0;
+  return 1;
+}
+__device__ inline V2 vartheta_langmuir(const ugks_block_desc &d, double D, double T, int face) {
+  if (d.constant_adsorb[face]) return v2(d.adsorb[face], 0.0);
+  const double *iso = d.iso[face];
+  const int32_t *tri = d.tri[face], *nbr = d.nbr[face];
+  const V2 xy = v2(0.5 * D * T, T);
+  auto pt = [&](int k) { return v2(iso[4 * k], iso[4 * k + 1]); };
+  int id = 0, outside = 0;
+  for (int counter = 0; counter < d.n_tri[face]; ++counter) {
+    const int32_t *t = tri + 4 * id;
+    const V2 a = pt(t[0]), b = pt(t[1]), c = pt(t[2]);
+    const V2 start = v2((1.0 / 3.0) * (a.x + b.x + c.x), (1.0 / 3.0) * (a.y + b.y + c.y));
+    const int hz = iso_intersect(a, b, start, xy), hx = iso_intersect(b, c, start, xy),
+              hy = iso_intersect(c, a, start, xy);
+    if ((hx + hy + hz) == 0) break;
+    const int32_t *nb = nbr + 4 * id;
+    if (hx) {
+      if (nb[0] == -1) { outside = 1; break; }
+      if (iso_segment_distance(b, c, xy) < 1e-12) break;
+      id = nb[0];
+    } else if (hy) {
+      if (nb[1] == -1) { outside = 1; break; }
+      if (iso_segment_distance(c, a, xy) < 1e-12) break;
+      id = nb[1];
+    } else {
+      if (nb[2] == -1) { outside = 1; break; }
+      if (iso_segment_distance(a, b, xy) < 1e-12) break;
+      id = nb[2];
+    }
+  }
+  const int32_t *t = tri + 4 * id;
+  const double *A = iso + 4 * t[0], *Bp = iso + 4 * t[1], *Cp = iso + 4 * t[2];
+  const double den = (Bp[1] - Cp[1]) * (A[0] - Cp[0]) + (Cp[0] - Bp[0]) * (A[1] - Cp[1]);
+  const double L1 = ((Bp[1] - Cp[1]) * (xy.x - Cp[0]) + (Cp[0] - Bp[0]) * (xy.y - Cp[1])) / den;
+  const double L2 = ((Cp[1] - A[1]) * (xy.x - Cp[0]) + (A[0] - Cp[0]) * (xy.y - Cp[1])) / den;
+  const double L3 = 1 - L1 - L2;
+  return v2(L1 * A[2] + L2 * Bp[2] + L3 * Cp[2], (double)outside);
+}
+
 // Cercignani-Lampis scattering (scatterNormal, scatterTangential,
 // CercignaniLampis: clFunctions.c:146-185), I0 from the CUDA math library
 __device__ __forceinline__ double scatter_normal(double c_in, double c_out, double an, double Tw) {

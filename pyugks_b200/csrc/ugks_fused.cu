@@ -506,7 +506,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     // adsorbingWall_P1 (clAdsorb.c:253-482)
     const long ti = dir == SOUTH ? mi : (wall == GEAST ? d.ni - 1 : 0);
     const long tj = dir == SOUTH ? (wall == GNORTH ? d.nj - 1 : 0) : mj;
-    const double Tw = 1.0 / blk.macro[4 * midx(d, ti, tj) + 3];
+    const double Tw = 1.0 / blk.macro[4 * midx(d, ti, tj) + 3], Dw = blk.macro[4 * midx(d, ti, tj)];
     double *cover = blk.wall_cover + 4 * (ci * 4 + wall);
     const double theta = cover[0];
     const double gf = d.gamma_f[wall];
@@ -538,12 +538,18 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
             ads_final = dvt / dt * d.alpha_p[wall];  // the reference's form (clAdsorb.c:420)
           }
         }
-        if (!d.constant_adsorb[wall]) {
-          atomicExch(&sol.status, 4);
-          ok = false;
+        if (d.k_des[wall] > 0.0) {
+          des = d.k_des[wall] * theta / d.alpha_p[wall];
         } else {
-          if (d.k_des[wall] > 0.0) des = d.k_des[wall] * theta / d.alpha_p[wall];
-          else des = gf * (1.0 / d.adsorb[wall] - 1.0) * s[2] * theta;
+          const V2 veq = vartheta_langmuir(d, Dw, Tw, wall);
+          if (veq.y == 1.0) {
+            atomicExch(&sol.status, 4);  // outside the tabulated isotherm
+            ok = false;
+          } else {
+            des = gf * (1.0 / veq.x - 1.0) * s[2] * theta;
+          }
+        }
+        if (ok) {
           if (d.dynamic[wall] == 1) {
             dvt -= dt * d.alpha_p[wall] * des;
             if ((theta + dvt) < 0.0) des = theta / (dt * d.alpha_p[wall]);
@@ -571,7 +577,15 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
         const V2 x = ld2(blk.wall_dist, k);
         st2(blk.wall_dist, k, v2(x.x * corr, x.y * corr));
       }
-    if (!ok) return;  // the reference skips the rest of this wall (ugks_block.py:949-950)
+    if (!ok) {
+      // the reference skips the rest of this wall face and carries on
+      // (ugks_block.py:949-950, 1084): its flux row keeps what iFace wrote
+      // there, the face values of (h, b), and its face macro flux is not
+      // written this step
+      void *fl = dir == SOUTH ? blk.flux_S : blk.flux_W;
+      for (int v = threadIdx.x; v < Nv; v += FT) St::store(fl, base + v, v2(fw[2 * v], fw[2 * v + 1]));
+      return;
+    }
     // re-emission of the reflected flux: adsorbingWallD_P2 (clAdsorb.c:821-975,
     // diffuse), adsorbingWallS_P2 (656-816, specular) or adsorbingWallCL_P2
     // (488-651, Cercignani-Lampis)

@@ -779,13 +779,14 @@ __global__ void __launch_bounds__(VT) k_adsorbingWall_P1(ugks_block_desc d, size
   long gi = a, gj = b, ci;
   int rot, fid;
   wall_face(d, face, gi, gj, ci, rot, fid);
-  double T;
+  size_t mc;  // the cell beside the wall face
   switch (face) {
-    case GNORTH: T = 1.0 / macro[4 * midx(d, ci, gj - d.ghost - 1) + 3]; break;
-    case GEAST: T = 1.0 / macro[4 * midx(d, gi - d.ghost - 1, ci) + 3]; break;
-    case GSOUTH: T = 1.0 / macro[4 * midx(d, ci, gj - d.ghost) + 3]; break;
-    default: T = 1.0 / macro[4 * midx(d, gi - d.ghost, ci) + 3]; break;
+    case GNORTH: mc = midx(d, ci, gj - d.ghost - 1); break;
+    case GEAST: mc = midx(d, gi - d.ghost - 1, ci); break;
+    case GSOUTH: mc = midx(d, ci, gj - d.ghost); break;
+    default: mc = midx(d, gi - d.ghost, ci); break;
   }
+  const double T = 1.0 / macro[4 * mc + 3], D = macro[4 * mc];
   if (!wall_range(d, fid, gi, gj)) return;
   V2 n = ld2(normal, faceidx(d, gi, gj, fid));
   double *cover = wall_cover + 4 * (ci * 4 + face);
@@ -820,16 +821,20 @@ __global__ void __launch_bounds__(VT) k_adsorbingWall_P1(ugks_block_desc d, size
           ads_final = dvt / dt * d.alpha_p[face];  // the reference's form (clAdsorb.c:420)
         }
       }
-      if (!d.constant_adsorb[face]) {
-        flag[0] = 4.0;
-        ok = false;
+      if (d.k_des[face] > 0.0) {
+        // first-order desorption k_des * theta (no counterpart in the reference)
+        des = d.k_des[face] * theta / d.alpha_p[face];
       } else {
-        if (d.k_des[face] > 0.0) {
-          // first-order desorption k_des * theta (no counterpart in the reference)
-          des = d.k_des[face] * theta / d.alpha_p[face];
+        // Langmuir desorption with the equilibrium coverage of the isotherm
+        const V2 veq = vartheta_langmuir(d, D, T, face);
+        if (veq.y == 1.0) {
+          flag[0] = 4.0;  // outside the tabulated isotherm
+          ok = false;
         } else {
-          des = gf * (1.0 / d.adsorb[face] - 1.0) * s[2] * theta;
+          des = gf * (1.0 / veq.x - 1.0) * s[2] * theta;
         }
+      }
+      if (ok) {
         if (d.dynamic[face] == 1) {
           dvt -= dt * d.alpha_p[face] * des;
           if ((theta + dvt) < 0.0) des = theta / (dt * d.alpha_p[face]);

@@ -10,13 +10,14 @@ import numpy as np
 
 from . import _lib
 from . import defs as D
-from .problem import Constants, wall_values
+from .problem import Constants, isotherm_tables, wall_values
 
 
 class VelocityTables:
     """Device copies of quad, weight and the mirror permutations."""
 
     def __init__(self, const: Constants, device):
+        self.keep = []  # device tables referenced by block descriptors (isotherms)
         import torch
         vg = const.vgrid
         self.quad = torch.from_numpy(np.ascontiguousarray(vg.quad)).to(device)
@@ -39,16 +40,18 @@ def block_desc(const: Constants, block: dict, tabs: VelocityTables) -> "_lib.Blo
     d.quad, d.weight = tabs.quad.data_ptr(), tabs.weight.data_ptr()
     d.mirror_NS, d.mirror_EW, d.mirror_D = (tabs.mirror_NS.data_ptr(), tabs.mirror_EW.data_ptr(),
                                             tabs.mirror_D.data_ptr())
-    fill_walls(d, block)
+    fill_walls(d, block, tabs.keep, tabs.quad.device)
     return d
 
 
 REFLECT_CODES = {"S": 0, "D": 1, "CL": 2}
 
 
-def fill_walls(d, block: dict):
+def fill_walls(d, block: dict, keep: list, device):
     """Wall values and the adsorbing-wall tables of ugks_block_desc, printed
-    as the reference's generated header prints them (ugks_CL.py:102-185)."""
+    as the reference's generated header prints them (ugks_CL.py:102-185);
+    the device copies of tabulated isotherms are appended to ``keep``."""
+    import torch
     for f, bc in enumerate(block["bc"]):
         d.wall_D[f], d.wall_U[f], d.wall_V[f], d.wall_T[f], d.wall_P[f] = wall_values(bc)
         if bc["type"] == D.ADSORBING:
@@ -62,6 +65,12 @@ def fill_walls(d, block: dict):
             scalar = np.ndim(bc["adsorb"]) == 0
             d.constant_adsorb[f] = 1 if scalar else 0
             d.adsorb[f] = float("%g" % bc["adsorb"]) if scalar else 0.0
+            if not scalar:
+                pts, tri, nbr = isotherm_tables(bc["adsorb"])
+                tabs = [torch.from_numpy(x).to(device) for x in (pts, tri, nbr)]
+                keep.extend(tabs)
+                d.iso[f], d.tri[f], d.nbr[f] = (t.data_ptr() for t in tabs)
+                d.n_tri[f] = tri.shape[0]
             d.k_des[f] = float(bc.get("k_des", 0.0))
             rt = bc.get("reflect_type", "S")
             d.reflect[f] = REFLECT_CODES.get(rt, 0)

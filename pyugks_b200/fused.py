@@ -189,7 +189,7 @@ class FusedSolver:
         d.quad, d.weight = tabs["quad"].data_ptr(), tabs["weight"].data_ptr()
         d.mirror_NS, d.mirror_EW, d.mirror_D = (tabs["mNS"].data_ptr(), tabs["mEW"].data_ptr(),
                                                 tabs["mD"].data_ptr())
-        fill_walls(d, b)
+        fill_walls(d, b, self._keep, self.device)
         for f, bc in enumerate(b["bc"]):
             x.bc_type[f] = bc["type"]
             if bc["type"] == D.ADJACENT:

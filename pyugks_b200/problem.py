@@ -347,3 +347,22 @@ def fill_arrays(block: dict):
     Q[:, :, 0] *= f.get("qx", 0.0)
     Q[:, :, 1] *= f.get("qy", 0.0)
     return macro, Q
+
+
+def isotherm_tables(adsorb):
+    """A tabulated isotherm as the generated header holds it
+    (ugks_CL.py:158-252): points (P, T, theta) printed with %0.15e, padded to
+    (n, 4); the Delaunay triangles of (P, T) (scipy.spatial.Delaunay) and
+    their neighbours, padded to (n_tri, 4)."""
+    from scipy.spatial import Delaunay
+    a = np.asarray(adsorb, dtype=np.float64)
+    if a.ndim != 2 or a.shape[1] != 3:
+        raise ValueError("an isotherm table is an (n, 3) array of (P, T, theta)")
+    pts = np.zeros((a.shape[0], 4))
+    pts[:, :3] = np.vectorize(lambda x: float("%0.15e" % x))(a)
+    dl = Delaunay(a[:, 0:2])
+    tri = np.zeros((dl.simplices.shape[0], 4), dtype=np.int32)
+    nbr = np.zeros((dl.neighbors.shape[0], 4), dtype=np.int32)
+    tri[:, :3] = dl.simplices
+    nbr[:, :3] = dl.neighbors
+    return pts, tri, nbr

@@ -18,6 +18,8 @@ Cases:
   channel8_specular / channel8_cl
                channel8 with specular (adsorbingWallS_P2) or Cercignani-Lampis
                (adsorbingWallCL_P2, alpha_n 0.5, alpha_t 0.7) re-emission
+  channel8_isotherm
+               channel8 with a tabulated Langmuir isotherm (configs.langmuir_table)
   cavity32     the 32x32 cavity, 25x25 velocities on [-4,4]^2, vanLeer, Kn 0.075,
                CFL 0.8, lid 0.15 (fields at steps 1/10/100/1000)
   cavity32_perturbed
@@ -48,6 +50,8 @@ CASES = {
                           (1, 10, 30), True),
     "channel8_cl": (lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0, reflect_type="CL", alpha_n=0.5,
                                             alpha_t=0.7), (1, 10, 30), True),
+    "channel8_isotherm": (lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0,
+                                                  adsorb=configs.langmuir_table()), (1, 10, 30), True),
 }
 
 

@@ -123,6 +123,7 @@ CASES = {
     "channel_specular": lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0, reflect_type="S"),
     "channel_cl": lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.01, reflect_type="CL", alpha_n=0.5,
                                           alpha_t=0.7),
+    "channel_isotherm": lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0, adsorb=configs.langmuir_table()),
 }
 
 
@@ -138,7 +139,7 @@ def test_every_kernel_matches_oracle(cuda, name):
 
 
 @pytest.mark.parametrize("name", ["cavity_vanleer", "multiblock_weno5", "channel_first_order",
-                                  "channel_specular", "channel_cl"])
+                                  "channel_specular", "channel_cl", "channel_isotherm"])
 def test_dropin_driver_matches_oracle(cuda, name):
     case = CASES[name]()
     ora = host.OracleSim(case, "port")

@@ -57,6 +57,30 @@ def test_channel_adsorbing_fp64(cuda, reflect, k_des):
         assert rel_err(cov[:8, 2, :], ob.wall_cover[:8, 2, :]) < FP64_TOL
 
 
+def test_channel_tabulated_isotherm_fp64(cuda):
+    """Langmuir desorption with the equilibrium coverage interpolated from a
+    tabulated isotherm (vartheta_langmuir, clAdsorb.c:171-247)."""
+    case = configs.channel(nblocks=2, n=8, m=8, k_des=0.0, adsorb=configs.langmuir_table())
+    ora, gpu = run_both(case, 20)
+    assert gpu.solve_state()[0]["status"] == 0
+    assert fields_err(gpu.fields(), ora.fields()) < FP64_TOL
+    for bi, ob in zip(gpu.solve_block_ids(0), ora.blocks):
+        cov = gpu.blocks[bi].wall_cover.cpu().numpy()
+        assert rel_err(cov[:8, 2, :], ob.wall_cover[:8, 2, :]) < FP64_TOL
+
+
+def test_isotherm_outside_the_table_flags_status_4(cuda):
+    """A wall state outside the tabulated isotherm sets the reference's
+    ERR_CLAMPING_ADSORB_ISOTHERM (4) in the solve record; nothing faults."""
+    table = configs.langmuir_table(p_range=(2.0, 3.0))   # pressures far above the channel's
+    case = configs.channel(nblocks=2, n=8, m=8, k_des=0.0, adsorb=table)
+    ora, gpu = run_both(case, 2)
+    assert gpu.solve_state()[0]["status"] == 4
+    # the reference skips the rest of that wall face and ignores the error
+    # return (ugks_block.py:949-950, 1084); so does the oracle
+    assert fields_err(gpu.fields(), ora.fields()) < FP64_TOL
+
+
 def test_cavity_mixed_precision(cuda):
     ora, gpu = run_both(configs.cavity(n=8, m=8, vlim=4.0), 30, precision="mixed")
     assert fields_err(gpu.fields(), ora.fields()) < MIXED_TOL

@@ -23,6 +23,8 @@ CASES = {
     "channel8_specular": (lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0, reflect_type="S"), (1, 10, 30)),
     "channel8_cl": (lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0, reflect_type="CL", alpha_n=0.5,
                                             alpha_t=0.7), (1, 10, 30)),
+    "channel8_isotherm": (lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0,
+                                                  adsorb=configs.langmuir_table()), (1, 10, 30)),
 }
 # the Cercignani-Lampis kernel's Bessel I0: a power series in the port, a
 # rational approximation in the reference
