@@ -214,6 +214,18 @@ int ugks_adsorbingWallD_P2(const ugks_block_desc *d, size_t g0, size_t g1, const
                            int face, const double *wall_prop, const double *wall_cover,
                            const double *wall_dist, double *flux_f, const double *macro,
                            double dt, UGKS_STREAM);
+/* Geometry set-up (UGKSBlock.updateGeom, ugks_block.py:667-760).
+   clGhostRoutines.c:155-284: ghost vertices from the neighbouring block */
+int ugks_xyExchange(const ugks_block_desc *d, size_t g0, size_t g1, double *xyA, int this_face,
+                    const double *xyB, int NIB, int NJB, int that_face, int ori, int affine,
+                    int flip_normal, int this_block_id, int that_block_id, UGKS_STREAM);
+/* clGhostRoutines.c:291-398: ghost vertices by extrapolation */
+int ugks_xyExtrapolate(const ugks_block_desc *d, size_t g0, size_t g1, double *xy, int this_face,
+                       UGKS_STREAM);
+/* clKernel.c:31-135: normals, areas, centroids, mid-sides, side lengths */
+int ugks_cellGeom(const ugks_block_desc *d, size_t g0, size_t g1, const double *xy, double *area,
+                  double *centre, double *mid_side, double *normal, double *side_length, UGKS_STREAM);
+
 /* clAdsorb.c:656-816: specular re-emission of the reflected flux */
 int ugks_adsorbingWallS_P2(const ugks_block_desc *d, size_t g0, size_t g1, const double *normal,
                            int face, const double *wall_prop, const double *wall_cover,

@@ -83,6 +83,7 @@ KERNEL_SIGNATURES = {
     "edgeMirror": "pi", "edgeBounceBack": "pi", "edgeConstGrad": "pi",
     "adsorbingWall_P1": "pipppppdp", "adsorbingWallD_P2": "pipppppd",
     "adsorbingWallS_P2": "pipppppd", "adsorbingWallCL_P2": "pipppppd",
+    "xyExchange": "pipiiiiiiii", "xyExtrapolate": "pi", "cellGeom": "pppppp",
 }
 _CT = {"p": vp, "i": C.c_int, "d": f64}
 

@@ -18,6 +18,10 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 
 
+# the geometry set-up keeps every product and sum separately rounded
+FILE_FLAGS = {"ugks_geometry.cu": ["-fmad=false"]}
+
+
 def sources():
     return sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
 
@@ -43,7 +47,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
     os.makedirs(bdir, exist_ok=True)
     for src in sources():
         obj = os.path.join(bdir, os.path.basename(src)[:-3] + ".o")
-        cmd = [nvcc, *NVCC_FLAGS, "-I", os.path.join(ROOT, "include"), "-c", src, "-o", obj]
+        cmd = [nvcc, *NVCC_FLAGS, *FILE_FLAGS.get(os.path.basename(src), []), "-I", os.path.join(ROOT, "include"),
+               "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)

@@ -147,6 +147,26 @@ def cavity_multiblock(nb=2, n=64, m=32, vlim=5.0, flux_method="WENO5", Kn=0.01, 
     return case
 
 
+def warp_grid(x, y, amp=0.04):
+    """Curvilinear vertices on the unit square: each vertex moved by
+    amp sin(2 pi x) sin(pi y) along x and amp sin(pi x) sin(2 pi y) along y,
+    which vanishes on the square's edges (straight walls) and is the same
+    function on every block, so shared block edges stay shared."""
+    xs = x + amp * np.sin(2 * np.pi * x) * np.sin(np.pi * y)
+    ys = y + amp * np.sin(np.pi * x) * np.sin(2 * np.pi * y)
+    return np.ascontiguousarray(xs), np.ascontiguousarray(ys)
+
+
+def warped_cavity(nb=1, n=16, m=8, vlim=4.0, flux_method="vanLeer", Kn=0.05, lid=0.15, amp=0.04, CFL=0.3):
+    """The lid-driven cavity on a curvilinear grid (warp_grid), as nb x nb
+    connected blocks of n x n cells."""
+    case = cavity_multiblock(nb=nb, n=n, m=m, vlim=vlim, flux_method=flux_method, Kn=Kn, lid=lid, CFL=CFL) \
+        if nb > 1 else cavity(n=n, m=m, vlim=vlim, flux_method=flux_method, Kn=Kn, lid=lid, CFL=CFL)
+    for b in case["blocks"]:
+        b["x"], b["y"] = warp_grid(b["x"], b["y"], amp)
+    return case
+
+
 def channel(nblocks=4, n=64, m=32, vlim=5.0, flux_method="WENO5", Kn=0.05, rho_in=1.2,
             rho_out=1.0, length=4.0, height=1.0, gamma_f=0.5, k_des=0.01, CFL=0.3, nj=None,
             adsorb=0.5, reflect_type="D", alpha_n=1.0, alpha_t=1.0):

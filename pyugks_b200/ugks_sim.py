@@ -21,10 +21,12 @@ from .ugks_block import UGKSBlock
 
 
 class UGKSim:
-    def __init__(self, case: dict, device="cuda", queue=None, restart=None):
+    def __init__(self, case: dict, device="cuda", queue=None, restart=None, device_geometry=False):
         """restart: checkpoint path (or the dict of checkpoint.read) to resume
         from, as the reference's ``gdata.restart`` (``restart``,
-        ugks_sim.py:824-840)."""
+        ugks_sim.py:824-840).  device_geometry: build the block geometry with
+        the xyExchange / xyExtrapolate / cellGeom kernels on the device, as the
+        reference's initGeom does, instead of on the host."""
         import torch
         self.case = case
         self.const = Constants(case)
@@ -40,7 +42,11 @@ class UGKSim:
         self.step = 0 if restart is None else int(restart["final_step"])
         self.force_time = False
         self.tabs = VelocityTables(self.const, self.device)
-        geoms = geometry(case, self.const.ghost)
+        if device_geometry:
+            from .geometry import device_geometry as _dg
+            geoms = _dg(case, device, queue)
+        else:
+            geoms = geometry(case, self.const.ghost)
         self.blocks = [UGKSBlock(self, k, b, g, self.tabs, self.device, queue)
                        for k, (b, g) in enumerate(zip(case["blocks"], geoms))]
         self.is_open = any(bc["type"] in (D.EXTRAPOLATE_OUT, D.INFLOW, D.OUTFLOW, D.CONSTANT)
