@@ -77,6 +77,7 @@ typedef struct ugks_block_desc {
   const int32_t *tri[4];
   const int32_t *nbr[4];
   int32_t n_tri[4];
+  double B;              /* degrees of freedom b (getInternal's T divisor)  */
 } ugks_block_desc;
 
 #define UGKS_REFLECT_SPECULAR 0
@@ -214,6 +215,11 @@ int ugks_adsorbingWallD_P2(const ugks_block_desc *d, size_t g0, size_t g1, const
                            int face, const double *wall_prop, const double *wall_cover,
                            const double *wall_dist, double *flux_f, const double *macro,
                            double dt, UGKS_STREAM);
+/* clKernel.c:314-375: per interior cell the directional temperatures
+   Txyz = (Tx, Ty, Tz, T) and the stress (tau_xx, tau_xy, tau_yy, 0) */
+int ugks_getInternal(const ugks_block_desc *d, size_t g0, size_t g1, const double *Fin, double *Txyz,
+                     double *Stress, UGKS_STREAM);
+
 /* Geometry set-up (UGKSBlock.updateGeom, ugks_block.py:667-760).
    clGhostRoutines.c:155-284: ghost vertices from the neighbouring block */
 int ugks_xyExchange(const ugks_block_desc *d, size_t g0, size_t g1, double *xyA, int this_face,

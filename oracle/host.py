@@ -99,6 +99,24 @@ class OracleBlock:
                     wall_prop=self.wall_prop.copy(), wall_cover=self.wall_cover.copy(),
                     wall_fluxes=self.wall_fluxes.copy(), f=self.f.copy() if with_f else None)
 
+    # getInternal (clKernel.c:314-375)
+    def internal_data(self):
+        txyz, stress = np.zeros((self.ni, self.nj, 4)), np.zeros((self.ni, self.nj, 4))
+        self.prg.getInternal((self.ni, self.nj), self.f, txyz, stress)
+        return txyz, stress[:, :, 0:3]
+
+    # get_interface_distribution (ugks_block.py:985-1047), into scratch arrays
+    def interface_distribution(self):
+        G, Ni, Nj = self.G, self.Ni, self.Nj
+        face, sigma = np.zeros_like(self.f), np.zeros_like(self.f)
+        self.prg.iFace((self.ni, self.nj + 1), self.f, face, sigma, self.centre, self.side, self.normal, S_DIR)
+        out = {"N": face[G:Ni - G, Nj - G].copy(), "S": face[G:Ni - G, G].copy()}
+        face[:] = 0.0
+        self.prg.iFace((self.ni + 1, self.nj), self.f, face, sigma, self.centre, self.side, self.normal, W_DIR)
+        out["E"] = face[Ni - G, G:Nj - G].copy()
+        out["W"] = face[G, G:Nj - G].copy()
+        return out
+
     # ugks_block.py:621-665
     def update_bc(self):
         for face, bc in enumerate(self.bc_list):

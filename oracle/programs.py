@@ -38,7 +38,7 @@ SIGNATURES = {
     "edgeMirror": "pi", "edgeBounceBack": "pi", "edgeConstGrad": "pi",
     "adsorbingWall_P1": "pipppppdp", "adsorbingWallD_P2": "pipppppd",
     "adsorbingWallS_P2": "pipppppd", "adsorbingWallCL_P2": "pipppppd",
-    "xyExchange": "pipiiiiiiii", "xyExtrapolate": "pi", "cellGeom": "pppppp",
+    "xyExchange": "pipiiiiiiii", "xyExtrapolate": "pi", "cellGeom": "pppppp", "getInternal": "ppp",
 }
 _CT = {"p": C.c_void_p, "i": C.c_int, "d": C.c_double}
 

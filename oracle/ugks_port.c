@@ -580,6 +580,36 @@ static d2 vartheta_langmuir(PP, double D, double T, int face) {
   return v;
 }
 
+/* getInternal (clKernel.c:314-375): directional temperatures and stress */
+void port_getInternal(PP, size_t g0, size_t g1, const double *Fin, double *Txyz, double *Stress) {
+  for (size_t a = 0; a < g0; ++a)
+    for (size_t b = 0; b < g1; ++b) {
+      if (!(a < (size_t)P->ni && b < (size_t)P->nj)) continue;
+      size_t gi = a + P->ghost, gj = b + P->ghost;
+      double D = 0.0, M1 = 0.0, M2 = 0.0, M4 = 0.0, M5 = 0.0, M6 = 0.0, H = 0.0;
+      for (size_t v = 0; v < (size_t)P->Nv; ++v) {
+        d2 uv = quad_at(P, v);
+        d2 f = ld2(Fin, FIDX(gi, gj, v));
+        D += f.x;
+        M1 += uv.x * f.x;
+        M2 += uv.y * f.x;
+        M4 += uv.x * uv.x * f.x;
+        M5 += uv.y * uv.y * f.x;
+        M6 += uv.x * uv.y * f.x;
+        H += f.y;
+      }
+      double U = M1 / D, V = M2 / D;
+      double Tx = 2 * (M4 / D - U * U), Ty = 2 * (M5 / D - V * V), Tz = 2 * (H / D);
+      double T = (Tx + Ty + Tz) / P->B;
+      size_t m = MIDX(a, b);
+      Txyz[4 * m] = Tx; Txyz[4 * m + 1] = Ty; Txyz[4 * m + 2] = Tz; Txyz[4 * m + 3] = T;
+      Stress[4 * m] = M4 - D * (U * U + T / 2.0);
+      Stress[4 * m + 1] = M6 - D * (U * V + T / 2.0);
+      Stress[4 * m + 2] = M5 - D * (V * V + T / 2.0);
+      Stress[4 * m + 3] = 0.0;
+    }
+}
+
 /* wall-face addressing shared by the wall kernels (clUGKS.c:795-824) */
 static void wall_face(PP, int face, size_t *gi, size_t *gj, size_t *ci, int *rot, int *face_id) {
   switch (face) {

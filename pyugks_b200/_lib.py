@@ -32,6 +32,7 @@ class BlockDesc(C.Structure):
         ("u_num", i32), ("v_num", i32),
         ("alpha_n", f64 * 4), ("alpha_t", f64 * 4), ("reflect", i32 * 4),
         ("iso", vp * 4), ("tri", vp * 4), ("nbr", vp * 4), ("n_tri", i32 * 4),
+        ("B", f64),
     ]
 
 
@@ -83,7 +84,7 @@ KERNEL_SIGNATURES = {
     "edgeMirror": "pi", "edgeBounceBack": "pi", "edgeConstGrad": "pi",
     "adsorbingWall_P1": "pipppppdp", "adsorbingWallD_P2": "pipppppd",
     "adsorbingWallS_P2": "pipppppd", "adsorbingWallCL_P2": "pipppppd",
-    "xyExchange": "pipiiiiiiii", "xyExtrapolate": "pi", "cellGeom": "pppppp",
+    "xyExchange": "pipiiiiiiii", "xyExtrapolate": "pi", "cellGeom": "pppppp", "getInternal": "ppp",
 }
 _CT = {"p": vp, "i": C.c_int, "d": f64}
 

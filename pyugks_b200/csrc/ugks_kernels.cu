@@ -862,6 +862,39 @@ __global__ void __launch_bounds__(VT) k_adsorbingWall_P1(ugks_block_desc d, size
     }
 }
 
+// getInternal (clKernel.c:314-375): one work group per interior cell;
+// directional temperatures (Tx, Ty, Tz, T) and stress (xx, xy, yy, 0) from
+// the moments of f
+__global__ void __launch_bounds__(VT) k_getInternal(ugks_block_desc d, size_t g1, const double *Fin, double *Txyz,
+                                                    double *Stress) {
+  __shared__ double scratch[7 * VT / 32];
+  size_t a, b;
+  work_group(g1, a, b);
+  if (!(a < (size_t)d.ni && b < (size_t)d.nj)) return;
+  const long gi = a + d.ghost, gj = b + d.ghost;
+  double m[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};  // D, M1, M2, M4, M5, M6, H
+  for (int v = threadIdx.x; v < d.Nv; v += blockDim.x) {
+    const V2 uv = quad_at(d, v);
+    const V2 f = ld2(Fin, fidx(d, gi, gj, v));
+    m[0] += f.x;
+    m[1] += uv.x * f.x;
+    m[2] += uv.y * f.x;
+    m[3] += uv.x * uv.x * f.x;
+    m[4] += uv.y * uv.y * f.x;
+    m[5] += uv.x * uv.y * f.x;
+    m[6] += f.y;
+  }
+  block_sum<7>(m, scratch);
+  if (threadIdx.x == 0) {
+    const double D = m[0], U = m[1] / D, V = m[2] / D;
+    const double Tx = 2 * (m[3] / D - U * U), Ty = 2 * (m[4] / D - V * V), Tz = 2 * (m[6] / D);
+    const double T = (Tx + Ty + Tz) / d.B;
+    const size_t k = midx(d, a, b);
+    st4(Txyz, k, p4(Tx, Ty, Tz, T));
+    st4(Stress, k, p4(m[3] - D * (U * U + T / 2.0), m[5] - D * (U * V + T / 2.0), m[4] - D * (V * V + T / 2.0), 0.0));
+  }
+}
+
 // adsorbingWallS_P2 (clAdsorb.c:656-816) and adsorbingWallCL_P2
 // (clAdsorb.c:488-651): the reflected part of the incoming flux (wall_dist,
 // per incoming velocity, from adsorbingWall_P1) is re-emitted specularly,
@@ -1196,6 +1229,10 @@ int ugks_adsorbingWallD_P2(const ugks_block_desc *d, size_t g0, size_t g1, const
                            double dt, void *stream) {
   (void)wall_dist; (void)macro; (void)dt;
   VEL_LAUNCH(k_adsorbingWallD_P2, normal, face, wall_prop, wall_cover, flux_f);
+}
+int ugks_getInternal(const ugks_block_desc *d, size_t g0, size_t g1, const double *Fin, double *Txyz,
+                     double *Stress, void *stream) {
+  VEL_LAUNCH(k_getInternal, Fin, Txyz, Stress);
 }
 int ugks_adsorbingWallS_P2(const ugks_block_desc *d, size_t g0, size_t g1, const double *normal,
                            int face, const double *wall_prop, const double *wall_cover,

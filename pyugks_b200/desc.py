@@ -37,6 +37,7 @@ def block_desc(const: Constants, block: dict, tabs: VelocityTables) -> "_lib.Blo
     d.u_num, d.v_num = const.vgrid.u_num, const.vgrid.v_num
     d.PI, d.Pr, d.umax, d.vmax = const.PI, const.Pr, const.umax, const.vmax
     d.Kn_eff, d.gam, d.K, d.omega = const.Kn_eff, const.gam, const.K, const.omega
+    d.B = const.B
     d.quad, d.weight = tabs.quad.data_ptr(), tabs.weight.data_ptr()
     d.mirror_NS, d.mirror_EW, d.mirror_D = (tabs.mirror_NS.data_ptr(), tabs.mirror_EW.data_ptr(),
                                             tabs.mirror_D.data_ptr())

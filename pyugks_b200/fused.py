@@ -186,6 +186,7 @@ class FusedSolver:
         d.u_num, d.v_num = const.vgrid.u_num, const.vgrid.v_num
         d.PI, d.Pr, d.umax, d.vmax = const.PI, const.Pr, const.umax, const.vmax
         d.Kn_eff, d.gam, d.K, d.omega = const.Kn_eff, const.gam, const.K, const.omega
+        d.B = const.B
         d.quad, d.weight = tabs["quad"].data_ptr(), tabs["weight"].data_ptr()
         d.mirror_NS, d.mirror_EW, d.mirror_D = (tabs["mNS"].data_ptr(), tabs["mEW"].data_ptr(),
                                                 tabs["mD"].data_ptr())
@@ -316,6 +317,34 @@ class FusedSolver:
         return [self.blocks[bi].f[self.blocks[bi].G:-self.blocks[bi].G,
                                   self.blocks[bi].G:-self.blocks[bi].G].double().cpu().numpy()
                 for bi in self.solve_blocks[self.order[solve]]]
+
+    def _program(self, bi):
+        from .kernel_program import KernelProgram
+        b = self.blocks[bi]
+        if not hasattr(b, "prg"):
+            b.prg = KernelProgram(b.struct.d)
+        return b.prg
+
+    def internal_data(self, solve: int = 0):
+        """Per block of the caller's solve (Txyz [ni, nj, 4], stress
+        [ni, nj, 3]) from getInternal (clKernel.c:314-375)."""
+        from .diagnostics import internal_data
+        out = []
+        for bi in self.solve_blocks[self.order[solve]]:
+            b = self.blocks[bi]
+            out.append(internal_data(self._program(bi), b.f, b.ni, b.nj))
+        return out
+
+    def interface_distribution(self, solve: int = 0):
+        """Per block of the caller's solve the reconstructed distribution
+        at its walls (get_interface_distribution, ugks_block.py:985-1047)."""
+        from .diagnostics import interface_distribution
+        out = []
+        for bi in self.solve_blocks[self.order[solve]]:
+            b = self.blocks[bi]
+            out.append(interface_distribution(self._program(bi), b.f, b.centre, b.mid_side, b.normal, b.ni, b.nj,
+                                              b.G))
+        return out
 
     def solve_block_ids(self, solve: int):
         """Indices in self.blocks of the blocks of the caller's solve."""

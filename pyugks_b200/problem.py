@@ -90,6 +90,7 @@ class Constants:
         self.Pr = _round_py2(case["Pr"])
         self.gam = _round_py2(gamma)
         self.K = _round_py2(b - 2)
+        self.B = _round_py2(b)
         self.omega = _round_py2(case["omega"])
         self.umax = _round_py2(self.vgrid.umax_exact)
         self.vmax = _round_py2(self.vgrid.vmax_exact)

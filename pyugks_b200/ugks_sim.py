@@ -121,15 +121,30 @@ class UGKSim:
         self.updateAllBC()
         return False
 
-    def run(self, max_step: int, residual_count: int = 0, min_residual: float = 0.0):
-        """Step until max_step, a NaN, or (with residual_count > 0) until every
-        residual component is <= min_residual (ugks_sim.py:542-645)."""
+    def run(self, max_step: int, residual_count: int = 0, min_residual: float = 0.0, res_drop: float = np.inf,
+            residual_start: int = 0, slope_start: float = np.inf, min_slope: float = 0.0,
+            max_time: float = np.inf):
+        """The run loop of UGKSim.run (ugks_sim.py:503-710) without its I/O:
+        step until max_step, a NaN, max_time, or one of the residual exits of
+        diagnostics.ResidualMonitor when residual_count > 0 (a residual every
+        residual_count steps).  The last step is shortened to land on
+        max_time, as the reference does.  Returns the reason it stopped; the
+        residual history is kept in self.monitor."""
+        from .diagnostics import ResidualMonitor
+        self.monitor = ResidualMonitor(min_residual, res_drop, residual_start, slope_start, min_slope)
         while self.step < max_step:
             get_res = residual_count > 0 and ((self.step + 1) % residual_count == 0)
             if self.one_step(True, get_res):
                 return "nan"
-            if get_res and np.all(self.global_residual[:4] <= min_residual):
-                return "converged"
+            if self.time >= max_time:
+                return "time limit reached"
+            if get_res:
+                why = self.monitor.record(self.step, self.global_residual)
+                if why:
+                    return why
+            if (max_time - self.time) < self.dt:
+                self.dt = max_time - self.time
+                self.force_time = True
         return "max_step"
 
     # ------------------------------------------------------------------ host views
@@ -145,6 +160,18 @@ class UGKSim:
             out.append(dict(rho=m[:, :, 0], U=m[:, :, 1], V=m[:, :, 2], T=1.0 / m[:, :, 3],
                             qx=q[:, :, 0], qy=q[:, :, 1]))
         return out
+
+    def internal_data(self):
+        """Per block (Txyz [ni, nj, 4], stress [ni, nj, 3]) from getInternal."""
+        from .diagnostics import internal_data
+        return [internal_data(b.prg, b.f_D, b.ni, b.nj, self.queue) for b in self.blocks]
+
+    def interface_distribution(self):
+        """Per block the reconstructed distribution at its four walls
+        (get_interface_distribution, ugks_block.py:985-1047)."""
+        from .diagnostics import interface_distribution
+        return [interface_distribution(b.prg, b.f_D, b.centre_D, b.side_D, b.normal_D, b.ni, b.nj, b.ghost,
+                                       self.queue) for b in self.blocks]
 
     def save_checkpoint(self, path: str, save_f: bool = True):
         """saveHDF5 + close_HDF5 (ugks_sim.py:1022-1096) into one .npz:
