@@ -23,6 +23,7 @@
 #include <float.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "ugks_device.cuh"
@@ -41,7 +42,19 @@ constexpr int FT = 128;  // threads per face / cell / ghost CTA
 #ifndef FACE_MIN_BLOCKS_WIDE
 #define FACE_MIN_BLOCKS_WIDE 4
 #endif
-constexpr int FACE_NARROW_MAX_NV = 1100;  // 6 x (32 B x 1100 + 2.5 KB) <= 228 KB
+#ifndef FACE_MIN_BLOCKS_F32
+#define FACE_MIN_BLOCKS_F32 7
+#endif
+// per storage type: the narrow and wide register budgets and the largest
+// velocity grid of the narrow one (that many face CTAs fit in shared memory:
+// FP64 6 x (32 B x 1100 + 3 KB), FP32 7 x (24 B x 1200 + 3 KB) <= 228 KB)
+template <typename T> struct FaceBudget;
+template <> struct FaceBudget<double> {
+  static constexpr int narrow = FACE_MIN_BLOCKS, wide = FACE_MIN_BLOCKS_WIDE, narrow_max_nv = 1100;
+};
+template <> struct FaceBudget<float> {
+  static constexpr int narrow = FACE_MIN_BLOCKS_F32, wide = FACE_MIN_BLOCKS_WIDE, narrow_max_nv = 1200;
+};
 #ifndef CELL_MIN_BLOCKS
 #define CELL_MIN_BLOCKS 2  // CTAs of 8 cell warps (128 registers: the update loop does not spill)
 #endif
@@ -113,23 +126,19 @@ __device__ __forceinline__ P4 micro_slope_rcp(double K, P4 prim, Rcp r, P4 sw) {
   return a;
 }
 
-__device__ __forceinline__ void moments_u_rcp(double PI, double K, P4 prim, Rcp r, double Mu[MNUM],
-                                              double Mv[MTUM], double Mxi[3], double MuL[MNUM],
-                                              double MuR[MNUM]) {
+// momentU (clUGKS.c:47-80) over one half range: sg = +1 gives the moments
+// <u^k> over u > 0 (MuL), sg = -1 those over u < 0 (MuR); Mv and Mxi are the
+// full-range moments of v and xi.  The two halves are the same instruction
+// stream with the sign flipped, so two lanes compute them side by side.
+__device__ __forceinline__ void half_moments_rcp(double PI, double K, P4 prim, Rcp r, double sg,
+                                                 double Mh[MNUM], double Mv[MTUM], double Mxi[3]) {
   const double sl = sqrt(prim.s3);
   const double g = 0.5 * exp(-prim.s3 * (prim.s1 * prim.s1)) * nr_rcp(sqrt(PI * prim.s3));
   const double hl = 0.5 * r.lam;
-  MuL[0] = 0.5 * erfc(-sl * prim.s1);
-  MuL[1] = prim.s1 * MuL[0] + g;
-  MuR[0] = 0.5 * erfc(sl * prim.s1);
-  MuR[1] = prim.s1 * MuR[0] - g;
+  Mh[0] = 0.5 * erfc((-sg * sl) * prim.s1);
+  Mh[1] = prim.s1 * Mh[0] + sg * g;
 #pragma unroll
-  for (int i = 2; i < MNUM; ++i) {
-    MuL[i] = prim.s1 * MuL[i - 1] + ((i - 1) * hl) * MuL[i - 2];
-    MuR[i] = prim.s1 * MuR[i - 1] + ((i - 1) * hl) * MuR[i - 2];
-  }
-#pragma unroll
-  for (int i = 0; i < MNUM; ++i) Mu[i] = MuL[i] + MuR[i];
+  for (int i = 2; i < MNUM; ++i) Mh[i] = prim.s1 * Mh[i - 1] + ((i - 1) * hl) * Mh[i - 2];
   Mv[0] = 1.0;
   Mv[1] = prim.s2;
 #pragma unroll
@@ -137,6 +146,16 @@ __device__ __forceinline__ void moments_u_rcp(double PI, double K, P4 prim, Rcp 
   Mxi[0] = 1.0;
   Mxi[1] = K * hl;
   Mxi[2] = (K * K + 2.0 * K) * (hl * hl);
+}
+
+// named barrier 1 between warp 0 (waits) and warp 1 (arrives): whole warps
+__device__ __forceinline__ void pair_wait() {
+  __syncwarp();
+  asm volatile("bar.sync 1, 64;" ::: "memory");
+}
+__device__ __forceinline__ void pair_arrive() {
+  __syncwarp();
+  asm volatile("bar.arrive 1, 64;" ::: "memory");
 }
 
 // 1 / relaxTime
@@ -165,6 +184,9 @@ __device__ __forceinline__ void time_weights_rcp(double inv_tau, double dt, doub
 struct FaceShared {
   double scratch[16 * (FT / 32)];
   double bcast[48];
+  double nbr[2][5];  // left / right cell: rho, u, v (face frame), lambda, 1/|mid - centre|
+  double lr[2][19];  // per side: half-range Mu [7], slope a [4], <a u psi> [4], <a u^2 psi> [4]
+  double mt[5];      // time weights
 };
 
 // WENO5 (clFunctions.c:266-313) of one component, up to the final division:
@@ -230,13 +252,80 @@ __device__ __forceinline__ void reconstruct(const typename Store<T>::vec *p, lon
   fb = Sb[MID] + sb * ds;
 }
 
+// The FP32 flux path (FP32 storage of h and b): the same reconstructions in
+// single precision.  WENO5 keeps the difference form above, with the three
+// smoothness terms e_k (>= 12e-16) divided by their sum before the products:
+// the weights only enter as ratios, the largest scaled e_k is >= 1/3 and the
+// smallest >= 1e-17, so the weight of the smoothest stencil stays a normal
+// FP32 number (>= 1e-35) while only negligible weights can underflow.
+__device__ __forceinline__ float frcp(float x) { return __fdividef(1.0f, x); }
+__device__ __forceinline__ float fsign(float a) {
+  return a > 0.0f ? 1.0f : (a < 0.0f ? -1.0f : (a == 0.0f ? a : 0.0f));
+}
+__device__ __forceinline__ float fminmod(float a, float b) {
+  float out = 0.0f;
+  if ((fabsf(a) < fabsf(b)) && (a * b > 0.0f)) out = a;
+  else if ((fabsf(b) < fabsf(a)) && (a * b > 0.0f)) out = b;
+  else if (a == b) out = a;
+  return out;
+}
+__device__ __forceinline__ void weno5_part_f(const float (&S)[5], float &num, float &den) {
+  const float D0 = S[1] - S[0], D1 = S[2] - S[1], D2 = S[3] - S[2], D3 = S[4] - S[3];
+  const float p0 = D1 - D0, p1 = D2 - D1, p2 = D3 - D2;
+  const float r0 = fmaf(3.0f, D1, -D0), r1 = D1 + D2, r2 = fmaf(-3.0f, D2, D3);
+  float e0 = 12e-16f + fmaf(13.0f * p0, p0, (3.0f * r0) * r0);
+  float e1 = 12e-16f + fmaf(13.0f * p1, p1, (3.0f * r1) * r1);
+  float e2 = 12e-16f + fmaf(13.0f * p2, p2, (3.0f * r2) * r2);
+  const float sc = frcp((e0 + e1) + e2);
+  e0 *= sc;
+  e1 *= sc;
+  e2 *= sc;
+  const float q0 = e0 * e0, q1 = e1 * e1, q2 = e2 * e2;
+  const float a0 = q1 * q2, a1 = 6.0f * (q0 * q2), a2 = 3.0f * (q0 * q1);
+  const float f0 = fmaf(-1.0f / 3.0f, D0, (5.0f / 6.0f) * D1);
+  const float f1 = fmaf(1.0f / 6.0f, D1, (1.0f / 3.0f) * D2);
+  const float f2 = fmaf(2.0f / 3.0f, D2, (-1.0f / 6.0f) * D3);
+  num = fmaf(a0, f0, fmaf(a1, f1, a2 * f2));
+  den = (a0 + a1) + a2;
+}
+template <int FM>
+__device__ __forceinline__ void reconstruct_f(const float2 *p, long st, float inv_l, float ds, float inv_ds,
+                                              float &fh, float &fb, float &sh, float &sb) {
+  constexpr int L = FM == 1 ? 5 : 3, MID = FM == 1 ? 2 : 1;
+  float Sh[L], Sb[L];
+#pragma unroll
+  for (int s = 0; s < L; ++s) {
+    const float2 x = p[s * st];
+    Sh[s] = x.x;
+    Sb[s] = x.y;
+  }
+  if constexpr (FM == 0) {
+    const float h1 = (Sh[1] - Sh[0]) * inv_l, h2 = (Sh[2] - Sh[1]) * inv_l;
+    const float b1 = (Sb[1] - Sb[0]) * inv_l, b2 = (Sb[2] - Sb[1]) * inv_l;
+    sh = (fsign(h1) + fsign(h2)) * (fabsf(h1) * fabsf(h2)) * frcp(fabsf(h1) + fabsf(h2) + 1e-16f);
+    sb = (fsign(b1) + fsign(b2)) * (fabsf(b1) * fabsf(b2)) * frcp(fabsf(b1) + fabsf(b2) + 1e-16f);
+  } else if constexpr (FM == 1) {
+    float nh, dh, nb, db;
+    weno5_part_f(Sh, nh, dh);
+    weno5_part_f(Sb, nb, db);
+    sh = nh * frcp(dh) * inv_ds;
+    sb = nb * frcp(db) * inv_ds;
+  } else {
+    sh = (0.5f * fminmod(Sh[2] - Sh[1], Sh[1] - Sh[0])) * inv_ds;
+    sb = (0.5f * fminmod(Sb[2] - Sb[1], Sb[1] - Sb[0])) * inv_ds;
+  }
+  fh = fmaf(sh, ds, Sh[MID]);
+  fb = fmaf(sb, ds, Sb[MID]);
+}
+
 // scale * exp(-lambda (x - c)^2) over the nodes of one velocity axis
-__device__ __forceinline__ void axis_exp(double *out, const double *quad, int n, int stride,
+template <typename R>
+__device__ __forceinline__ void axis_exp(R *out, const double *quad, int n, int stride,
                                          int comp, double c, double lambda, int t, int nt,
                                          double scale = 1.0) {
   for (int i = t; i < n; i += nt) {
     const double x = quad[2 * (size_t)i * stride + comp] - c;
-    out[i] = scale * exp(-lambda * (x * x));
+    out[i] = (R)(scale * exp(-lambda * (x * x)));
   }
 }
 
@@ -277,8 +366,14 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     else if (mi == d.ni && is_wall(blk.bc_type[GEAST])) wall = GEAST;
   }
 
-  // per velocity: (h, b) at the face and their slopes, kept for the later sweeps
-  double2 *fhb = reinterpret_cast<double2 *>(dyn), *sgb = fhb + Nv;
+  // per velocity: (h, b) at the face and their slopes, kept for the later
+  // sweeps, in the storage precision; the FP32 path also keeps the face-frame
+  // velocity of every node
+  constexpr bool F32 = std::is_same<T, float>::value;
+  using R = T;
+  using R2 = typename St::vec;
+  R2 *fhb = reinterpret_cast<R2 *>(dyn), *sgb = fhb + Nv;
+  float2 *uvf = reinterpret_cast<float2 *>(sgb + Nv);
   const V2 n = ld2(blk.normal, faceidx(d, gi, gj, dir));
   const V2 mid = ld2(blk.mid_side, faceidx(d, gi, gj, dir));
   // stencil geometry for both upwind directions (iFace, clUGKS.c:148-176):
@@ -306,22 +401,61 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
   // ---- sweep 1: reconstruction (+ interior faces: the face moments W of
   // getFaceCons; the 1/2 of the energy moment is applied after the sum)
   double m[4] = {0.0, 0.0, 0.0, 0.0};
+  if constexpr (F32) {
+    const float fl0 = (float)il0, fl1 = (float)il1, fd0 = (float)dist0, fd1 = (float)dist1;
+    const float fi0 = (float)idist0, fi1 = (float)idist1;
 #pragma unroll 2
-  for (int v = threadIdx.x; v < Nv; v += FT) {
-    const V2 uv = face_velocity(d, v, n);
-    const bool up = uv.x > 0.0;
-    double ffh, ffb, sx, sy;
-    reconstruct<T, FM>((up ? up1 : up0) + v, up ? step : -step, up ? il1 : il0, up ? dist1 : dist0,
-                       up ? idist1 : idist0, ffh, ffb, sx, sy);
-    fhb[v] = make_double2(ffh, ffb);
-    sgb[v] = make_double2(sx, sy);
-    if (wall < 0) {
-      const double uu = fma(uv.x, uv.x, uv.y * uv.y);
-      m[0] += ffh;
-      m[1] = fma(uv.x, ffh, m[1]);
-      m[2] = fma(uv.y, ffh, m[2]);
-      m[3] += fma(uu, ffh, ffb);
+    for (int v = threadIdx.x; v < Nv; v += FT) {
+      const V2 uv = face_velocity(d, v, n);
+      const bool up = uv.x > 0.0;
+      float ffh, ffb, sx, sy;
+      reconstruct_f<FM>((up ? up1 : up0) + v, up ? step : -step, up ? fl1 : fl0, up ? fd1 : fd0,
+                        up ? fi1 : fi0, ffh, ffb, sx, sy);
+      fhb[v] = make_float2(ffh, ffb);
+      sgb[v] = make_float2(sx, sy);
+      uvf[v] = make_float2((float)uv.x, (float)uv.y);
+      if (wall < 0) {
+        const double uu = fma(uv.x, uv.x, uv.y * uv.y), dh = ffh;
+        m[0] += dh;
+        m[1] = fma(uv.x, dh, m[1]);
+        m[2] = fma(uv.y, dh, m[2]);
+        m[3] += fma(uu, dh, (double)ffb);
+      }
     }
+  } else {
+#pragma unroll 2
+    for (int v = threadIdx.x; v < Nv; v += FT) {
+      const V2 uv = face_velocity(d, v, n);
+      const bool up = uv.x > 0.0;
+      double ffh, ffb, sx, sy;
+      reconstruct<T, FM>((up ? up1 : up0) + v, up ? step : -step, up ? il1 : il0, up ? dist1 : dist0,
+                         up ? idist1 : idist0, ffh, ffb, sx, sy);
+      fhb[v] = make_double2(ffh, ffb);
+      sgb[v] = make_double2(sx, sy);
+      if (wall < 0) {
+        const double uu = fma(uv.x, uv.x, uv.y * uv.y);
+        m[0] += ffh;
+        m[1] = fma(uv.x, ffh, m[1]);
+        m[2] = fma(uv.y, ffh, m[2]);
+        m[3] += fma(uu, ffh, ffb);
+      }
+    }
+  }
+  // the two cells beside an interior face (the inputs of getAL / getAR and
+  // the getPLR slopes, clUGKS.c:424-436), loaded by the last warp, which has
+  // the fewest velocities in sweep 1
+  if (wall < 0 && threadIdx.x >= FT - 32 && threadIdx.x < FT - 30) {
+    const int side = threadIdx.x - (FT - 32);  // 0: left (u > 0 upwind), 1: right
+    const size_t k = side == 0 ? gidx(d, gi - dir, gj - (1 - dir)) : gidx(d, gi, gj);
+    const P4 mc = ld4(blk.cell_mom, k);
+    const V2 uc = to_local(v2(mc.s1, mc.s2), n);
+    const V2 cc = ld2(blk.centre, k);
+    double *o = sh.nbr[side];
+    o[0] = mc.s0;
+    o[1] = uc.x;
+    o[2] = uc.y;
+    o[3] = mc.s3;
+    o[4] = nr_rcp(sqrt((mid.x - cc.x) * (mid.x - cc.x) + (mid.y - cc.y) * (mid.y - cc.y)));
   }
   const double len = blk.side_length[faceidx(d, gi, gj, dir)];
 
@@ -333,49 +467,66 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     const P4 prim = to_primary_rcp(d, W, rc);  // getPLR (clUGKS.c:421-422), every thread
     const int un = d.u_num, vn = d.v_num;
     const bool sep = un > 0 && un * vn == Nv && un + vn <= 512;
-    double *Eu = dyn + 4 * Nv, *Ev = Eu + (sep ? un : 0);
+    R *Eu = reinterpret_cast<R *>(F32 ? (void *)(uvf + Nv) : (void *)(sgb + Nv)), *Ev = Eu + (sep ? un : 0);
     const V2 Ug = to_global(v2(prim.s1, prim.s2), n);  // face mean velocity, global frame
     // Maxwellian prefactor rho lambda / pi (fM, clFunctions.c:49-58), times the
     // face length: every per-velocity flux below carries the length
     const double chl = (prim.s0 * (prim.s3 / d.PI)) * len;
     double q[2] = {0.0, 0.0};
     if (threadIdx.x < 32) {
+      // getPLR slopes (clUGKS.c:424-436) and initMacroFlux (446-518), split
+      // over lanes 0 / 1 of warp 0 (one per side, the same instructions)
+      // while lane 0 of warp 1 computes the time weights
+      const double kb = (0.5 * d.K) * rc.lam;
+      double Mv[MTUM], Mxi[3];
+      P4 a;
+      if (threadIdx.x < 2) {
+        const int side = threadIdx.x;
+        const double sg = side == 0 ? 1.0 : -1.0;
+        double Mh[MNUM];
+        half_moments_rcp(d.PI, d.K, prim, rc, sg, Mh, Mv, Mxi);
+        const double *o = sh.nbr[side];
+        // left: (W - W_L) / |mid - c_L|; right: (W_R - W) / |mid - c_R|
+        const double id = sg * o[4];
+        a = micro_slope_rcp(d.K, prim, rc,
+                            p4((W.s0 - o[0]) * id, (W.s1 - o[1]) * id, (W.s2 - o[2]) * id, (W.s3 - o[3]) * id));
+        const P4 t1 = moment_au(a, Mh, Mv, Mxi, 1, 0), t2 = moment_au(a, Mh, Mv, Mxi, 2, 0);
+        double *x = sh.lr[side];
+#pragma unroll
+        for (int k = 0; k < MNUM; ++k) x[k] = Mh[k];
+        x[7] = a.s0; x[8] = a.s1; x[9] = a.s2; x[10] = a.s3;
+        x[11] = t1.s0; x[12] = t1.s1; x[13] = t1.s2; x[14] = t1.s3;
+        x[15] = t2.s0; x[16] = t2.s1; x[17] = t2.s2; x[18] = t2.s3;
+      }
+      pair_wait();
+      double Mt[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) Mt[k] = sh.mt[k];
+      double *c = sh.bcast;
+      if (threadIdx.x < 2) {
+        // distFlux coefficients of the upwind slope (derivation at sweep 3)
+        const double xk = Mxi[2] - kb * kb;
+        double *ck = c + 5 * threadIdx.x;
+        ck[0] = Mt[1] * fma(0.5 * a.s3, kb, a.s0);
+        ck[1] = Mt[1] * a.s1;
+        ck[2] = Mt[1] * a.s2;
+        ck[3] = Mt[1] * (0.5 * a.s3);
+        ck[4] = Mt[1] * (0.5 * a.s3 * xk);
+      }
       if (threadIdx.x == 0) {
-        // getPLR slopes (clUGKS.c:424-436) from the cell moments of the two
-        // cells beside the face (getAL / getAR), and initMacroFlux (446-518)
-        const size_t kl = gidx(d, gi - dir, gj - (1 - dir)), kr = gidx(d, gi, gj);
-        const P4 ml = ld4(blk.cell_mom, kl), mr = ld4(blk.cell_mom, kr);
-        const V2 ul = to_local(v2(ml.s1, ml.s2), n), ur = to_local(v2(mr.s1, mr.s2), n);
-        const V2 cl = ld2(blk.centre, kl), cr = ld2(blk.centre, kr);
-        const double idl = nr_rcp(sqrt((mid.x - cl.x) * (mid.x - cl.x) + (mid.y - cl.y) * (mid.y - cl.y)));
-        const double idr = nr_rcp(sqrt((mid.x - cr.x) * (mid.x - cr.x) + (mid.y - cr.y) * (mid.y - cr.y)));
-        const P4 aL = micro_slope_rcp(d.K, prim, rc, p4((W.s0 - ml.s0) * idl, (W.s1 - ul.x) * idl,
-                                                        (W.s2 - ul.y) * idl, (W.s3 - ml.s3) * idl));
-        const P4 aR = micro_slope_rcp(d.K, prim, rc, p4((mr.s0 - W.s0) * idr, (ur.x - W.s1) * idr,
-                                                        (ur.y - W.s2) * idr, (mr.s3 - W.s3) * idr));
-        double Mu[MNUM], Mv[MTUM], Mxi[3], MuL[MNUM], MuR[MNUM], Mt[5];
-        moments_u_rcp(d.PI, d.K, prim, rc, Mu, Mv, Mxi, MuL, MuR);
+        const double *xl = sh.lr[0], *xr = sh.lr[1];
+        double Mu[MNUM];
+#pragma unroll
+        for (int k = 0; k < MNUM; ++k) Mu[k] = xl[k] + xr[k];
         const P4 aT = micro_slope_rcp(d.K, prim, rc,
-                                      scale(-prim.s0, add(moment_au(aL, MuL, Mv, Mxi, 1, 0),
-                                                          moment_au(aR, MuR, Mv, Mxi, 1, 0))));
-        time_weights_rcp(inv_relax_time_rcp(d, prim, rc), dt, Mt);
+                                      scale(-prim.s0, add(p4(xl[11], xl[12], xl[13], xl[14]),
+                                                          p4(xr[11], xr[12], xr[13], xr[14]))));
         const P4 g0 = scale(prim.s0,
                             add(add(scale(Mt[0], moment_uv(Mu, Mv, Mxi, 1, 0, 0)),
-                                    scale(Mt[1], add(moment_au(aL, MuL, Mv, Mxi, 2, 0),
-                                                     moment_au(aR, MuR, Mv, Mxi, 2, 0)))),
+                                    scale(Mt[1], add(p4(xl[15], xl[16], xl[17], xl[18]),
+                                                     p4(xr[15], xr[16], xr[17], xr[18])))),
                                 scale(Mt[2], moment_au(aT, Mu, Mv, Mxi, 1, 0))));
-        // distFlux coefficients folded per face (derivation at sweep 3)
-        const double kb = (0.5 * d.K) * rc.lam, xk = Mxi[2] - kb * kb;
-        double *c = sh.bcast;
-        const P4 as[2] = {aL, aR};
-#pragma unroll
-        for (int k = 0; k < 2; ++k) {
-          c[5 * k + 0] = Mt[1] * fma(0.5 * as[k].s3, kb, as[k].s0);
-          c[5 * k + 1] = Mt[1] * as[k].s1;
-          c[5 * k + 2] = Mt[1] * as[k].s2;
-          c[5 * k + 3] = Mt[1] * (0.5 * as[k].s3);
-          c[5 * k + 4] = Mt[1] * (0.5 * as[k].s3 * xk);
-        }
+        const double xk = Mxi[2] - kb * kb;
         c[10] = Mt[2] * fma(0.5 * aT.s3, kb, aT.s0) + Mt[0];
         c[11] = Mt[2] * aT.s1;
         c[12] = Mt[2] * aT.s2;
@@ -387,17 +538,38 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
         c[18] = len * g0.s0; c[19] = len * g0.s1; c[20] = len * g0.s2; c[21] = len * g0.s3;
       }
     } else {
+      if (threadIdx.x < 64) {
+        if (threadIdx.x == 32) {
+          double Mt[5];
+          time_weights_rcp(inv_relax_time_rcp(d, prim, rc), dt, Mt);
+#pragma unroll
+          for (int k = 0; k < 5; ++k) sh.mt[k] = Mt[k];
+        }
+        pair_arrive();
+      }
       // meanwhile: face heat flux (calcFaceQ, clUGKS.c:522-585) and the
-      // axis factors of the face Maxwellian
-      const int t = threadIdx.x - 32, nt = FT - 32;
+      // axis factors of the face Maxwellian; warp 1, which computed the time
+      // weights, takes the last offsets
+      const int t = (threadIdx.x + 32) % (FT - 32), nt = FT - 32;
       const double Kinv = 1.0 / d.K;
-      for (int v = t; v < Nv; v += nt) {
-        const V2 uv = face_velocity(d, v, n);
-        const double cx = uv.x - prim.s1, cy = uv.y - prim.s2, c2 = cx * cx + cy * cy;
-        const double2 fv = fhb[v];
-        const double tq = c2 * fv.x + fv.y * Kinv;
-        q[0] += 0.5 * (cx * tq);
-        q[1] += 0.5 * (cy * tq);
+      if constexpr (F32) {
+        const float Ux = (float)prim.s1, Uy = (float)prim.s2, Ki = (float)Kinv;
+        for (int v = t; v < Nv; v += nt) {
+          const float2 uv = uvf[v], fv = fhb[v];
+          const float cx = uv.x - Ux, cy = uv.y - Uy, c2 = fmaf(cx, cx, cy * cy);
+          const float tq = fmaf(c2, fv.x, fv.y * Ki);
+          q[0] += (double)(0.5f * (cx * tq));
+          q[1] += (double)(0.5f * (cy * tq));
+        }
+      } else {
+        for (int v = t; v < Nv; v += nt) {
+          const V2 uv = face_velocity(d, v, n);
+          const double cx = uv.x - prim.s1, cy = uv.y - prim.s2, c2 = cx * cx + cy * cy;
+          const double2 fv = fhb[v];
+          const double tq = c2 * fv.x + fv.y * Kinv;
+          q[0] += 0.5 * (cx * tq);
+          q[1] += 0.5 * (cy * tq);
+        }
       }
       if (sep) {
         axis_exp(Eu, d.quad, un, vn, 0, Ug.x, prim.s3, t, nt, chl);
@@ -429,38 +601,89 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     void *flux = dir == SOUTH ? blk.flux_S : blk.flux_W;
     const int qs = sep ? FT / vn : 0, rs = sep ? FT % vn : 0;
     int iu = sep ? threadIdx.x / vn : 0, jv = sep ? threadIdx.x % vn : 0;
-    for (int v = threadIdx.x; v < Nv; v += FT) {
-      const V2 uv = face_velocity(d, v, n);
-      const double u = uv.x, vt = uv.y, uu = fma(u, u, vt * vt);
-      const double cx = u - Ux, cy = vt - Uy, c2 = fma(cx, cx, cy * cy);
-      double E;
-      if (sep) {
-        E = Eu[iu] * Ev[jv];
-        jv += rs;
-        iu += qs;
-        if (jv >= vn) { jv -= vn; ++iu; }
-      } else {
-        E = chl * exp(-lam * c2);
+    if constexpr (F32) {
+      // the same per-velocity flux in FP32; the macro flux sums stay FP64
+      const float fUx = (float)Ux, fUy = (float)Uy, flam = (float)lam, flam2 = (float)lam2, fkb = (float)kb;
+      const float fsx = (float)sx, fsy = (float)sy, fchl = (float)chl;
+      const float fT0 = (float)T0, fT1 = (float)T1, fT2 = (float)T2, fT3 = (float)T3, fCT = (float)CT;
+      const float fMt3 = (float)Mt3, fMt4 = (float)Mt4;
+      float AL[5], AR[5];
+#pragma unroll
+      for (int k = 0; k < 5; ++k) {
+        AL[k] = (float)c[k];
+        AR[k] = (float)c[5 + k];
       }
-      const double h0 = d.weight[v] * E;
-      const double Sp = fma(cx, sx, cy * sy);
-      const double S4 = Sp * fma(lam2, c2, -4.0), S2 = fma(2.0, Sp, S4);
-      const double *A = c + (u > 0.0 ? 0 : 5);
-      const double MP = fma(A[3], uu, fma(A[2], vt, fma(A[1], u, A[0])));
-      const double Bk = fma(u, MP, fma(T3, uu, fma(T2, vt, fma(T1, u, T0))));
-      const double2 fd = fhb[v], fs = sgb[v];
-      const double mu = Mt4 * u;
-      const double Rh = fma(-mu, fs.x, Mt3 * fd.x), Rb = fma(-mu, fs.y, Mt3 * fd.y);
-      const double Zh = u * fma(S4, h0, Rh), Zb = u * fma(S2, h0 * kb, Rb);
-      const double uh = u * h0;
-      const double hx = fma(uh, Bk, Zh);
-      const double hy = fma(uh, fma(kb, Bk, fma(A[4], u, CT)), Zb);
-      acc[0] += Zh;
-      acc[1] = fma(u, Zh, acc[1]);
-      acc[2] = fma(vt, Zh, acc[2]);
-      acc[3] = fma(uu, Zh, acc[3]);
-      acc[4] += Zb;
-      St::store(flux, base + v, v2(hx, hy));
+      float2 *fl = reinterpret_cast<float2 *>(flux) + base;
+      for (int v = threadIdx.x; v < Nv; v += FT) {
+        const float2 uv = uvf[v];
+        const float u = uv.x, vt = uv.y, uu = fmaf(u, u, vt * vt);
+        const float cx = u - fUx, cy = vt - fUy, c2 = fmaf(cx, cx, cy * cy);
+        float E;
+        if (sep) {
+          E = Eu[iu] * Ev[jv];
+          jv += rs;
+          iu += qs;
+          if (jv >= vn) { jv -= vn; ++iu; }
+        } else {
+          E = fchl * expf(-flam * c2);
+        }
+        const float h0 = (float)d.weight[v] * E;
+        const float Sp = fmaf(cx, fsx, cy * fsy);
+        const float S4 = Sp * fmaf(flam2, c2, -4.0f), S2 = fmaf(2.0f, Sp, S4);
+        const bool pos = u > 0.0f;
+        const float A0 = pos ? AL[0] : AR[0], A1 = pos ? AL[1] : AR[1], A2 = pos ? AL[2] : AR[2];
+        const float A3 = pos ? AL[3] : AR[3], A4 = pos ? AL[4] : AR[4];
+        const float MP = fmaf(A3, uu, fmaf(A2, vt, fmaf(A1, u, A0)));
+        const float Bk = fmaf(u, MP, fmaf(fT3, uu, fmaf(fT2, vt, fmaf(fT1, u, fT0))));
+        const float2 fd = fhb[v], fs = sgb[v];
+        const float mu = fMt4 * u;
+        const float Rh = fmaf(-mu, fs.x, fMt3 * fd.x), Rb = fmaf(-mu, fs.y, fMt3 * fd.y);
+        const float Zh = u * fmaf(S4, h0, Rh), Zb = u * fmaf(S2, h0 * fkb, Rb);
+        const float uh = u * h0;
+        const float hx = fmaf(uh, Bk, Zh);
+        const float hy = fmaf(uh, fmaf(fkb, Bk, fmaf(A4, u, fCT)), Zb);
+        const double zh = Zh;
+        acc[0] += zh;
+        acc[1] = fma((double)u, zh, acc[1]);
+        acc[2] = fma((double)vt, zh, acc[2]);
+        acc[3] = fma((double)uu, zh, acc[3]);
+        acc[4] += (double)Zb;
+        fl[v] = make_float2(hx, hy);
+      }
+    } else {
+      for (int v = threadIdx.x; v < Nv; v += FT) {
+        const V2 uv = face_velocity(d, v, n);
+        const double u = uv.x, vt = uv.y, uu = fma(u, u, vt * vt);
+        const double cx = u - Ux, cy = vt - Uy, c2 = fma(cx, cx, cy * cy);
+        double E;
+        if (sep) {
+          E = Eu[iu] * Ev[jv];
+          jv += rs;
+          iu += qs;
+          if (jv >= vn) { jv -= vn; ++iu; }
+        } else {
+          E = chl * exp(-lam * c2);
+        }
+        const double h0 = d.weight[v] * E;
+        const double Sp = fma(cx, sx, cy * sy);
+        const double S4 = Sp * fma(lam2, c2, -4.0), S2 = fma(2.0, Sp, S4);
+        const double *A = c + (u > 0.0 ? 0 : 5);
+        const double MP = fma(A[3], uu, fma(A[2], vt, fma(A[1], u, A[0])));
+        const double Bk = fma(u, MP, fma(T3, uu, fma(T2, vt, fma(T1, u, T0))));
+        const double2 fd = fhb[v], fs = sgb[v];
+        const double mu = Mt4 * u;
+        const double Rh = fma(-mu, fs.x, Mt3 * fd.x), Rb = fma(-mu, fs.y, Mt3 * fd.y);
+        const double Zh = u * fma(S4, h0, Rh), Zb = u * fma(S2, h0 * kb, Rb);
+        const double uh = u * h0;
+        const double hx = fma(uh, Bk, Zh);
+        const double hy = fma(uh, fma(kb, Bk, fma(A[4], u, CT)), Zb);
+        acc[0] += Zh;
+        acc[1] = fma(u, Zh, acc[1]);
+        acc[2] = fma(vt, Zh, acc[2]);
+        acc[3] = fma(uu, Zh, acc[3]);
+        acc[4] += Zb;
+        St::store(flux, base + v, v2(hx, hy));
+      }
     }
     block_sum<5>(acc, sh.scratch);
     if (threadIdx.x == 0) {
@@ -474,7 +697,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
   }
 
   // ---------------- wall face ----------------
-  double *fw = reinterpret_cast<double *>(fhb);  // (h, b) per velocity
+  R *fw = reinterpret_cast<R *>(fhb);  // (h, b) per velocity, storage precision
   const int rot = (wall == GNORTH || wall == GEAST) ? -1 : 1;
   const long ci = dir == SOUTH ? mi : mj;
   P4 wl = ld4(blk.wall_prop, ci * 4 + wall);
@@ -499,8 +722,8 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
       const V2 uv = face_velocity(d, v, n);
       const int delta = upwind_flag(uv.x, rot);
       const V2 M = maxwellian(d, wl, uv, v);
-      fw[2 * v] = ratio * delta * M.x + (1 - delta) * fw[2 * v];
-      fw[2 * v + 1] = ratio * delta * M.y + (1 - delta) * fw[2 * v + 1];
+      fw[2 * v] = (R)(ratio * delta * M.x + (1 - delta) * fw[2 * v]);
+      fw[2 * v + 1] = (R)(ratio * delta * M.y + (1 - delta) * fw[2 * v + 1]);
     }
   } else {
     // adsorbingWall_P1 (clAdsorb.c:253-482)
@@ -595,12 +818,13 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     if (refl > 0.0) {
       // the reflected incoming distribution (wall_dist) of every velocity,
       // staged in the slope buffer, which wall faces do not use
-      double2 *rin = sgb;
+      R2 *rin = sgb;
       __syncthreads();
       if (kind != UGKS_REFLECT_DIFFUSE)
         for (int v = threadIdx.x; v < Nv; v += FT) {
           const V2 x = ld2(blk.wall_dist, (size_t)ci * Nv + v);
-          rin[v] = make_double2(x.x, x.y);
+          rin[v].x = (R)x.x;
+          rin[v].y = (R)x.y;
         }
       __syncthreads();
       const double an = d.alpha_n[wall], at = d.alpha_t[wall], Tw = 1.0 / wl.s3;
@@ -616,7 +840,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
             for (int va = 0; va < Nv; ++va) {
               const V2 uv_in = face_velocity(d, va, n);
               if (!upwind_flag(uv_in.x, rot) && uv_in.x != 0.0) {
-                const double2 fi = rin[va];
+                const R2 fi = rin[va];
                 const V2 c = cercignani_lampis(d.PI, uv_in, uv, v2(fi.x, fi.y), an, at, Tw, wl.s3);
                 out.x += c.x;
                 out.y += c.y;
@@ -625,12 +849,12 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
             out.x *= d.weight[v];
             out.y *= d.weight[v];
           } else {
-            const double2 x = rin[dir == WEST ? d.mirror_EW[v] : d.mirror_NS[v]];
+            const R2 x = rin[dir == WEST ? d.mirror_EW[v] : d.mirror_NS[v]];
             out = v2(x.x, x.y);
           }
         }
-        fw[2 * v] = delta * out.x + (1 - delta) * fw[2 * v];
-        fw[2 * v + 1] = delta * out.y + (1 - delta) * fw[2 * v + 1];
+        fw[2 * v] = (R)(delta * out.x + (1 - delta) * fw[2 * v]);
+        fw[2 * v + 1] = (R)(delta * out.y + (1 - delta) * fw[2 * v + 1]);
         r[0] += rot * uv.x * out.x;
       }
       block_sum<1>(r, sh.scratch);
@@ -649,8 +873,8 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
       y += delta * M.y;
       x -= account * delta * x;
       y -= account * delta * y;
-      fw[2 * v] = x;
-      fw[2 * v + 1] = y;
+      fw[2 * v] = (R)x;
+      fw[2 * v + 1] = (R)y;
     }
   }
   // wallFlux (clUGKS.c:910-1011) and wallMassEnergyFluxes (1019-1147)
@@ -1230,8 +1454,11 @@ void set_face_attributes() {
 }
 
 // shared memory of a face CTA: (h, b) and slopes per velocity + axis tables
+// (FP32: also the face-frame velocity per node, as float2)
+template <typename T>
 inline size_t face_smem(int max_nv, int max_axes) {
-  return (size_t)4 * sizeof(double) * (size_t)max_nv + sizeof(double) * (size_t)max_axes;
+  const size_t per_v = std::is_same<T, float>::value ? 3 * sizeof(float2) : 4 * sizeof(double);
+  return per_v * (size_t)max_nv + sizeof(T) * (size_t)max_axes;
 }
 
 // the main face pass of one segment (one flux method, one register budget)
@@ -1262,17 +1489,17 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
   cudaStream_t st = S(stream);
   // face pass: (h, b) and slopes per velocity + the two axis factor tables;
   // cell pass: the axis factor tables of the old and new macro state
-  const size_t smem = face_smem(z->max_nv, z->max_axes);
+  const size_t smem = face_smem<T>(z->max_nv, z->max_axes);
   const int cstride = 2 * z->max_axes + CELL_COEF;  // doubles of shared memory per cell warp
   const size_t csmem = (size_t)CW * cstride * sizeof(double);
   static bool attr_set = false;  // one flag per instantiation
   if (!attr_set) {
-    set_face_attributes<T, 0, FACE_MIN_BLOCKS>();
-    set_face_attributes<T, 1, FACE_MIN_BLOCKS>();
-    set_face_attributes<T, 3, FACE_MIN_BLOCKS>();
-    set_face_attributes<T, 0, FACE_MIN_BLOCKS_WIDE>();
-    set_face_attributes<T, 1, FACE_MIN_BLOCKS_WIDE>();
-    set_face_attributes<T, 3, FACE_MIN_BLOCKS_WIDE>();
+    set_face_attributes<T, 0, FaceBudget<T>::narrow>();
+    set_face_attributes<T, 1, FaceBudget<T>::narrow>();
+    set_face_attributes<T, 3, FaceBudget<T>::narrow>();
+    set_face_attributes<T, 0, FaceBudget<T>::wide>();
+    set_face_attributes<T, 1, FaceBudget<T>::wide>();
+    set_face_attributes<T, 3, FaceBudget<T>::wide>();
     attr_set = true;
   }
   if (smem > 200 * 1024) return -(int)cudaErrorInvalidValue;
@@ -1283,18 +1510,18 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
   mark(0);
   for (int k = 0; k < z->n_segments && k < UGKS_MAX_FACE_SEGMENTS; ++k) {
     if (z->seg_count[k] <= 0) continue;
-    const size_t sm = face_smem(z->seg_max_nv[k], z->seg_max_axes[k]);
-    if (z->seg_max_nv[k] <= FACE_NARROW_MAX_NV)
-      launch_segment<T, FACE_MIN_BLOCKS>(B, nb, solves, z->seg_method[k], z->seg_begin[k], z->seg_count[k], sm, st);
+    const size_t sm = face_smem<T>(z->seg_max_nv[k], z->seg_max_axes[k]);
+    if (z->seg_max_nv[k] <= FaceBudget<T>::narrow_max_nv)
+      launch_segment<T, FaceBudget<T>::narrow>(B, nb, solves, z->seg_method[k], z->seg_begin[k], z->seg_count[k], sm, st);
     else
-      launch_segment<T, FACE_MIN_BLOCKS_WIDE>(B, nb, solves, z->seg_method[k], z->seg_begin[k], z->seg_count[k], sm, st);
+      launch_segment<T, FaceBudget<T>::wide>(B, nb, solves, z->seg_method[k], z->seg_begin[k], z->seg_count[k], sm, st);
   }
-  const bool narrow = z->max_nv <= FACE_NARROW_MAX_NV;
+  const bool narrow = z->max_nv <= FaceBudget<T>::narrow_max_nv;
   mark(1);
   dt_check<<<sg, 128, 0, st>>>(solves, ns, 0);
   mark(2);
-  if (narrow) launch_retry<T, FACE_MIN_BLOCKS>(B, nb, z, solves, ns, smem, st);
-  else launch_retry<T, FACE_MIN_BLOCKS_WIDE>(B, nb, z, solves, ns, smem, st);
+  if (narrow) launch_retry<T, FaceBudget<T>::narrow>(B, nb, z, solves, ns, smem, st);
+  else launch_retry<T, FaceBudget<T>::wide>(B, nb, z, solves, ns, smem, st);
   mark(3);
   dt_check<<<sg, 128, 0, st>>>(solves, ns, 1);
   mark(4);
