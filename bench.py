@@ -250,7 +250,9 @@ def run_ours(args, rank, world, dist):
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": t_max / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None,
+        # mixed: FP32 per-velocity face fluxes, FP64 sums, cell update and relaxation
+        "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
         "config": {"workload": desc, "precision": args.precision, "units_per_step": units,
                    "parallelism": "replicas" if world > 1 else "single GPU",
                    "l2": "working set > 126 MB L2 (f and face fluxes %.2f GB), no flush"

@@ -404,7 +404,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
   if constexpr (F32) {
     const float fl0 = (float)il0, fl1 = (float)il1, fd0 = (float)dist0, fd1 = (float)dist1;
     const float fi0 = (float)idist0, fi1 = (float)idist1;
-#pragma unroll 2
+#pragma unroll 1
     for (int v = threadIdx.x; v < Nv; v += FT) {
       const V2 uv = face_velocity(d, v, n);
       const bool up = uv.x > 0.0;
@@ -423,7 +423,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
       }
     }
   } else {
-#pragma unroll 2
+#pragma unroll 1
     for (int v = threadIdx.x; v < Nv; v += FT) {
       const V2 uv = face_velocity(d, v, n);
       const bool up = uv.x > 0.0;
@@ -554,6 +554,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
       const double Kinv = 1.0 / d.K;
       if constexpr (F32) {
         const float Ux = (float)prim.s1, Uy = (float)prim.s2, Ki = (float)Kinv;
+#pragma unroll 1
         for (int v = t; v < Nv; v += nt) {
           const float2 uv = uvf[v], fv = fhb[v];
           const float cx = uv.x - Ux, cy = uv.y - Uy, c2 = fmaf(cx, cx, cy * cy);
@@ -614,6 +615,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
         AR[k] = (float)c[5 + k];
       }
       float2 *fl = reinterpret_cast<float2 *>(flux) + base;
+#pragma unroll 1
       for (int v = threadIdx.x; v < Nv; v += FT) {
         const float2 uv = uvf[v];
         const float u = uv.x, vt = uv.y, uu = fmaf(u, u, vt * vt);
@@ -1054,7 +1056,7 @@ __global__ void __launch_bounds__(CW * 32, CELL_MIN_BLOCKS) cell_pass(const ugks
   const int qs = sep ? 32 / vn : 0, rs = sep ? 32 % vn : 0;
   int iu = sep ? lane / vn : 0, jv = sep ? lane % vn : 0;
   bool nan = false;
-#pragma unroll 2
+#pragma unroll 1
   for (int v = lane; v < Nv; v += 32) {
     const size_t k = base + v;
     const V2 f = St::load(blk.f, k);
