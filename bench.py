@@ -344,7 +344,7 @@ def run_serving(args):
     line = {
         "metric": METRIC, "value": server.units / server.wall, "unit": UNIT, "n_gpus": 1,
         "steps": None, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
+        "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
         "config": {"workload": "serving stream: %d requests over %.1f s (Poisson 20/s, seed 2), "
                                "max %d steps or residual < 1e-6" % (len(reqs), args.arrival_seconds,
                                                                      args.max_steps),
