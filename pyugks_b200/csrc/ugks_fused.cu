@@ -63,8 +63,34 @@ template <> struct FaceBudget<float> {
 #ifndef CELL_MIN_BLOCKS_F32
 #define CELL_MIN_BLOCKS_F32 3
 #endif
-template <typename T> struct CellBudget { static constexpr int minb = CELL_MIN_BLOCKS; };
-template <> struct CellBudget<float> { static constexpr int minb = CELL_MIN_BLOCKS_F32; };
+// ...and the depth of the per-warp ring of asynchronous copies that stream
+// the f and flux rows of the cell update into shared memory
+// (FP64 only: with 8-byte FP32 elements the ring was 18% slower than plain loads)
+#ifndef CELL_RING_F64
+#define CELL_RING_F64 3
+#endif
+template <typename T> struct CellBudget { static constexpr int minb = CELL_MIN_BLOCKS, ring = CELL_RING_F64; };
+template <> struct CellBudget<float> { static constexpr int minb = CELL_MIN_BLOCKS_F32, ring = 0; };
+// shared memory of the cell-update ring: per warp, ring stages x 5 rows
+// (f, S face j, S face j+1, W face i, W face i+1) x 32 lanes
+template <typename T>
+constexpr size_t cell_ring_bytes() {
+  return (size_t)CellBudget<T>::ring * 5 * 32 * sizeof(typename Store<T>::vec);
+}
+
+// cp.async (sm_80+ asynchronous global -> shared copy of 8 or 16 bytes per
+// thread; a thread waits only for its own groups)
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *dst, const void *src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (BYTES == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(d), "l"(src), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 inline cudaStream_t S(void *s) { return reinterpret_cast<cudaStream_t>(s); }
 inline int launch_status() {
@@ -1085,12 +1111,50 @@ __global__ void __launch_bounds__(CW * 32, CellBudget<T>::minb) cell_pass(const 
   const int qs = sep ? 32 / vn : 0, rs = sep ? 32 % vn : 0;
   int iu = sep ? lane / vn : 0, jv = sep ? lane % vn : 0;
   bool nan = false;
+  // FP64: the five rows this lane reads run D velocities (of this lane)
+  // ahead through a ring of cp.async stages; a stage is refilled only after
+  // the store that consumed its values, whose operands are the stage's loads
+  constexpr int D = CellBudget<T>::ring;
+  using E = typename St::vec;
+  E *ring = reinterpret_cast<E *>(dyn + (size_t)CW * wstride) + (size_t)warp * (D * 5 * 32) + lane;
+  const E *gf = reinterpret_cast<const E *>(blk.f), *gS = reinterpret_cast<const E *>(blk.flux_S),
+          *gW = reinterpret_cast<const E *>(blk.flux_W);
+  auto issue = [&](int vv, int stage) {
+    if (D == 0) return;
+    if (vv < Nv) {
+      const size_t k = base + vv;
+      E *r = ring + stage * (5 * 32);
+      cp_async<sizeof(E)>(r, gf + k);
+      cp_async<sizeof(E)>(r + 32, gS + k);
+      cp_async<sizeof(E)>(r + 64, gS + k + sj);
+      cp_async<sizeof(E)>(r + 96, gW + k);
+      cp_async<sizeof(E)>(r + 128, gW + k + si);
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int s = 0; s < D; ++s) issue(lane + 32 * s, s);
+  int stage = 0;
 #pragma unroll 1
   for (int v = lane; v < Nv; v += 32) {
     const size_t k = base + v;
-    const V2 f = St::load(blk.f, k);
-    const V2 s0 = St::load(blk.flux_S, k), s1 = St::load(blk.flux_S, k + sj);
-    const V2 w0 = St::load(blk.flux_W, k), w1 = St::load(blk.flux_W, k + si);
+    V2 f, s0, s1, w0, w1;
+    if constexpr (D > 0) {
+      cp_async_wait<D - 1>();
+      const E *r = ring + stage * (5 * 32);
+      const E fe = r[0], s0e = r[32], s1e = r[64], w0e = r[96], w1e = r[128];
+      f = v2(fe.x, fe.y);
+      s0 = v2(s0e.x, s0e.y);
+      s1 = v2(s1e.x, s1e.y);
+      w0 = v2(w0e.x, w0e.y);
+      w1 = v2(w1e.x, w1e.y);
+    } else {
+      f = St::load(blk.f, k);
+      s0 = St::load(blk.flux_S, k);
+      s1 = St::load(blk.flux_S, k + sj);
+      w0 = St::load(blk.flux_W, k);
+      w1 = St::load(blk.flux_W, k + si);
+    }
     const V2 e = quad_at(d, v);
     const double wv = d.weight[v];
     const double ox = e.x - old.s1, oy = e.y - old.s2, o2 = fma(ox, ox, oy * oy);
@@ -1116,7 +1180,12 @@ __global__ void __launch_bounds__(CW * 32, CellBudget<T>::minb) cell_pass(const 
     const V2 out = v2(fma(f.x, a1, fma(flh, a2, eh)), fma(f.y, a1, fma(flb, a2, eb)));
     nan |= isnan(out.x) || isnan(out.y);
     St::store(blk.f, k, out);
+    if constexpr (D > 0) {
+      issue(v + 32 * D, stage);
+      stage = stage + 1 == D ? 0 : stage + 1;
+    }
   }
+  if constexpr (D > 0) cp_async_wait<0>();
   if (nan) atomicExch(&sol.status, 1);
   // moments of f^{n+1} for the next face pass, and calcQ (clKernel.c:480-543)
   // of f^{n+1} with the new macro for the next cell pass: a second sweep over
@@ -1522,7 +1591,7 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
   // cell pass: the axis factor tables of the old and new macro state
   const size_t smem = face_smem<T>(z->max_nv, z->max_axes);
   const int cstride = 2 * z->max_axes + CELL_COEF;  // doubles of shared memory per cell warp
-  const size_t csmem = (size_t)CW * cstride * sizeof(double);
+  const size_t csmem = (size_t)CW * cstride * sizeof(double) + (size_t)CW * cell_ring_bytes<T>();
   static bool attr_set = false;  // one flag per instantiation
   if (!attr_set) {
     set_face_attributes<T, 0, FaceBudget<T>::narrow>();
@@ -1531,9 +1600,10 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
     set_face_attributes<T, 0, FaceBudget<T>::wide>();
     set_face_attributes<T, 1, FaceBudget<T>::wide>();
     set_face_attributes<T, 3, FaceBudget<T>::wide>();
+    cudaFuncSetAttribute(cell_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_set = true;
   }
-  if (smem > 200 * 1024) return -(int)cudaErrorInvalidValue;
+  if (smem > 200 * 1024 || csmem > 200 * 1024) return -(int)cudaErrorInvalidValue;
   const unsigned sg = (unsigned)((ns + 127) / 128);
   auto mark = [&](int k) {
     if (events) cudaEventRecord(reinterpret_cast<cudaEvent_t>(events[k]), st);
