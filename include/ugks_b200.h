@@ -290,6 +290,11 @@ typedef struct ugks_fused_block {
   double *Q_next;              /* [ni][nj] x 2: calcQ of f^{n+1} with the macro of
                                   step n+1, accumulated by the cell pass of step n
                                   and moved to Q by the cell pass of step n+1 */
+  double *face_geo;            /* [Ni][Nj][2] x 6: reconstruction geometry of every
+                                  face (iFace, clUGKS.c:148-176): |mid - c|, its
+                                  reciprocal and 1/|c - c'| for the u <= 0 stencil,
+                                  then the same for u > 0; written by ugks_init_* and
+                                  ugks_restart_* from centre and mid_side */
 } ugks_fused_block;
 
 typedef struct ugks_solve_state {

@@ -47,7 +47,7 @@ class FusedBlock(C.Structure):
         ("macro", vp), ("Q", vp), ("prim_old", vp),
         ("area", vp), ("centre", vp), ("mid_side", vp), ("normal", vp), ("side_length", vp),
         ("xy", vp), ("wall_prop", vp), ("wall_cover", vp), ("wall_fluxes", vp), ("wall_dist", vp),
-        ("cell_mom", vp), ("Q_next", vp),
+        ("cell_mom", vp), ("Q_next", vp), ("face_geo", vp),
     ]
 
 

@@ -367,6 +367,42 @@ __device__ __forceinline__ void axis_exp(R *out, const double *quad, int n, int 
   }
 }
 
+// stencil geometry of a face for both upwind directions (iFace,
+// clUGKS.c:148-176): |mid - c|, 1/|mid - c| and 1/|c - c'| with c, c' the
+// cells MID and MID-1 from the face (u <= 0), then the cells before the face
+// (u > 0)
+__device__ __forceinline__ void stencil_geometry(const ugks_fused_block &blk, long gi, long gj, int dir, V2 mid,
+                                                 double *out) {
+  const ugks_block_desc &d = blk.d;
+  auto geo = [&](long c0, long c1, double *o) {
+    const long c0i = dir == SOUTH ? gi : gi + c0, c0j = dir == SOUTH ? gj + c0 : gj;
+    const long c1i = dir == SOUTH ? gi : gi + c1, c1j = dir == SOUTH ? gj + c1 : gj;
+    const V2 a = ld2(blk.centre, gidx(d, c0i, c0j)), b = ld2(blk.centre, gidx(d, c1i, c1j));
+    o[0] = sqrt((mid.x - a.x) * (mid.x - a.x) + (mid.y - a.y) * (mid.y - a.y));
+    o[1] = 1.0 / o[0];
+    o[2] = 1.0 / sqrt((a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y));
+  };
+  geo(0, 1, out);        // u <= 0
+  geo(-1, -2, out + 3);  // u > 0
+}
+
+// the same for every face, once at set-up (read by the FP64 face pass)
+__global__ void face_geometry(const ugks_fused_block *__restrict__ B, int nb, int n_faces) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= n_faces) return;
+  const int bi = find_block<0>(B, nb, w);
+  const ugks_fused_block &blk = B[bi];
+  const ugks_block_desc &d = blk.d;
+  int lf = w - blk.face_begin;
+  const int dir = lf & 1;
+  lf >>= 1;
+  const int mi = lf / (d.nj + 1), mj = lf % (d.nj + 1);
+  if (dir == SOUTH ? (mi >= d.ni) : (mj >= d.nj)) return;
+  const long gi = mi + d.ghost, gj = mj + d.ghost;
+  stencil_geometry(blk, gi, gj, dir, ld2(blk.mid_side, faceidx(d, gi, gj, dir)),
+                   blk.face_geo + 6 * faceidx(d, gi, gj, dir));
+}
+
 // one face work item (all threads of the CTA take part)
 template <typename T, int FM>
 __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B, int nb,
@@ -416,19 +452,17 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
   const V2 mid = ld2(blk.mid_side, faceidx(d, gi, gj, dir));
   // stencil geometry for both upwind directions (iFace, clUGKS.c:148-176):
   // index 1 for u > 0 (upwind cell before the face), 0 otherwise
-  double dist0, dist1, idist0, idist1, il0, il1;
-  {
-    auto geo = [&](long c0, long c1, double &ds, double &ids, double &il) {
-      const long c0i = dir == SOUTH ? gi : gi + c0, c0j = dir == SOUTH ? gj + c0 : gj;
-      const long c1i = dir == SOUTH ? gi : gi + c1, c1j = dir == SOUTH ? gj + c1 : gj;
-      const V2 a = ld2(blk.centre, gidx(d, c0i, c0j)), b = ld2(blk.centre, gidx(d, c1i, c1j));
-      ds = sqrt((mid.x - a.x) * (mid.x - a.x) + (mid.y - a.y) * (mid.y - a.y));
-      ids = 1.0 / ds;
-      il = 1.0 / sqrt((a.x - b.x) * (a.x - b.x) + (a.y - b.y) * (a.y - b.y));
-    };
-    geo(0, 1, dist0, idist0, il0);     // cells MID and MID-1 relative to the face, u <= 0
-    geo(-1, -2, dist1, idist1, il1);   // u > 0
+  // (FP64: precomputed by face_geometry; FP32: computed here, which measured
+  // faster than waiting for the loads)
+  double g6[6];
+  if constexpr (std::is_same<T, float>::value) {
+    stencil_geometry(blk, gi, gj, dir, mid, g6);
+  } else {
+    const double *fg = blk.face_geo + 6 * faceidx(d, gi, gj, dir);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) g6[k] = fg[k];
   }
+  const double dist0 = g6[0], idist0 = g6[1], il0 = g6[2], dist1 = g6[3], idist1 = g6[4], il1 = g6[5];
   const int step = dir == SOUTH ? Nv : d.Nj * Nv;
   const size_t base = fidx(d, gi, gj, 0);
   constexpr int MID = FM == 1 ? 2 : 1;
@@ -1528,6 +1562,7 @@ int init_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
               int ns, void *stream) {
   cudaStream_t st = S(stream);
   init_walls<<<nb, 128, 0, st>>>(B, nb);
+  if (z->n_faces) face_geometry<<<(z->n_faces + 127) / 128, 128, 0, st>>>(B, nb, z->n_faces);
   if (z->n_cells) init_cells<T><<<z->n_cells, FT, 0, st>>>(B, nb, solves);
   dt_init<<<(ns + 127) / 128, 128, 0, st>>>(solves, ns);
   if (z->n_ghost) ghost_pass<T><<<z->n_ghost, FT, 0, st>>>(B, nb, solves);
@@ -1539,6 +1574,7 @@ int restart_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, u
                  int ns, void *stream) {
   cudaStream_t st = S(stream);
   init_walls<<<nb, 128, 0, st>>>(B, nb);
+  if (z->n_faces) face_geometry<<<(z->n_faces + 127) / 128, 128, 0, st>>>(B, nb, z->n_faces);
   if (z->n_cells) restart_cells<T><<<z->n_cells, FT, 0, st>>>(B, nb, solves);
   dt_init<<<(ns + 127) / 128, 128, 0, st>>>(solves, ns);
   if (z->n_ghost) ghost_pass<T><<<z->n_ghost, FT, 0, st>>>(B, nb, solves);

@@ -179,6 +179,7 @@ class FusedSolver:
         blk.wall_dist = z(wl, Nv, 2)
         blk.cell_mom = z(Ni, Nj, 4)
         blk.Q_next = z(ni, nj, 2)
+        blk.face_geo = z(Ni, Nj, 2, 6)
         x = _lib.FusedBlock()
         d = x.d
         d.ni, d.nj, d.Ni, d.Nj, d.ghost, d.Nv = ni, nj, Ni, Nj, G, Nv
@@ -201,7 +202,7 @@ class FusedSolver:
         x.solve = s
         for name in ("f", "flux_S", "flux_W", "flux_macro_S", "flux_macro_W", "macro", "Q", "prim_old",
                      "area", "centre", "mid_side", "normal", "side_length", "xy", "wall_prop",
-                     "wall_cover", "wall_fluxes", "wall_dist", "cell_mom", "Q_next"):
+                     "wall_cover", "wall_fluxes", "wall_dist", "cell_mom", "Q_next", "face_geo"):
             setattr(x, name, getattr(blk, name).data_ptr())
         blk.struct = x
         return blk
