@@ -403,6 +403,31 @@ __global__ void face_geometry(const ugks_fused_block *__restrict__ B, int nb, in
                    blk.face_geo + 6 * faceidx(d, gi, gj, dir));
 }
 
+// block_sum whose result only thread 0 needs
+template <int N>
+__device__ __forceinline__ void block_sum_to0(double (&x)[N], double *scratch) {
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x[k] += __shfl_xor_sync(0xffffffffu, x[k], o);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) scratch[k * nw + warp] = x[k];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      double s = 0.0;
+      for (int w = 0; w < nw; ++w) s += scratch[k * nw + w];
+      x[k] = s;
+    }
+  }
+}
+
 // one face work item (all threads of the CTA take part)
 template <typename T, int FM>
 __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B, int nb,
@@ -450,6 +475,14 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
   float2 *uvf = reinterpret_cast<float2 *>(sgb + Nv);
   const V2 n = ld2(blk.normal, faceidx(d, gi, gj, dir));
   const V2 mid = ld2(blk.mid_side, faceidx(d, gi, gj, dir));
+  // velocity tables and the face-frame velocity (interfaceVelocity,
+  // clFunctions.c:191-209), with the table pointers held in registers
+  const double2 *__restrict__ qd = reinterpret_cast<const double2 *>(d.quad);
+  const double *__restrict__ wt = d.weight;
+  auto fvel = [&](int vv) {
+    const double2 e = qd[vv];
+    return v2(e.x * n.x + e.y * n.y, e.x * (-n.y) + e.y * n.x);
+  };
   // stencil geometry for both upwind directions (iFace, clUGKS.c:148-176):
   // index 1 for u > 0 (upwind cell before the face), 0 otherwise
   // (FP64: precomputed by face_geometry; FP32: computed here, which measured
@@ -482,7 +515,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     float2 nx[L];
     V2 nuv = v2(0.0, 0.0);
     if (threadIdx.x < Nv) {
-      nuv = face_velocity(d, threadIdx.x, n);
+      nuv = fvel(threadIdx.x);
       const bool upn = nuv.x > 0.0;
       load_stencil<L>((upn ? up1 : up0) + threadIdx.x, upn ? step : -step, nx);
     }
@@ -493,7 +526,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
       for (int k = 0; k < L; ++k) cur[k] = nx[k];
       const V2 uv = nuv;
       if (v + FT < Nv) {
-        nuv = face_velocity(d, v + FT, n);
+        nuv = fvel(v + FT);
         const bool upn = nuv.x > 0.0;
         load_stencil<L>((upn ? up1 : up0) + v + FT, upn ? step : -step, nx);
       }
@@ -514,7 +547,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
   } else {
 #pragma unroll 1
     for (int v = threadIdx.x; v < Nv; v += FT) {
-      const V2 uv = face_velocity(d, v, n);
+      const V2 uv = fvel(v);
       const bool up = uv.x > 0.0;
       double ffh, ffb, sx, sy;
       reconstruct<T, FM>((up ? up1 : up0) + v, up ? step : -step, up ? il1 : il0, up ? dist1 : dist0,
@@ -653,7 +686,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
         }
       } else {
         for (int v = t; v < Nv; v += nt) {
-          const V2 uv = face_velocity(d, v, n);
+          const V2 uv = fvel(v);
           const double cx = uv.x - prim.s1, cy = uv.y - prim.s2, c2 = cx * cx + cy * cy;
           const double2 fv = fhb[v];
           const double tq = c2 * fv.x + fv.y * Kinv;
@@ -718,7 +751,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
         } else {
           E = fchl * expf(-flam * c2);
         }
-        const float h0 = (float)d.weight[v] * E;
+        const float h0 = (float)wt[v] * E;
         const float Sp = fmaf(cx, fsx, cy * fsy);
         const float S4 = Sp * fmaf(flam2, c2, -4.0f), S2 = fmaf(2.0f, Sp, S4);
         const bool pos = u > 0.0f;
@@ -743,7 +776,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
       }
     } else {
       for (int v = threadIdx.x; v < Nv; v += FT) {
-        const V2 uv = face_velocity(d, v, n);
+        const V2 uv = fvel(v);
         const double u = uv.x, vt = uv.y, uu = fma(u, u, vt * vt);
         const double cx = u - Ux, cy = vt - Uy, c2 = fma(cx, cx, cy * cy);
         double E;
@@ -755,7 +788,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
         } else {
           E = chl * exp(-lam * c2);
         }
-        const double h0 = d.weight[v] * E;
+        const double h0 = wt[v] * E;
         const double Sp = fma(cx, sx, cy * sy);
         const double S4 = Sp * fma(lam2, c2, -4.0), S2 = fma(2.0, Sp, S4);
         const double *A = c + (u > 0.0 ? 0 : 5);
@@ -776,7 +809,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
         St::store(flux, base + v, v2(hx, hy));
       }
     }
-    block_sum<5>(acc, sh.scratch);
+    block_sum_to0<5>(acc, sh.scratch);
     if (threadIdx.x == 0) {
       P4 out = p4(acc[0] + c[18], acc[1] + c[19], acc[2] + c[20], 0.5 * (acc[3] + acc[4]) + c[21]);
       const V2 g = to_global(v2(out.s1, out.s2), n);
@@ -802,7 +835,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     // accommodatingWallDist (clUGKS.c:774-906)
     double s[2] = {0.0, 0.0};
     for (int v = threadIdx.x; v < Nv; v += FT) {
-      const V2 uv = face_velocity(d, v, n);
+      const V2 uv = fvel(v);
       const int delta = upwind_flag(uv.x, rot);
       s[0] += uv.x * (1 - delta) * fw[2 * v];
       s[1] -= uv.x * delta * maxwellian(d, wl, uv, v).x;
@@ -810,7 +843,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     block_sum<2>(s, sh.scratch);
     const double ratio = s[0] / s[1];
     for (int v = threadIdx.x; v < Nv; v += FT) {
-      const V2 uv = face_velocity(d, v, n);
+      const V2 uv = fvel(v);
       const int delta = upwind_flag(uv.x, rot);
       const V2 M = maxwellian(d, wl, uv, v);
       fw[2 * v] = (R)(ratio * delta * M.x + (1 - delta) * fw[2 * v]);
@@ -826,7 +859,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     const double gf = d.gamma_f[wall];
     double s[3] = {0.0, 0.0, 0.0};
     for (int v = threadIdx.x; v < Nv; v += FT) {
-      const V2 uv = face_velocity(d, v, n);
+      const V2 uv = fvel(v);
       const int delta = upwind_flag(uv.x, rot);
       const double k = -rot * uv.x * (1 - delta);
       const V2 total = v2(k * fw[2 * v], k * fw[2 * v + 1]);
@@ -921,7 +954,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
       const double an = d.alpha_n[wall], at = d.alpha_t[wall], Tw = 1.0 / wl.s3;
       double r[1] = {0.0};
       for (int v = threadIdx.x; v < Nv; v += FT) {
-        const V2 uv = face_velocity(d, v, n);
+        const V2 uv = fvel(v);
         const int delta = upwind_flag(uv.x, rot);
         V2 out = v2(0.0, 0.0);
         if (delta) {
@@ -929,7 +962,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
             out = maxwellian(d, wl, uv, v);
           } else if (kind == UGKS_REFLECT_CL) {
             for (int va = 0; va < Nv; ++va) {
-              const V2 uv_in = face_velocity(d, va, n);
+              const V2 uv_in = fvel(va);
               if (!upwind_flag(uv_in.x, rot) && uv_in.x != 0.0) {
                 const R2 fi = rin[va];
                 const V2 c = cercignani_lampis(d.PI, uv_in, uv, v2(fi.x, fi.y), an, at, Tw, wl.s3);
@@ -937,8 +970,8 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
                 out.y += c.y;
               }
             }
-            out.x *= d.weight[v];
-            out.y *= d.weight[v];
+            out.x *= wt[v];
+            out.y *= wt[v];
           } else {
             const R2 x = rin[dir == WEST ? d.mirror_EW[v] : d.mirror_NS[v]];
             out = v2(x.x, x.y);
@@ -955,7 +988,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     P4 wd = wl;
     wd.s0 = 2 * des * sqrt(d.PI * wl.s3);
     for (int v = threadIdx.x; v < Nv; v += FT) {
-      const V2 uv = face_velocity(d, v, n);
+      const V2 uv = fvel(v);
       const int delta = upwind_flag(uv.x, rot);
       const double sc = 1 - delta * (1 - ratio);
       double x = fw[2 * v] * sc, y = fw[2 * v + 1] * sc;
@@ -974,7 +1007,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
 #pragma unroll
   for (int k = 0; k < 12; ++k) s[k] = 0.0;
   for (int v = threadIdx.x; v < Nv; v += FT) {
-    const V2 uv = face_velocity(d, v, n);
+    const V2 uv = fvel(v);
     const double wh = fw[2 * v], wb = fw[2 * v + 1];
     const double oh = uv.x * wh * len * dt, ob = uv.x * wb * len * dt;
     St::store(flux, base + v, v2(oh, ob));
