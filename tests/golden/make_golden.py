@@ -20,6 +20,8 @@ Cases:
                (adsorbingWallCL_P2, alpha_n 0.5, alpha_t 0.7) re-emission
   channel8_isotherm
                channel8 with a tabulated Langmuir isotherm (configs.langmuir_table)
+  cavity8_minmod
+               cavity8 with the minmod (NND) limiter, FLUX_METHOD 3, CFL 0.5
   cavity32     the 32x32 cavity, 25x25 velocities on [-4,4]^2, vanLeer, Kn 0.075,
                CFL 0.8, lid 0.15 (fields at steps 1/10/100/1000)
   cavity32_perturbed
@@ -52,6 +54,8 @@ CASES = {
                                             alpha_t=0.7), (1, 10, 30), True),
     "channel8_isotherm": (lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0,
                                                   adsorb=configs.langmuir_table()), (1, 10, 30), True),
+    "cavity8_minmod": (lambda: configs.cavity(n=8, m=8, vlim=4.0, flux_method="minmod", CFL=0.5),
+                       (1, 10, 50), True),
 }
 
 

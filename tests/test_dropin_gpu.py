@@ -117,6 +117,7 @@ def tee_sim(case):
 
 CASES = {
     "cavity_vanleer": lambda: configs.cavity(n=8, m=8, vlim=4.0),
+    "cavity_minmod": lambda: configs.cavity(n=8, m=8, vlim=4.0, flux_method="minmod", CFL=0.5),
     "multiblock_weno5": lambda: configs.cavity_multiblock(nb=2, n=8, m=8),
     "channel_langmuir": lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0),
     "channel_first_order": lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.01),

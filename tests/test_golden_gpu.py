@@ -20,6 +20,7 @@ CASES = {
     "multiblock8": (lambda: configs.cavity_multiblock(nb=2, n=8, m=8), (1, 10, 30)),
     "channel8": (lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0), (1, 10, 30)),
     "cavity32": (lambda: configs.cavity(n=32, m=24, vlim=4.0), (1, 10, 100, 1000)),
+    "cavity8_minmod": (lambda: configs.cavity(n=8, m=8, vlim=4.0, flux_method="minmod", CFL=0.5), (1, 10, 50)),
 }
 
 
@@ -70,7 +71,7 @@ def test_fused_fp64_matches_golden(cuda, name):
         check(g, s, gpu.fields(), gpu.interior_f(), st["dt"], st["time"], name)
 
 
-@pytest.mark.parametrize("name", ["cavity8", "multiblock8", "channel8"])
+@pytest.mark.parametrize("name", ["cavity8", "multiblock8", "channel8", "cavity8_minmod"])
 def test_dropin_driver_matches_golden(cuda, name):
     make, steps = CASES[name]
     g = np.load(os.path.join(GOLDEN, name + ".npz"))

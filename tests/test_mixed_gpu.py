@@ -1,7 +1,8 @@
 """Mixed precision (FP32 f and face fluxes, FP64 moments / conserved update /
 relaxation / dt) against the plain FP64 step: relative L2 error of density,
 velocity, temperature and heat flux <= 1e-5 on small versions of every
-workload (cavity, multi-block WENO5 cavity, adsorbing channel, a mixed batch)."""
+workload (cavity with each limiter, multi-block WENO5 cavity, adsorbing
+channel, a mixed batch)."""
 import pytest
 
 from pyugks_b200 import configs
@@ -13,6 +14,7 @@ L2_TOL = 1e-5
 
 @pytest.mark.parametrize("make", [
     lambda: [configs.cavity(n=16, m=24, vlim=4.0)],
+    lambda: [configs.cavity(n=12, m=16, vlim=4.0, flux_method="minmod", CFL=0.5)],
     lambda: [configs.cavity_multiblock(nb=2, n=8, m=16)],
     lambda: [configs.channel(nblocks=2, n=8, m=16)],
     lambda: [configs.cavity(n=12, m=16, vlim=5.0, flux_method="WENO5", Kn=0.01),

@@ -25,6 +25,7 @@ CASES = {
                                             alpha_t=0.7), (1, 10, 30)),
     "channel8_isotherm": (lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0,
                                                   adsorb=configs.langmuir_table()), (1, 10, 30)),
+    "cavity8_minmod": (lambda: configs.cavity(n=8, m=8, vlim=4.0, flux_method="minmod", CFL=0.5), (1, 10, 50)),
 }
 # the Cercignani-Lampis kernel's Bessel I0: a power series in the port, a
 # rational approximation in the reference
