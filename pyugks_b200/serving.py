@@ -44,7 +44,7 @@ def footprint_bytes(case: dict, precision: str) -> int:
     for b in case["blocks"]:
         Ni, Nj = b["ni"] + 2 * G, b["nj"] + 2 * G
         total += 3 * Ni * Nj * nv * 2 * es
-        total += Ni * Nj * 8 * (4 * 3 + 2 * 2 + 2 * 2 + 1 + 2 + 2 * 2 + 2)
+        total += Ni * Nj * 8 * (4 * 3 + 2 * 2 + 2 * 2 + 1 + 2 + 2 * 2 + 2 + 2 * 6)  # incl. face_geo
         total += max(b["ni"], b["nj"]) * 4 * 8 * (4 + 4 + 8) + max(b["ni"], b["nj"]) * nv * 16
     return total
 
