@@ -33,27 +33,41 @@ using namespace ugks;
 namespace {
 
 constexpr int FT = 128;  // threads per face / cell / ghost CTA
-// face kernels come in two register budgets: FACE_MIN_BLOCKS CTAs per SM
-// (fits while 32 B x Nv of shared memory per face allows that many) and
-// FACE_MIN_BLOCKS_WIDE for larger velocity grids
+// face kernels come in two shapes: narrow, FT threads per face at
+// FACE_MIN_BLOCKS CTAs per SM (fits while the per-face shared memory allows
+// that many), and wide, for larger velocity grids, where shared memory allows
+// only 2-3 faces per SM: 384 (FP64) or 256 (FP32) threads per face keep the
+// warps per SM up (config-3 batch: face pass 29.6 -> 23.7 ms FP64, 20.1 ->
+// 18.1 ms FP32, against 128 threads)
 #ifndef FACE_MIN_BLOCKS
 #define FACE_MIN_BLOCKS 6
 #endif
-#ifndef FACE_MIN_BLOCKS_WIDE
-#define FACE_MIN_BLOCKS_WIDE 4
-#endif
 #ifndef FACE_MIN_BLOCKS_F32
 #define FACE_MIN_BLOCKS_F32 7
+#endif
+#ifndef FACE_MIN_BLOCKS_WIDE
+#define FACE_MIN_BLOCKS_WIDE 2
+#endif
+#ifndef FACE_MIN_BLOCKS_WIDE_F32
+#define FACE_MIN_BLOCKS_WIDE_F32 3
+#endif
+#ifndef FACE_WIDE_THREADS
+#define FACE_WIDE_THREADS 384
+#endif
+#ifndef FACE_WIDE_THREADS_F32
+#define FACE_WIDE_THREADS_F32 256
 #endif
 // per storage type: the narrow and wide register budgets and the largest
 // velocity grid of the narrow one (that many face CTAs fit in shared memory:
 // FP64 6 x (32 B x 1100 + 3 KB), FP32 7 x (24 B x 1200 + 3 KB) <= 228 KB)
 template <typename T> struct FaceBudget;
 template <> struct FaceBudget<double> {
-  static constexpr int narrow = FACE_MIN_BLOCKS, wide = FACE_MIN_BLOCKS_WIDE, narrow_max_nv = 1100;
+  static constexpr int narrow = FACE_MIN_BLOCKS, wide = FACE_MIN_BLOCKS_WIDE, narrow_max_nv = 1100,
+                       wide_threads = FACE_WIDE_THREADS;
 };
 template <> struct FaceBudget<float> {
-  static constexpr int narrow = FACE_MIN_BLOCKS_F32, wide = FACE_MIN_BLOCKS_WIDE, narrow_max_nv = 1200;
+  static constexpr int narrow = FACE_MIN_BLOCKS_F32, wide = FACE_MIN_BLOCKS_WIDE_F32, narrow_max_nv = 1200,
+                       wide_threads = FACE_WIDE_THREADS_F32;
 };
 // CTAs of 8 cell warps per SM: FP64 at 128 registers (at 80 the update loop
 // spills and the pass is 12% slower), FP32 storage at 80 (6% faster than 128)
@@ -214,8 +228,9 @@ __device__ __forceinline__ void time_weights_rcp(double inv_tau, double dt, doub
   Mt[2] = 0.5 * (dt * dt) - tau * Mt[0];
 }
 
+template <int NT>
 struct FaceShared {
-  double scratch[16 * (FT / 32)];
+  double scratch[16 * (NT / 32)];
   double bcast[48];
   double nbr[2][5];  // left / right cell: rho, u, v (face frame), lambda, 1/|mid - centre|
   double lr[2][19];  // per side: half-range Mu [7], slope a [4], <a u psi> [4], <a u^2 psi> [4]
@@ -429,12 +444,12 @@ __device__ __forceinline__ void block_sum_to0(double (&x)[N], double *scratch) {
 }
 
 // one face work item (all threads of the CTA take part)
-template <typename T, int FM>
+template <typename T, int FM, int NT>
 __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B, int nb,
                                           ugks_solve_state *__restrict__ solves, const int w,
                                           int retry_pass) {
   extern __shared__ double dyn[];
-  __shared__ FaceShared sh;
+  __shared__ FaceShared<NT> sh;
   using St = Store<T>;
 
   const int bi = find_block<0>(B, nb, w);
@@ -520,15 +535,15 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
       load_stencil<L>((upn ? up1 : up0) + threadIdx.x, upn ? step : -step, nx);
     }
 #pragma unroll 1
-    for (int v = threadIdx.x; v < Nv; v += FT) {
+    for (int v = threadIdx.x; v < Nv; v += NT) {
       float2 cur[L];
 #pragma unroll
       for (int k = 0; k < L; ++k) cur[k] = nx[k];
       const V2 uv = nuv;
-      if (v + FT < Nv) {
-        nuv = fvel(v + FT);
+      if (v + NT < Nv) {
+        nuv = fvel(v + NT);
         const bool upn = nuv.x > 0.0;
-        load_stencil<L>((upn ? up1 : up0) + v + FT, upn ? step : -step, nx);
+        load_stencil<L>((upn ? up1 : up0) + v + NT, upn ? step : -step, nx);
       }
       const bool up = uv.x > 0.0;
       float ffh, ffb, sx, sy;
@@ -546,7 +561,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     }
   } else {
 #pragma unroll 1
-    for (int v = threadIdx.x; v < Nv; v += FT) {
+    for (int v = threadIdx.x; v < Nv; v += NT) {
       const V2 uv = fvel(v);
       const bool up = uv.x > 0.0;
       double ffh, ffb, sx, sy;
@@ -566,8 +581,8 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
   // the two cells beside an interior face (the inputs of getAL / getAR and
   // the getPLR slopes, clUGKS.c:424-436), loaded by the last warp, which has
   // the fewest velocities in sweep 1
-  if (wall < 0 && threadIdx.x >= FT - 32 && threadIdx.x < FT - 30) {
-    const int side = threadIdx.x - (FT - 32);  // 0: left (u > 0 upwind), 1: right
+  if (wall < 0 && threadIdx.x >= NT - 32 && threadIdx.x < NT - 30) {
+    const int side = threadIdx.x - (NT - 32);  // 0: left (u > 0 upwind), 1: right
     const size_t k = side == 0 ? gidx(d, gi - dir, gj - (1 - dir)) : gidx(d, gi, gj);
     const P4 mc = ld4(blk.cell_mom, k);
     const V2 uc = to_local(v2(mc.s1, mc.s2), n);
@@ -672,7 +687,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
       // meanwhile: face heat flux (calcFaceQ, clUGKS.c:522-585) and the
       // axis factors of the face Maxwellian; warp 1, which computed the time
       // weights, takes the last offsets
-      const int t = (threadIdx.x + 32) % (FT - 32), nt = FT - 32;
+      const int t = (threadIdx.x + NT - 96) % (NT - 32), nt = NT - 32;
       const double Kinv = 1.0 / d.K;
       if constexpr (F32) {
         const float Ux = (float)prim.s1, Uy = (float)prim.s2, Ki = (float)Kinv;
@@ -722,7 +737,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     const double T0 = c[10], T1 = c[11], T2 = c[12], T3 = c[13], CT = c[14];
     double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     void *flux = dir == SOUTH ? blk.flux_S : blk.flux_W;
-    const int qs = sep ? FT / vn : 0, rs = sep ? FT % vn : 0;
+    const int qs = sep ? NT / vn : 0, rs = sep ? NT % vn : 0;
     int iu = sep ? threadIdx.x / vn : 0, jv = sep ? threadIdx.x % vn : 0;
     if constexpr (F32) {
       // the same per-velocity flux in FP32; the macro flux sums stay FP64
@@ -738,7 +753,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
       }
       float2 *fl = reinterpret_cast<float2 *>(flux) + base;
 #pragma unroll 1
-      for (int v = threadIdx.x; v < Nv; v += FT) {
+      for (int v = threadIdx.x; v < Nv; v += NT) {
         const float2 uv = uvf[v];
         const float u = uv.x, vt = uv.y, uu = fmaf(u, u, vt * vt);
         const float cx = u - fUx, cy = vt - fUy, c2 = fmaf(cx, cx, cy * cy);
@@ -775,7 +790,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
         fl[v] = make_float2(hx, hy);
       }
     } else {
-      for (int v = threadIdx.x; v < Nv; v += FT) {
+      for (int v = threadIdx.x; v < Nv; v += NT) {
         const V2 uv = fvel(v);
         const double u = uv.x, vt = uv.y, uu = fma(u, u, vt * vt);
         const double cx = u - Ux, cy = vt - Uy, c2 = fma(cx, cx, cy * cy);
@@ -834,7 +849,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
   if (blk.bc_type[wall] == BC_DIFFUSE) {
     // accommodatingWallDist (clUGKS.c:774-906)
     double s[2] = {0.0, 0.0};
-    for (int v = threadIdx.x; v < Nv; v += FT) {
+    for (int v = threadIdx.x; v < Nv; v += NT) {
       const V2 uv = fvel(v);
       const int delta = upwind_flag(uv.x, rot);
       s[0] += uv.x * (1 - delta) * fw[2 * v];
@@ -842,7 +857,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     }
     block_sum<2>(s, sh.scratch);
     const double ratio = s[0] / s[1];
-    for (int v = threadIdx.x; v < Nv; v += FT) {
+    for (int v = threadIdx.x; v < Nv; v += NT) {
       const V2 uv = fvel(v);
       const int delta = upwind_flag(uv.x, rot);
       const V2 M = maxwellian(d, wl, uv, v);
@@ -858,7 +873,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     const double theta = cover[0];
     const double gf = d.gamma_f[wall];
     double s[3] = {0.0, 0.0, 0.0};
-    for (int v = threadIdx.x; v < Nv; v += FT) {
+    for (int v = threadIdx.x; v < Nv; v += NT) {
       const V2 uv = fvel(v);
       const int delta = upwind_flag(uv.x, rot);
       const double k = -rot * uv.x * (1 - delta);
@@ -919,7 +934,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     const double corr = sh.bcast[0];
     const bool ok = sh.bcast[1] != 0.0;
     if (corr != 1.0)
-      for (int v = threadIdx.x; v < Nv; v += FT) {
+      for (int v = threadIdx.x; v < Nv; v += NT) {
         const size_t k = (size_t)ci * Nv + v;
         const V2 x = ld2(blk.wall_dist, k);
         st2(blk.wall_dist, k, v2(x.x * corr, x.y * corr));
@@ -930,7 +945,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
       // there, the face values of (h, b), and its face macro flux is not
       // written this step
       void *fl = dir == SOUTH ? blk.flux_S : blk.flux_W;
-      for (int v = threadIdx.x; v < Nv; v += FT) St::store(fl, base + v, v2(fw[2 * v], fw[2 * v + 1]));
+      for (int v = threadIdx.x; v < Nv; v += NT) St::store(fl, base + v, v2(fw[2 * v], fw[2 * v + 1]));
       return;
     }
     // re-emission of the reflected flux: adsorbingWallD_P2 (clAdsorb.c:821-975,
@@ -945,7 +960,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
       R2 *rin = sgb;
       __syncthreads();
       if (kind != UGKS_REFLECT_DIFFUSE)
-        for (int v = threadIdx.x; v < Nv; v += FT) {
+        for (int v = threadIdx.x; v < Nv; v += NT) {
           const V2 x = ld2(blk.wall_dist, (size_t)ci * Nv + v);
           rin[v].x = (R)x.x;
           rin[v].y = (R)x.y;
@@ -953,7 +968,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
       __syncthreads();
       const double an = d.alpha_n[wall], at = d.alpha_t[wall], Tw = 1.0 / wl.s3;
       double r[1] = {0.0};
-      for (int v = threadIdx.x; v < Nv; v += FT) {
+      for (int v = threadIdx.x; v < Nv; v += NT) {
         const V2 uv = fvel(v);
         const int delta = upwind_flag(uv.x, rot);
         V2 out = v2(0.0, 0.0);
@@ -987,7 +1002,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     const int account = ((des == 0.0) && (ads > 0.0) && (refl == 0.0)) ? 1 : 0;
     P4 wd = wl;
     wd.s0 = 2 * des * sqrt(d.PI * wl.s3);
-    for (int v = threadIdx.x; v < Nv; v += FT) {
+    for (int v = threadIdx.x; v < Nv; v += NT) {
       const V2 uv = fvel(v);
       const int delta = upwind_flag(uv.x, rot);
       const double sc = 1 - delta * (1 - ratio);
@@ -1006,7 +1021,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
   double s[12];
 #pragma unroll
   for (int k = 0; k < 12; ++k) s[k] = 0.0;
-  for (int v = threadIdx.x; v < Nv; v += FT) {
+  for (int v = threadIdx.x; v < Nv; v += NT) {
     const V2 uv = fvel(v);
     const double wh = fw[2 * v], wb = fw[2 * v + 1];
     const double oh = uv.x * wh * len * dt, ob = uv.x * wb * len * dt;
@@ -1033,18 +1048,18 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
 }
 
 // main face pass: one CTA per face work item of the blocks of one flux method
-template <typename T, int FM, int MINB>
-__global__ void __launch_bounds__(FT, MINB) face_pass(const ugks_fused_block *__restrict__ B, int nb,
+template <typename T, int FM, int MINB, int NT>
+__global__ void __launch_bounds__(NT, MINB) face_pass(const ugks_fused_block *__restrict__ B, int nb,
                                                                  ugks_solve_state *__restrict__ solves,
                                                                  int first) {
-  face_item<T, FM>(B, nb, solves, first + (int)blockIdx.x, 0);
+  face_item<T, FM, NT>(B, nb, solves, first + (int)blockIdx.x, 0);
 }
 
 // the flux pass redone after a dt change (ugks_sim.py:432-441): RETRY_CTAS
 // CTAs per solve; a solve whose retry flag is clear costs one early exit each
 constexpr int RETRY_CTAS = 148;
-template <typename T, int FM, int MINB>
-__global__ void __launch_bounds__(FT, MINB) face_retry(const ugks_fused_block *__restrict__ B, int nb,
+template <typename T, int FM, int MINB, int NT>
+__global__ void __launch_bounds__(NT, MINB) face_retry(const ugks_fused_block *__restrict__ B, int nb,
                                                                   ugks_solve_state *__restrict__ solves,
                                                                   int ns) {
   const int s = blockIdx.x / RETRY_CTAS, r = blockIdx.x % RETRY_CTAS;
@@ -1055,7 +1070,7 @@ __global__ void __launch_bounds__(FT, MINB) face_retry(const ugks_fused_block *_
   if (b0.d.flux_method != FM) return;
   const int end = bl.face_begin + 2 * (bl.d.ni + 1) * (bl.d.nj + 1);
   for (int w = b0.face_begin + r; w < end; w += RETRY_CTAS) {
-    face_item<T, FM>(B, nb, solves, w, 1);
+    face_item<T, FM, NT>(B, nb, solves, w, 1);
     __syncthreads();  // the next item reuses the shared tables
   }
 }
@@ -1614,11 +1629,11 @@ int restart_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, u
   return launch_status();
 }
 
-template <typename T, int FM, int MINB>
+template <typename T, int FM, int MINB, int NT>
 void set_face_attributes() {
-  cudaFuncSetAttribute(face_pass<T, FM, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(face_retry<T, FM, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(face_pass<T, FM, MINB>, cudaFuncAttributePreferredSharedMemoryCarveout,
+  cudaFuncSetAttribute(face_pass<T, FM, MINB, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(face_retry<T, FM, MINB, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  cudaFuncSetAttribute(face_pass<T, FM, MINB, NT>, cudaFuncAttributePreferredSharedMemoryCarveout,
                        cudaSharedmemCarveoutMaxShared);
 }
 
@@ -1631,25 +1646,25 @@ inline size_t face_smem(int max_nv, int max_axes) {
 }
 
 // the main face pass of one segment (one flux method, one register budget)
-template <typename T, int MINB>
+template <typename T, int MINB, int NT>
 void launch_segment(const ugks_fused_block *B, int nb, ugks_solve_state *solves, int method, int first,
                     int count, size_t smem, cudaStream_t st) {
   switch (method) {
-    case 0: face_pass<T, 0, MINB><<<count, FT, smem, st>>>(B, nb, solves, first); break;
-    case 1: face_pass<T, 1, MINB><<<count, FT, smem, st>>>(B, nb, solves, first); break;
-    case 3: face_pass<T, 3, MINB><<<count, FT, smem, st>>>(B, nb, solves, first); break;
+    case 0: face_pass<T, 0, MINB, NT><<<count, NT, smem, st>>>(B, nb, solves, first); break;
+    case 1: face_pass<T, 1, MINB, NT><<<count, NT, smem, st>>>(B, nb, solves, first); break;
+    case 3: face_pass<T, 3, MINB, NT><<<count, NT, smem, st>>>(B, nb, solves, first); break;
     default: break;
   }
 }
 
 // the retry pass of every flux method (per solve; rare)
-template <typename T, int MINB>
+template <typename T, int MINB, int NT>
 void launch_retry(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks_solve_state *solves,
                   int ns, size_t smem, cudaStream_t st) {
   const unsigned rg = (unsigned)ns * RETRY_CTAS;
-  if (z->face_count[0]) face_retry<T, 0, MINB><<<rg, FT, smem, st>>>(B, nb, solves, ns);
-  if (z->face_count[1]) face_retry<T, 1, MINB><<<rg, FT, smem, st>>>(B, nb, solves, ns);
-  if (z->face_count[3]) face_retry<T, 3, MINB><<<rg, FT, smem, st>>>(B, nb, solves, ns);
+  if (z->face_count[0]) face_retry<T, 0, MINB, NT><<<rg, NT, smem, st>>>(B, nb, solves, ns);
+  if (z->face_count[1]) face_retry<T, 1, MINB, NT><<<rg, NT, smem, st>>>(B, nb, solves, ns);
+  if (z->face_count[3]) face_retry<T, 3, MINB, NT><<<rg, NT, smem, st>>>(B, nb, solves, ns);
 }
 
 template <typename T>
@@ -1663,12 +1678,12 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
   const size_t csmem = (size_t)CW * cstride * sizeof(double) + (size_t)CW * cell_ring_bytes<T>();
   static bool attr_set = false;  // one flag per instantiation
   if (!attr_set) {
-    set_face_attributes<T, 0, FaceBudget<T>::narrow>();
-    set_face_attributes<T, 1, FaceBudget<T>::narrow>();
-    set_face_attributes<T, 3, FaceBudget<T>::narrow>();
-    set_face_attributes<T, 0, FaceBudget<T>::wide>();
-    set_face_attributes<T, 1, FaceBudget<T>::wide>();
-    set_face_attributes<T, 3, FaceBudget<T>::wide>();
+    set_face_attributes<T, 0, FaceBudget<T>::narrow, FT>();
+    set_face_attributes<T, 1, FaceBudget<T>::narrow, FT>();
+    set_face_attributes<T, 3, FaceBudget<T>::narrow, FT>();
+    set_face_attributes<T, 0, FaceBudget<T>::wide, FaceBudget<T>::wide_threads>();
+    set_face_attributes<T, 1, FaceBudget<T>::wide, FaceBudget<T>::wide_threads>();
+    set_face_attributes<T, 3, FaceBudget<T>::wide, FaceBudget<T>::wide_threads>();
     cudaFuncSetAttribute(cell_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_set = true;
   }
@@ -1682,16 +1697,16 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
     if (z->seg_count[k] <= 0) continue;
     const size_t sm = face_smem<T>(z->seg_max_nv[k], z->seg_max_axes[k]);
     if (z->seg_max_nv[k] <= FaceBudget<T>::narrow_max_nv)
-      launch_segment<T, FaceBudget<T>::narrow>(B, nb, solves, z->seg_method[k], z->seg_begin[k], z->seg_count[k], sm, st);
+      launch_segment<T, FaceBudget<T>::narrow, FT>(B, nb, solves, z->seg_method[k], z->seg_begin[k], z->seg_count[k], sm, st);
     else
-      launch_segment<T, FaceBudget<T>::wide>(B, nb, solves, z->seg_method[k], z->seg_begin[k], z->seg_count[k], sm, st);
+      launch_segment<T, FaceBudget<T>::wide, FaceBudget<T>::wide_threads>(B, nb, solves, z->seg_method[k], z->seg_begin[k], z->seg_count[k], sm, st);
   }
   const bool narrow = z->max_nv <= FaceBudget<T>::narrow_max_nv;
   mark(1);
   dt_check<<<sg, 128, 0, st>>>(solves, ns, 0);
   mark(2);
-  if (narrow) launch_retry<T, FaceBudget<T>::narrow>(B, nb, z, solves, ns, smem, st);
-  else launch_retry<T, FaceBudget<T>::wide>(B, nb, z, solves, ns, smem, st);
+  if (narrow) launch_retry<T, FaceBudget<T>::narrow, FT>(B, nb, z, solves, ns, smem, st);
+  else launch_retry<T, FaceBudget<T>::wide, FaceBudget<T>::wide_threads>(B, nb, z, solves, ns, smem, st);
   mark(3);
   dt_check<<<sg, 128, 0, st>>>(solves, ns, 1);
   mark(4);

@@ -84,3 +84,16 @@ def test_isotherm_outside_the_table_flags_status_4(cuda):
 def test_cavity_mixed_precision(cuda):
     ora, gpu = run_both(configs.cavity(n=8, m=8, vlim=4.0), 30, precision="mixed")
     assert fields_err(gpu.fields(), ora.fields()) < MIXED_TOL
+
+
+@pytest.mark.parametrize("flux_method", ["vanLeer", "WENO5"])
+def test_wide_velocity_grid(cuda, flux_method):
+    """49 x 49 = 2401 velocities: above the narrow kernels' shared-memory limit,
+    so the face pass runs its wide shape (more threads per face)."""
+    case = lambda: configs.cavity(n=6, m=48, vlim=5.0, flux_method=flux_method, Kn=0.05, CFL=0.3)
+    ora, gpu = run_both(case(), 12)
+    assert gpu.blocks[0].Nv == 2401
+    assert fields_err(gpu.fields(), ora.fields()) < FP64_TOL
+    assert rel_err(gpu.interior_f()[0], ora.interior_f()[0]) < FP64_TOL
+    ora, mixed = run_both(case(), 12, precision="mixed")
+    assert fields_err(mixed.fields(), ora.fields()) < MIXED_TOL
