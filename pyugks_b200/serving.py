@@ -151,10 +151,12 @@ class SolvePool:
             _lib.check(self._step_fn(self._table.data_ptr(), self._nblocks, C.byref(self._sizes),
                                      self._states.data_ptr(), len(self._order), stream), "ugks_step")
 
-    def states(self):
-        """{id: solve record dict} with the residual of the last step."""
+    def states(self, rebuild=True):
+        """{id: solve record dict} with the residual of the last step.  With
+        rebuild=False the solves admitted since the last step are left out
+        (they have not stepped yet)."""
         import torch
-        if self._dirty:
+        if self._dirty and rebuild:
             self._rebuild()
         if self._table is None:
             return {}
@@ -196,31 +198,49 @@ class Server:
 
     def run(self, requests, time_limit=None):
         """Serve a list of Request (arrival in seconds from the start).
-        Returns the completed requests."""
+        Returns the completed requests.
+
+        A tick's steps are launched first; requests that arrived meanwhile are
+        then set up (allocation, geometry, initialisation) on a side stream
+        while the tick runs, and join the table at the next tick."""
         import torch
+        dev = self.pool.device
+        main = torch.cuda.current_stream(dev)
+        side = torch.cuda.Stream(device=dev)
         queue = sorted(requests, key=lambda r: r.arrival)
         waiting = []
         active = {}
         t0 = time.perf_counter()
         i = 0
-        while i < len(queue) or waiting or active:
+
+        def arrivals():
+            nonlocal i
             now = time.perf_counter() - t0
-            if time_limit is not None and now > time_limit:
-                break
             while i < len(queue) and queue[i].arrival <= now:
                 waiting.append(queue[i])
                 i += 1
-            # admit in arrival order while the footprint fits
+            return now
+
+        def admit():
+            # in arrival order while the footprint fits
             while waiting:
                 r = waiting[0]
                 need = footprint_bytes(r.case, self.precision)
                 if self.used + need > self.budget and active:
                     break
                 waiting.pop(0)
-                sid = self.pool.admit(r.case)
+                with torch.cuda.stream(side):
+                    sid = self.pool.admit(r.case)
                 r.admitted, r.need, r.sid = time.perf_counter() - t0, need, sid
                 self.used += need
                 active[sid] = r
+
+        while i < len(queue) or waiting or active:
+            now = arrivals()
+            if time_limit is not None and now > time_limit:
+                break
+            admit()
+            main.wait_stream(side)
             if not active:
                 if i < len(queue):
                     time.sleep(max(0.0, min(queue[i].arrival - now, 0.05)))
@@ -228,7 +248,10 @@ class Server:
             units = self.pool.units_per_step()
             self.pool.step(self.steps_per_tick)
             self.units += units * self.steps_per_tick
-            states = self.pool.states()   # synchronises
+            arrivals()
+            admit()                                      # overlaps the tick
+            states = self.pool.states(rebuild=False)     # synchronises
+            main.wait_stream(side)
             now = time.perf_counter() - t0
             for sid, st in states.items():
                 r = active[sid]
