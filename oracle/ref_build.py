@@ -34,7 +34,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_OUT = os.path.join(HERE, "_ref")
-DEFAULT_REFERENCE = "/root/reference"
+# the pyUGKS checkout: $UGKS_REFERENCE, else a directory named "reference"
+# beside this repository's root
+DEFAULT_REFERENCE = os.path.normpath(os.path.join(HERE, os.pardir, os.pardir, "reference"))
 
 sys.path.insert(0, HERE)
 import ugks_setup as us  # noqa: E402

@@ -58,6 +58,29 @@ def inflow(D_=1.0, T=1.0):
     return dict(type=D.INFLOW, D=D_, T=T, U=0.0, V=0.0)
 
 
+def constant(D_=1.0, T=1.0, U=0.0, V=0.0):
+    """``ConstantBC`` (``geom/geom_bc_defs.py:262-290``): ghosts hold
+    fEQ(D, U, V, T), U and V global x/y."""
+    return dict(type=D.CONSTANT, D=D_, T=T, U=U, V=V)
+
+
+def outflow(P=1.0, D_=1.0, T=1.0):
+    """``OutflowBC`` (``geom/geom_bc_defs.py:431-444``) with its D set as
+    well: the wall value P/D becomes the ghost's lambda = rho_cell / (D / (P/D))
+    (``clGhostRoutines.c:755-839``).  The class itself leaves D at 0, which
+    makes that lambda infinite, so a usable outflow face sets D too."""
+    return dict(type=D.OUTFLOW, D=D_, T=T, U=0.0, V=0.0, P=P)
+
+
+def periodic(other_block, other_face, orientation=0, flip=D.NO_FLIP):
+    """A PERIODIC face (BC code 5): copied through ``edgeExchange`` like an
+    ADJACENT one; its ghost vertices are extrapolated (``ugks_block.py:726-733``).
+    orientation 0 (HOLD) keeps the along-face order although the two faces'
+    corners lie apart."""
+    return dict(type=D.PERIODIC, other_block=other_block, other_face=other_face,
+                orientation=orientation, flip=flip, transform=D.TRANSFORM, flip_normal=0)
+
+
 def reflect():
     return dict(type=D.REFLECT)
 
@@ -164,6 +187,151 @@ def warped_cavity(nb=1, n=16, m=8, vlim=4.0, flux_method="vanLeer", Kn=0.05, lid
         if nb > 1 else cavity(n=n, m=m, vlim=vlim, flux_method=flux_method, Kn=Kn, lid=lid, CFL=CFL)
     for b in case["blocks"]:
         b["x"], b["y"] = warp_grid(b["x"], b["y"], amp)
+    return case
+
+
+# ---------------------------------------------------------------------------
+# block connections and open faces beyond the opposite-face, aligned pairs of
+# the cavity and channel: every one is a flow that makes physical sense, so
+# that several steps of it are a parity case, not only a copy test
+# ---------------------------------------------------------------------------
+
+def _fill(ni, nj, rho=1.0):
+    return dict(D=rho if np.ndim(rho) else float(rho), U=0.0, V=0.0, T=1.0, qx=0.0, qy=0.0)
+
+
+def rotated_pair(n=8, m=8, vlim=4.0, flux_method="vanLeer", Kn=0.05, lid=0.15, CFL=0.3):
+    """The unit-square cavity as two blocks whose grids are turned 90 degrees
+    against each other, joined NORTH to EAST (getSwapIndex's rotation
+    branches, clGhostRoutines.c:47-138).
+
+    A covers [0,1] x [0,1/2] (i along +x, j along +y, n x n/2 cells).  B covers
+    [0,1] x [1/2,1] with i along -y and j along +x (n/2 x n cells), so B's EAST
+    face lies on y = 1/2 against A's NORTH face, B's WEST face is the lid
+    (y = 1), its NORTH face the right wall and its SOUTH face the left wall."""
+    h = n // 2
+    case = base_case(flux_method, Kn, m, vlim, CFL)
+    xa, ya = uniform_grid(n, h, 0.0, 1.0, 0.0, 0.5)
+    i = np.arange(h + 1, dtype=np.float64)[:, None]
+    j = np.arange(n + 1, dtype=np.float64)[None, :]
+    xb = np.ascontiguousarray(j / n + 0.0 * i)
+    yb = np.ascontiguousarray(1.0 - 0.5 * (i / h) + 0.0 * j)
+    bc_a = [None] * 4
+    bc_a[D.NORTH] = adjacent(1, D.EAST)
+    bc_a[D.EAST], bc_a[D.SOUTH], bc_a[D.WEST] = diffuse(1.0), diffuse(1.0), diffuse(1.0)
+    bc_b = [None] * 4
+    bc_b[D.EAST] = adjacent(0, D.NORTH)
+    bc_b[D.WEST] = diffuse(1.0, U=lid)
+    bc_b[D.NORTH], bc_b[D.SOUTH] = diffuse(1.0), diffuse(1.0)
+    rho = smoothed_density(n, seed=4)
+    case["blocks"].append(dict(ni=n, nj=h, x=xa, y=ya, bc=bc_a,
+                               fill=_fill(n, h, np.ascontiguousarray(rho[:, :h]))))
+    # B's cell (i, j) sits at x index j, y index n - 1 - i of the square
+    case["blocks"].append(dict(ni=h, nj=n, x=xb, y=yb, bc=bc_b,
+                               fill=_fill(h, n, np.ascontiguousarray(rho[:, h:][:, ::-1].T))))
+    return case
+
+
+def flipped_pair(n=8, m=8, vlim=4.0, flux_method="vanLeer", Kn=0.05, lid=0.15, CFL=0.3):
+    """The unit-square cavity as two blocks joined NORTH to NORTH, the upper
+    block's grid turned 180 degrees: the two faces' corner vertices lie
+    apart, so with orientation 1 edgeExchange reverses the along-face index
+    (clGhostRoutines.c:506-513) before getSwapIndex.
+
+    A covers [0,1] x [0,1/2] (n x n/2 cells); B covers [0,1] x [1/2,1] with i
+    along -x and j along -y, so B's NORTH face lies on y = 1/2, its SOUTH face
+    is the lid, its EAST face the left wall and its WEST face the right wall.
+    Both sides copy vertices without the affine map (NO_TRANSFORM): the map
+    would send B's corner 1 onto A's corner 1, which the turned grid does not
+    share."""
+    h = n // 2
+    case = base_case(flux_method, Kn, m, vlim, CFL)
+    xa, ya = uniform_grid(n, h, 0.0, 1.0, 0.0, 0.5)
+    i = np.arange(n + 1, dtype=np.float64)[:, None]
+    j = np.arange(h + 1, dtype=np.float64)[None, :]
+    xb = np.ascontiguousarray(1.0 - i / n + 0.0 * j)
+    yb = np.ascontiguousarray(1.0 - 0.5 * (j / h) + 0.0 * i)
+    link = lambda other: dict(adjacent(other, D.NORTH, orientation=1), transform=D.NO_TRANSFORM)
+    bc_a = [None] * 4
+    bc_a[D.NORTH] = link(1)
+    bc_a[D.EAST], bc_a[D.SOUTH], bc_a[D.WEST] = diffuse(1.0), diffuse(1.0), diffuse(1.0)
+    bc_b = [None] * 4
+    bc_b[D.NORTH] = link(0)
+    bc_b[D.SOUTH] = diffuse(1.0, U=lid)
+    bc_b[D.EAST], bc_b[D.WEST] = diffuse(1.0), diffuse(1.0)
+    rho = smoothed_density(n, seed=5)
+    case["blocks"].append(dict(ni=n, nj=h, x=xa, y=ya, bc=bc_a,
+                               fill=_fill(n, h, np.ascontiguousarray(rho[:, :h]))))
+    # B's cell (i, j) sits at x index n - 1 - i, y index n - 1 - j
+    case["blocks"].append(dict(ni=n, nj=h, x=xb, y=yb, bc=bc_b,
+                               fill=_fill(n, h, np.ascontiguousarray(rho[::-1, ::-1][:, :h]))))
+    return case
+
+
+def mirror_cavity(n=8, m=8, vlim=4.0, flux_method="vanLeer", Kn=0.05, lid=0.15, CFL=0.3):
+    """A single-block cavity whose faces other than the lid are connected to
+    themselves through the velocity permutations of edgeExchange
+    (clGhostRoutines.c:517-535): SOUTH to SOUTH with FLIP_NS (a symmetry
+    plane, the same ghosts as REFLECT), WEST to WEST with FLIP_EW and EAST to
+    EAST with FLIP_D (a bounce-back wall).  Their ghost vertices are the
+    interior ones mirrored about the face (the MIRROR map of xyExchange)."""
+    case = base_case(flux_method, Kn, m, vlim, CFL)
+    x, y = uniform_grid(n, n)
+    bc = [None] * 4
+    bc[D.NORTH] = diffuse(1.0, U=lid)
+    # the ghost vertices are the interior ones mirrored about the face
+    # (xyExchange with the MIRROR map, clGhostRoutines.c:273-275)
+    self_link = lambda face, flip: dict(adjacent(0, face, flip=flip), transform=D.MIRROR)
+    bc[D.SOUTH] = self_link(D.SOUTH, D.FLIP_NS)
+    bc[D.WEST] = self_link(D.WEST, D.FLIP_EW)
+    bc[D.EAST] = self_link(D.EAST, D.FLIP_D)
+    case["blocks"].append(dict(ni=n, nj=n, x=x, y=y, bc=bc,
+                               fill=_fill(n, n, smoothed_density(n, seed=6))))
+    return case
+
+
+def periodic_couette(n=8, m=8, vlim=4.0, flux_method="WENO5", Kn=0.05, lid=0.15, CFL=0.3):
+    """Plane Couette flow, periodic in x, as two blocks of n/2 x n cells side
+    by side: A.EAST joins B.WEST (ADJACENT), B.EAST joins A.WEST as a
+    PERIODIC face (code 5) with orientation 0; the lid (NORTH) moves, the
+    floor (SOUTH) is at rest.  The density starts perturbed so that the
+    solution varies along x too."""
+    h = n // 2
+    case = base_case(flux_method, Kn, m, vlim, CFL)
+    rho = smoothed_density(n, seed=7)
+    for b in range(2):
+        x, y = uniform_grid(h, n, 0.5 * b, 0.5 * (b + 1), 0.0, 1.0)
+        bc = [None] * 4
+        bc[D.NORTH] = diffuse(1.0, U=lid)
+        bc[D.SOUTH] = diffuse(1.0)
+        if b == 0:
+            bc[D.EAST] = adjacent(1, D.WEST)
+            bc[D.WEST] = periodic(1, D.EAST)
+        else:
+            bc[D.WEST] = adjacent(0, D.EAST)
+            bc[D.EAST] = periodic(0, D.WEST)
+        case["blocks"].append(dict(ni=h, nj=n, x=x, y=y, bc=bc,
+                                   fill=_fill(h, n, np.ascontiguousarray(rho[b * h:(b + 1) * h, :]))))
+    return case
+
+
+def open_channel(nblocks=2, n=8, m=8, vlim=5.0, flux_method="WENO5", Kn=0.05, rho_in=1.2, u_in=0.05,
+                 P_out=1.0, D_out=1.0, length=2.0, height=1.0, CFL=0.3, nj=None):
+    """A channel between diffuse walls, fed through a CONSTANT inlet
+    (fEQ(rho_in, u_in, 0, T=1) ghosts, edgeConstant, clGhostRoutines.c:603-658)
+    and drained through an OUTFLOW face (edgeOutflow, 755-839, with P_out and
+    D_out set)."""
+    nj = n if nj is None else nj
+    case = base_case(flux_method, Kn, m, vlim, CFL)
+    for b in range(nblocks):
+        x, y = uniform_grid(n, nj, length * b / nblocks, length * (b + 1) / nblocks, 0.0, height)
+        bc = [None] * 4
+        bc[D.NORTH], bc[D.SOUTH] = diffuse(1.0), diffuse(1.0)
+        bc[D.WEST] = adjacent(b - 1, D.EAST) if b > 0 else constant(rho_in, 1.0, U=u_in)
+        bc[D.EAST] = adjacent(b + 1, D.WEST) if b + 1 < nblocks else outflow(P_out, D_out)
+        xc = 0.5 * (x[1:, :-1] + x[:-1, :-1])
+        rho = rho_in + (1.0 - rho_in) * xc / length
+        case["blocks"].append(dict(ni=n, nj=nj, x=x, y=y, bc=bc, fill=_fill(n, nj, np.ascontiguousarray(rho))))
     return case
 
 

@@ -137,6 +137,28 @@ __device__ __forceinline__ V2 shakhov_eq(const ugks_block_desc &d, P4 prim, V2 Q
   return v2(M.x + S.x, M.y + S.y);
 }
 
+// clFindDT (clKernel.c:224-308): the CFL frequency (dx u + dy v) / A of
+// interior cell (mi, mj) with macro state m (rho, U, V, lambda); Kn is the
+// host's unrounded Kn that ugks_block.py:1421 passes.  The drop-in kernel,
+// the fused cell and set-up passes and the allocation-free query all call it.
+__device__ __forceinline__ double cfl_frequency(const ugks_block_desc &d, const double *xy,
+                                                const double *area, P4 m, long mi, long mj,
+                                                double Kn) {
+  const long G = d.ghost, NY = d.Nj + 1;
+  const V2 a = ld2(xy, (mi + 1 + G) * NY + mj + G), b = ld2(xy, (mi + 1 + G) * NY + mj + 1 + G);
+  const V2 c = ld2(xy, (mi + G) * NY + mj + 1 + G), e = ld2(xy, (mi + G) * NY + mj + G);
+  const double dx = fmax(fmax(fmax(fabs(a.x - b.x), fabs(c.x - b.x)), fmax(fabs(c.x - e.x), fabs(a.x - e.x))),
+                         fmax(fabs(c.x - a.x), fabs(b.x - e.x)));
+  const double dy = fmax(fmax(fmax(fabs(a.y - b.y), fabs(c.y - b.y)), fmax(fabs(c.y - e.y), fabs(a.y - e.y))),
+                         fmax(fabs(c.y - a.y), fabs(b.y - e.y)));
+  const double sos = sqrt(0.5 * d.gam / m.s3);
+  const double lo_u = fmin(d.umax, fabs(m.s1) + sos), lo_v = fmin(d.vmax, fabs(m.s2) + sos);
+  const double hi_u = fmax(d.umax, fabs(m.s1) + sos), hi_v = fmax(d.vmax, fabs(m.s2) + sos);
+  const double sc = (erf(10 * (Kn - 1e-3)) + 1) / 2.0;
+  const double u = sc * (hi_u - lo_u) + lo_u, v = sc * (hi_v - lo_v) + lo_v;
+  return (dx * u + dy * v) / area[gidx(d, mi + G, mj + G)];
+}
+
 // getPrimary / getConserved / microSlope (clUGKS.c:16-45)
 __device__ __forceinline__ P4 to_primary(const ugks_block_desc &d, P4 w) {
   P4 p = w;

@@ -23,6 +23,7 @@
 #include <float.h>
 
 #include <algorithm>
+#include <mutex>
 #include <type_traits>
 #include <vector>
 
@@ -1079,23 +1080,9 @@ __global__ void __launch_bounds__(NT, MINB) face_retry(const ugks_fused_block *_
 // cell pass: calcQ (clKernel.c:480-543) + updateMacro (clUGKS.c:1158-1187) +
 // UGKS_update (clUGKS.c:1189-1257) + clFindDT (clKernel.c:224-308)
 // ---------------------------------------------------------------------------
+// clFindDT with the descriptor's Kn (the host's unrounded Kn, ugks_block.py:1421)
 __device__ __forceinline__ double cfl_freq(const ugks_fused_block &blk, P4 m, long mi, long mj) {
-  const ugks_block_desc &d = blk.d;
-  const long G = d.ghost, NY = d.Nj + 1;
-  const double *xy = blk.xy;
-  const V2 a = ld2(xy, (mi + 1 + G) * NY + mj + G), b = ld2(xy, (mi + 1 + G) * NY + mj + 1 + G);
-  const V2 c = ld2(xy, (mi + G) * NY + mj + 1 + G), e = ld2(xy, (mi + G) * NY + mj + G);
-  const double dx = fmax(fmax(fmax(fabs(a.x - b.x), fabs(c.x - b.x)), fmax(fabs(c.x - e.x), fabs(a.x - e.x))),
-                         fmax(fabs(c.x - a.x), fabs(b.x - e.x)));
-  const double dy = fmax(fmax(fmax(fabs(a.y - b.y), fabs(c.y - b.y)), fmax(fabs(c.y - e.y), fabs(a.y - e.y))),
-                         fmax(fabs(c.y - a.y), fabs(b.y - e.y)));
-  const double sos = sqrt(0.5 * d.gam / m.s3);
-  const double lo_u = fmin(d.umax, fabs(m.s1) + sos), lo_v = fmin(d.vmax, fabs(m.s2) + sos);
-  const double hi_u = fmax(d.umax, fabs(m.s1) + sos), hi_v = fmax(d.vmax, fabs(m.s2) + sos);
-  // clFindDT is called with the host's unrounded Kn (ugks_block.py:1421)
-  const double sc = (erf(10 * (d.Kn_eff - 1e-3)) + 1) / 2.0;
-  const double u = sc * (hi_u - lo_u) + lo_u, v = sc * (hi_v - lo_v) + lo_v;
-  return (dx * u + dy * v) / blk.area[gidx(d, mi + G, mj + G)];
+  return cfl_frequency(blk.d, blk.xy, blk.area, m, mi, mj, blk.d.Kn_eff);
 }
 
 // one warp per cell, CW cells per CTA: no block-wide barrier, so the serial
@@ -1630,11 +1617,43 @@ int restart_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, u
 }
 
 template <typename T, int FM, int MINB, int NT>
-void set_face_attributes() {
-  cudaFuncSetAttribute(face_pass<T, FM, MINB, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(face_retry<T, FM, MINB, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  cudaFuncSetAttribute(face_pass<T, FM, MINB, NT>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                       cudaSharedmemCarveoutMaxShared);
+cudaError_t set_face_attributes() {
+  cudaError_t e = cudaFuncSetAttribute(face_pass<T, FM, MINB, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       200 * 1024);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(face_retry<T, FM, MINB, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(face_pass<T, FM, MINB, NT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             cudaSharedmemCarveoutMaxShared);
+  return e;
+}
+
+// Kernel attributes (the dynamic shared memory above 48 KB that the face and
+// cell passes of large velocity grids need) hold per device: they are set
+// once for each device a step runs on, with that device current.
+constexpr int kMaxDevices = 64;
+template <typename T>
+cudaError_t set_step_attributes() {
+  static std::mutex lock;
+  static bool done[kMaxDevices] = {false};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> guard(lock);
+  if (done[dev]) return cudaSuccess;
+  cudaError_t r[7] = {
+      set_face_attributes<T, 0, FaceBudget<T>::narrow, FT>(),
+      set_face_attributes<T, 1, FaceBudget<T>::narrow, FT>(),
+      set_face_attributes<T, 3, FaceBudget<T>::narrow, FT>(),
+      set_face_attributes<T, 0, FaceBudget<T>::wide, FaceBudget<T>::wide_threads>(),
+      set_face_attributes<T, 1, FaceBudget<T>::wide, FaceBudget<T>::wide_threads>(),
+      set_face_attributes<T, 3, FaceBudget<T>::wide, FaceBudget<T>::wide_threads>(),
+      cudaFuncSetAttribute(cell_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)};
+  for (cudaError_t x : r)
+    if (x != cudaSuccess) return x;
+  done[dev] = true;
+  return cudaSuccess;
 }
 
 // shared memory of a face CTA: (h, b) and slopes per velocity + axis tables
@@ -1676,17 +1695,8 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
   const size_t smem = face_smem<T>(z->max_nv, z->max_axes);
   const int cstride = 2 * z->max_axes + CELL_COEF;  // doubles of shared memory per cell warp
   const size_t csmem = (size_t)CW * cstride * sizeof(double) + (size_t)CW * cell_ring_bytes<T>();
-  static bool attr_set = false;  // one flag per instantiation
-  if (!attr_set) {
-    set_face_attributes<T, 0, FaceBudget<T>::narrow, FT>();
-    set_face_attributes<T, 1, FaceBudget<T>::narrow, FT>();
-    set_face_attributes<T, 3, FaceBudget<T>::narrow, FT>();
-    set_face_attributes<T, 0, FaceBudget<T>::wide, FaceBudget<T>::wide_threads>();
-    set_face_attributes<T, 1, FaceBudget<T>::wide, FaceBudget<T>::wide_threads>();
-    set_face_attributes<T, 3, FaceBudget<T>::wide, FaceBudget<T>::wide_threads>();
-    cudaFuncSetAttribute(cell_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set = true;
-  }
+  const cudaError_t attr = set_step_attributes<T>();
+  if (attr != cudaSuccess) return -(int)attr;
   if (smem > 200 * 1024 || csmem > 200 * 1024) return -(int)cudaErrorInvalidValue;
   const unsigned sg = (unsigned)((ns + 127) / 128);
   auto mark = [&](int k) {

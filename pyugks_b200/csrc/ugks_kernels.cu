@@ -555,25 +555,7 @@ __global__ void __launch_bounds__(VT) k_initFunctions(ugks_block_desc d, size_t 
     st2(Fin, fidx(d, gi, gj, v), shakhov_eq(d, prim, Q, quad_at(d, v), v));
 }
 
-// clFindDT (clKernel.c:224-308)
-__device__ __forceinline__ double cfl_frequency(const ugks_block_desc &d, const double *xy,
-                                                const double *area, P4 m, long mi, long mj,
-                                                double Kn) {
-  const long G = d.ghost, NY = d.Nj + 1;
-  V2 a = ld2(xy, (mi + 1 + G) * NY + mj + G), b = ld2(xy, (mi + 1 + G) * NY + mj + 1 + G);
-  V2 c = ld2(xy, (mi + G) * NY + mj + 1 + G), e = ld2(xy, (mi + G) * NY + mj + G);
-  double dx = fmax(fmax(fmax(fabs(a.x - b.x), fabs(c.x - b.x)), fmax(fabs(c.x - e.x), fabs(a.x - e.x))),
-                   fmax(fabs(c.x - a.x), fabs(b.x - e.x)));
-  double dy = fmax(fmax(fmax(fabs(a.y - b.y), fabs(c.y - b.y)), fmax(fabs(c.y - e.y), fabs(a.y - e.y))),
-                   fmax(fabs(c.y - a.y), fabs(b.y - e.y)));
-  double sos = sqrt(0.5 * d.gam / m.s3);
-  double lo_u = fmin(d.umax, fabs(m.s1) + sos), lo_v = fmin(d.vmax, fabs(m.s2) + sos);
-  double hi_u = fmax(d.umax, fabs(m.s1) + sos), hi_v = fmax(d.vmax, fabs(m.s2) + sos);
-  double sc = (erf(10 * (Kn - 1e-3)) + 1) / 2.0;
-  double u = sc * (hi_u - lo_u) + lo_u, v = sc * (hi_v - lo_v) + lo_v;
-  return (dx * u + dy * v) / area[gidx(d, mi + G, mj + G)];
-}
-
+// clFindDT (clKernel.c:224-308): cfl_frequency of ugks_device.cuh per cell
 __global__ void k_clFindDT(ugks_block_desc d, size_t g0, size_t g1, const double *xy,
                            const double *area, const double *macro, double *time_step, double Kn) {
   size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;

@@ -50,20 +50,8 @@ __global__ void cell_frequency(ugks_block_desc d, const double *xy, const double
   const size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   const size_t n = (size_t)d.ni * d.nj;
   if (t >= n) return;
-  const long mi = t / d.nj, mj = t % d.nj, G = d.ghost, NY = d.Nj + 1;
-  const V2 a = ld2(xy, (mi + 1 + G) * NY + mj + G), b = ld2(xy, (mi + 1 + G) * NY + mj + 1 + G);
-  const V2 c = ld2(xy, (mi + G) * NY + mj + 1 + G), e = ld2(xy, (mi + G) * NY + mj + G);
-  const double dx = fmax(fmax(fmax(fabs(a.x - b.x), fabs(c.x - b.x)), fmax(fabs(c.x - e.x), fabs(a.x - e.x))),
-                         fmax(fabs(c.x - a.x), fabs(b.x - e.x)));
-  const double dy = fmax(fmax(fmax(fabs(a.y - b.y), fabs(c.y - b.y)), fmax(fabs(c.y - e.y), fabs(a.y - e.y))),
-                         fmax(fabs(c.y - a.y), fabs(b.y - e.y)));
-  const P4 m = ld4(macro, t);
-  const double sos = sqrt(0.5 * d.gam / m.s3);
-  const double lo_u = fmin(d.umax, fabs(m.s1) + sos), lo_v = fmin(d.vmax, fabs(m.s2) + sos);
-  const double hi_u = fmax(d.umax, fabs(m.s1) + sos), hi_v = fmax(d.vmax, fabs(m.s2) + sos);
-  const double sc = (erf(10 * (Kn - 1e-3)) + 1) / 2.0;
-  const double u = sc * (hi_u - lo_u) + lo_u, v = sc * (hi_v - lo_v) + lo_v;
-  freq[t] = (dx * u + dy * v) / area[(size_t)(mi + G) * d.Nj + (mj + G)];
+  const long mi = t / d.nj, mj = t % d.nj;
+  freq[t] = cfl_frequency(d, xy, area, ld4(macro, t), mi, mj, Kn);
 }
 
 // maximum of freq[0..n) into out[0], one CTA

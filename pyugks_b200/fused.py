@@ -194,7 +194,7 @@ class FusedSolver:
         fill_walls(d, b, self._keep, self.device)
         for f, bc in enumerate(b["bc"]):
             x.bc_type[f] = bc["type"]
-            if bc["type"] == D.ADJACENT:
+            if bc["type"] in (D.ADJACENT, D.PERIODIC):  # both copy through edgeExchange
                 x.bc_block[f] = first + bc["other_block"]
                 x.bc_face[f] = bc["other_face"]
                 x.bc_ori[f] = bc.get("orientation", 1)

@@ -116,7 +116,7 @@ class SolvePool:
                 x = _lib.FusedBlock.from_buffer_copy(bytes(blk.struct))
                 x.solve = k
                 for f in range(4):
-                    if blk.bc[f]["type"] == D.ADJACENT:
+                    if blk.bc[f]["type"] in (D.ADJACENT, D.PERIODIC):
                         x.bc_block[f] = first + blk.bc[f]["other_block"]
                 structs.append(x)
             rec = _lib.SolveState.from_buffer_copy(s.record.cpu().numpy().tobytes())

@@ -1,8 +1,8 @@
 """Generate the golden fixtures of tests/golden/ from the reference itself.
 
 Runs pyUGKS's own OpenCL kernels, compiled for the CPU by oracle/ref_build.py
-from the reference sources (so it needs them, under $UGKS_REFERENCE or
-/root/reference), driven by the oracle's restatement of the reference step
+from the reference sources (so it needs them: $UGKS_REFERENCE, else a
+directory "reference" beside the repository root), driven by the oracle's restatement of the reference step
 sequence (oracle/host.py), and stores macroscopic fields (rho, U, V, T, qx,
 qy), dt and time at several step counts -- plus the full interior f for the
 small cases -- as compressed .npz files:
@@ -22,6 +22,16 @@ Cases:
                channel8 with a tabulated Langmuir isotherm (configs.langmuir_table)
   cavity8_minmod
                cavity8 with the minmod (NND) limiter, FLUX_METHOD 3, CFL 0.5
+  rotated8     two blocks joined NORTH to EAST, grids turned 90 degrees
+               (configs.rotated_pair)
+  flipped8     two blocks joined NORTH to NORTH with misaligned corners and
+               orientation 1 (configs.flipped_pair)
+  mirror8      one block whose S, W and E faces connect to themselves with
+               FLIP_NS, FLIP_EW and FLIP_D (configs.mirror_cavity)
+  periodic8    Couette flow, periodic in x through a PERIODIC (code 5) face
+               (configs.periodic_couette)
+  open8        channel with a CONSTANT inlet and an OUTFLOW outlet
+               (configs.open_channel)
   cavity32     the 32x32 cavity, 25x25 velocities on [-4,4]^2, vanLeer, Kn 0.075,
                CFL 0.8, lid 0.15 (fields at steps 1/10/100/1000)
   cavity32_perturbed
@@ -56,6 +66,11 @@ CASES = {
                                                   adsorb=configs.langmuir_table()), (1, 10, 30), True),
     "cavity8_minmod": (lambda: configs.cavity(n=8, m=8, vlim=4.0, flux_method="minmod", CFL=0.5),
                        (1, 10, 50), True),
+    "rotated8": (lambda: configs.rotated_pair(n=8, m=8), (1, 10, 30), True),
+    "flipped8": (lambda: configs.flipped_pair(n=8, m=8), (1, 10, 30), True),
+    "mirror8": (lambda: configs.mirror_cavity(n=8, m=8), (1, 10, 30), True),
+    "periodic8": (lambda: configs.periodic_couette(n=8, m=8), (1, 10, 30), True),
+    "open8": (lambda: configs.open_channel(n=8, m=8), (1, 10, 30), True),
 }
 
 

@@ -125,6 +125,12 @@ CASES = {
     "channel_cl": lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.01, reflect_type="CL", alpha_n=0.5,
                                           alpha_t=0.7),
     "channel_isotherm": lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0, adsorb=configs.langmuir_table()),
+    # block connections beyond opposite aligned faces, and the open faces
+    "rotated_north_east": lambda: configs.rotated_pair(n=8, m=8),
+    "flipped_north_north": lambda: configs.flipped_pair(n=8, m=8),
+    "self_connected_flips": lambda: configs.mirror_cavity(n=8, m=8),
+    "periodic_couette": lambda: configs.periodic_couette(n=8, m=8),
+    "constant_outflow": lambda: configs.open_channel(n=8, m=8),
 }
 
 

@@ -21,6 +21,11 @@ CASES = {
     "channel8": (lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0), (1, 10, 30)),
     "cavity32": (lambda: configs.cavity(n=32, m=24, vlim=4.0), (1, 10, 100, 1000)),
     "cavity8_minmod": (lambda: configs.cavity(n=8, m=8, vlim=4.0, flux_method="minmod", CFL=0.5), (1, 10, 50)),
+    "rotated8": (lambda: configs.rotated_pair(n=8, m=8), (1, 10, 30)),
+    "flipped8": (lambda: configs.flipped_pair(n=8, m=8), (1, 10, 30)),
+    "mirror8": (lambda: configs.mirror_cavity(n=8, m=8), (1, 10, 30)),
+    "periodic8": (lambda: configs.periodic_couette(n=8, m=8), (1, 10, 30)),
+    "open8": (lambda: configs.open_channel(n=8, m=8), (1, 10, 30)),
 }
 
 
@@ -29,6 +34,9 @@ CASES = {
 # again with f perturbed by 1e-14 relative, and its distance from the golden
 # run is the envelope that any non-bit-identical implementation must stay in.
 ENVELOPE = {"cavity32": ("cavity32_perturbed", 100)}
+# the GPU run lands at about 1x the perturbed reference's distance at step
+# 1000; 2x leaves room for a different rounding history, not for a defect
+ENVELOPE_FACTOR = 2.0
 
 
 def envelope(name, s, k, gold_fields):
@@ -51,7 +59,7 @@ def check(g, s, fields, fs, dt, time, name=None):
             assert max(errs.values()) < TOL, (s, k, errs)
         else:
             for key, e in errs.items():
-                assert e <= max(TOL, 10.0 * env[key]), (s, k, key, e, env[key])
+                assert e <= max(TOL, ENVELOPE_FACTOR * env[key]), (s, k, key, e, env[key])
     if fs is not None and ("s%d_b0_f" % s) in g:
         for k, f in enumerate(fs):
             assert rel_err(f, g["s%d_b%d_f" % (s, k)]) < TOL
@@ -71,7 +79,8 @@ def test_fused_fp64_matches_golden(cuda, name):
         check(g, s, gpu.fields(), gpu.interior_f(), st["dt"], st["time"], name)
 
 
-@pytest.mark.parametrize("name", ["cavity8", "multiblock8", "channel8", "cavity8_minmod"])
+@pytest.mark.parametrize("name", ["cavity8", "multiblock8", "channel8", "cavity8_minmod", "rotated8",
+                                  "flipped8", "mirror8", "periodic8", "open8"])
 def test_dropin_driver_matches_golden(cuda, name):
     make, steps = CASES[name]
     g = np.load(os.path.join(GOLDEN, name + ".npz"))

@@ -26,6 +26,11 @@ CASES = {
     "channel8_isotherm": (lambda: configs.channel(nblocks=2, n=8, m=8, k_des=0.0,
                                                   adsorb=configs.langmuir_table()), (1, 10, 30)),
     "cavity8_minmod": (lambda: configs.cavity(n=8, m=8, vlim=4.0, flux_method="minmod", CFL=0.5), (1, 10, 50)),
+    "rotated8": (lambda: configs.rotated_pair(n=8, m=8), (1, 10, 30)),
+    "flipped8": (lambda: configs.flipped_pair(n=8, m=8), (1, 10, 30)),
+    "mirror8": (lambda: configs.mirror_cavity(n=8, m=8), (1, 10, 30)),
+    "periodic8": (lambda: configs.periodic_couette(n=8, m=8), (1, 10, 30)),
+    "open8": (lambda: configs.open_channel(n=8, m=8), (1, 10, 30)),
 }
 # the Cercignani-Lampis kernel's Bessel I0: a power series in the port, a
 # rational approximation in the reference
