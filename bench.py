@@ -267,6 +267,14 @@ def run_ours(args, rank, world, dist):
         "gpu_launches": solver.launches_per_step() * args.steps,
         "clocks": clocks,
     }
+    if world == 1 and args.workload == "multiblock" and args.precision == "fp64" and not args.no_north_star:
+        # the north-star comparison: batched mixed precision and serving
+        # against the plain FP64 method, measured in the same run
+        for key, fn in (("batched_mixed", batched_record), ("serving", serving_record)):
+            try:
+                line[key] = fn()
+            except Exception as exc:  # the main line is printed regardless
+                line[key] = {"error": "%s: %s" % (type(exc).__name__, exc)}
     if world == 1 and not args.no_cpu_baseline:
         budget = float(os.environ.get("UGKS_CPU_BASELINE_SECONDS", "20"))
         val, kind, cores, done = cpu_reference(cases, steps=50, warmup=1, time_budget=budget)
@@ -325,28 +333,72 @@ def run_e2e(solver, args, stream, dev, units):
     return {"ms": t0.elapsed_time(t1), "h2d": h2d // args.steps, "d2h": d2h // args.steps}
 
 
-def fp64_one_at_a_time(reqs, steps=100, budget_s=15.0):
-    """The config-5 comparison arm: the plain FP64 method run one solve at a
-    time over the same request stream (a bounded sample: requests in arrival
-    order until about budget_s of stepping).  Returns (units/s, requests,
-    steps per request)."""
+def batched_record(steps=10, warmup=3):
+    """Config 3 (64 independent cavities, seed 1) in one block table, mixed and
+    FP64: device-timed throughput of each, and the mixed fields' error against
+    the FP64 fields after the same steps (relative L2 / Linf per solve; the
+    worst over the 64 solves)."""
     import torch
     from pyugks_b200.fused import FusedSolver
-    units, el, n = 0, 0.0, 0
-    for r in reqs:
-        solver = FusedSolver([r.case], precision="fp64")
-        solver.step(3)
+    from pyugks_b200.mixed_error import errors
+    cases, desc = workload("batched")
+    units = units_per_step(cases)
+    out = {"workload": desc, "units_per_step": units, "steps": steps, "warmup": warmup}
+    solvers = {}
+    for prec in ("mixed", "fp64"):
+        s = FusedSolver(cases, precision=prec)
+        s.step(warmup)
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        solver.step(steps)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        s.step(steps)
+        b.record()
         torch.cuda.synchronize()
-        el += time.perf_counter() - t0
-        units += units_per_step([r.case]) * steps
-        n += 1
-        del solver
-        if el > budget_s:
-            break
-    return units / el, n, steps
+        ms = a.elapsed_time(b)
+        out[prec] = {"value": units * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps,
+                     "gpu_launches": s.launches_per_step() * steps}
+        solvers[prec] = s
+    out["ratio_mixed_over_fp64"] = out["mixed"]["value"] / out["fp64"]["value"]
+    worst = {}
+    for k in range(len(cases)):
+        e = errors(solvers["mixed"].fields(k), solvers["fp64"].fields(k))
+        for name, v in e.items():
+            w = worst.setdefault(name, {"L2": 0.0, "Linf": 0.0})
+            w["L2"], w["Linf"] = max(w["L2"], v["L2"]), max(w["Linf"], v["Linf"])
+    out["mixed_vs_fp64_error"] = {"after_steps": warmup + steps, "worst_over_solves": worst}
+    return out
+
+
+def serving_record(arrival_seconds=2.0, max_steps=2000, tol=1e-6, steps_per_tick=50):
+    """A bounded config-5 stream: Poisson arrivals at 20/s (seed 2) over
+    arrival_seconds, 70% cavities / 30% adsorbing channels with config 5's
+    size and parameter distributions, each run until its density residual is
+    below tol or max_steps steps.  Served by continuous batching in mixed
+    precision, and by the plain FP64 fused step one solve at a time to the
+    same stop rule (first come, first served)."""
+    from pyugks_b200.serving import Server, request_stream, serve_one_at_a_time
+    reqs = request_stream(seed=2, rate=20.0, duration=arrival_seconds, max_steps=max_steps, tol=tol)
+    server = Server(budget_bytes=150e9, precision="mixed", steps_per_tick=steps_per_tick)
+    done = server.run(reqs)
+    lat = np.array([r.finished - r.arrival for r in done])
+    batched = {"value": server.units / server.wall, "unit": UNIT, "wall_s": server.wall,
+               "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+               "completed": len(done), "converged": sum(r.reason == "converged" for r in done),
+               "step_limit": sum(r.reason == "max_steps" for r in done),
+               "errors": sum(r.reason == "error" for r in done)}
+    arm = serve_one_at_a_time(request_stream(seed=2, rate=20.0, duration=arrival_seconds, max_steps=max_steps,
+                                             tol=tol), precision="fp64", steps_per_tick=steps_per_tick)
+    la = np.array(arm["latency"])
+    fp64 = {"value": arm["value"], "unit": UNIT, "makespan_s": arm["makespan_s"],
+            "p50_s": float(np.percentile(la, 50)), "p99_s": float(np.percentile(la, 99)),
+            "converged": sum(x == "converged" for x in arm["reasons"]),
+            "step_limit": sum(x == "max_steps" for x in arm["reasons"]),
+            "errors": sum(x == "error" for x in arm["reasons"])}
+    return {"stream": "%d requests: Poisson 20/s over %.1f s (seed 2), stop at density residual < %g or %d steps"
+                      % (len(reqs), arrival_seconds, tol, max_steps),
+            "arrivals": len(reqs), "admitted": len(done), "backlog": len(reqs) - len(done),
+            "mixed_batched": batched, "fp64_one_at_a_time": fp64,
+            "ratio_throughput": batched["value"] / fp64["value"] if fp64["value"] else None}
 
 
 def run_serving(args):
@@ -354,34 +406,17 @@ def run_serving(args):
     for --arrival-seconds, 70% cavities / 30% adsorbing channels with the
     config-5 size distributions, each solve run to density residual < 1e-6 or
     --max-steps, admission by HBM footprint against 150 GB."""
-    import torch
-    from pyugks_b200.serving import Server, request_stream
     if args.impl == "reference":
         print(json.dumps({"impl": "reference", "unavailable":
                           "the reference has no serving loop; its CPU step is timed by the default workload"}))
         return
-    reqs = request_stream(seed=2, rate=20.0, duration=args.arrival_seconds, max_steps=args.max_steps,
-                          tol=1e-6)
-    server = Server(budget_bytes=150e9, precision=args.precision, steps_per_tick=25)
-    done = server.run(reqs)
-    base_value, base_n, base_steps = fp64_one_at_a_time(reqs)
-    lat = np.array([r.finished - r.arrival for r in done])
+    rec = serving_record(args.arrival_seconds, args.max_steps)
     line = {
-        "metric": METRIC, "value": server.units / server.wall, "unit": UNIT, "n_gpus": 1,
+        "metric": METRIC, "value": rec["mixed_batched"]["value"], "unit": UNIT, "n_gpus": 1,
         "steps": None, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "f32+f64", "data": "synthetic",
-        "config": {"workload": "serving stream: %d requests over %.1f s (Poisson 20/s, seed 2), "
-                               "max %d steps or residual < 1e-6" % (len(reqs), args.arrival_seconds,
-                                                                     args.max_steps),
-                   "precision": args.precision},
-        "latency": {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-                    "completed": len(done), "converged": sum(r.reason == "converged" for r in done),
-                    "wall_s": server.wall},
-        "fp64_one_at_a_time": {"value": base_value, "unit": UNIT,
-                               "sample": "the first %d requests of the stream, %d steps each, one solve at "
-                                         "a time on the plain FP64 fused step (wall clock, set-up excluded)"
-                                         % (base_n, base_steps),
-                               "ratio": server.units / server.wall / base_value},
+        "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": "serving stream: " + rec["stream"], "precision": "mixed"},
+        "serving": rec,
     }
     print(json.dumps(line), flush=True)
 
@@ -395,10 +430,12 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--workload", default="multiblock",
                     choices=["multiblock", "cavity", "channel", "batched", "serving"])
-    ap.add_argument("--arrival-seconds", type=float, default=3.0,
+    ap.add_argument("--arrival-seconds", type=float, default=2.0,
                     help="serving: length of the Poisson arrival window (rate 20/s)")
-    ap.add_argument("--max-steps", type=int, default=400, help="serving: step limit per solve")
+    ap.add_argument("--max-steps", type=int, default=2000, help="serving: step limit per solve")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-north-star", action="store_true",
+                    help="skip the batched-mixed and serving sub-records of the default line")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3

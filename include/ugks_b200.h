@@ -249,10 +249,32 @@ int ugks_adsorbingWallCL_P2(const ugks_block_desc *d, size_t g0, size_t g1, cons
  * A solve is one pyUGKS simulation (UGKSim); it owns one or more blocks.
  * The caller keeps, in device memory, an array of ugks_fused_block (one per
  * block of every solve) and an array of ugks_solve_state (one per solve).
- * f and the two face-flux arrays of a block are stored as FP64 (double2) by
- * the *_fp64 entry points and as FP32 (float2) by the *_mixed ones; all
- * moments, the conserved update, the relaxation and dt stay FP64.
+ *
+ * *_fp64: f and the two face-flux arrays of a block are FP64 in the reference
+ * layout [Ni][Nj][Nv] x (h, b).
+ *
+ * *_mixed: they are FP32 *deviations* from a reference Maxwellian M of the
+ * solve (ugks_fused_block.ref): f = M + df and
+ * flux = dt len (u . n) M + dflux, in a velocity-pair layout
+ * [Ni][Nj][(Nv + 1) / 2] x (h_2p, h_2p+1, b_2p, b_2p+1); an odd Nv pads the
+ * last pair with a velocity whose entries stay 0.  The tensor velocity grid
+ * (u_num * v_num == Nv) is required.  Moments, the conserved update, the
+ * relaxation, dt and the residual stay FP64 in both.
  * --------------------------------------------------------------------- */
+
+/* Reference Maxwellian of a mixed-precision solve: a device array of doubles
+ * shared by the solve's blocks, written once by the caller:
+ *   [UGKS_REF_LAMBDA] lambda0 = 1/T0, [UGKS_REF_P0] rho0 lambda0 / pi,
+ *   [UGKS_REF_KB0] K / (2 lambda0),
+ *   [UGKS_REF_MOM + k] the 13 sums over v of mh (1, u, v, u^2, u v, v^2,
+ *     u^3, u^2 v, u v^2, v^3) and of kb0 mh (1, u, v), (u, v) = quad[v],
+ *   [UGKS_REF_TAB + v] mh[v] = weight[v] rho0 lambda0 / pi exp(-lambda0 |quad[v]|^2),
+ *   then Au[u_num], Av[v_num] with mh(iu, jv) = Au[iu] Av[jv] (to rounding). */
+#define UGKS_REF_LAMBDA 0
+#define UGKS_REF_P0 1
+#define UGKS_REF_KB0 2
+#define UGKS_REF_MOM 4
+#define UGKS_REF_TAB 32
 typedef struct ugks_fused_block {
   ugks_block_desc d;           /* sizes, constants, tables, wall values    */
   int32_t solve;               /* index of the owning ugks_solve_state     */
@@ -295,6 +317,9 @@ typedef struct ugks_fused_block {
                                   reciprocal and 1/|c - c'| for the u <= 0 stencil,
                                   then the same for u > 0; written by ugks_init_* and
                                   ugks_restart_* from centre and mid_side */
+  const double *ref;           /* *_mixed only: the solve's reference Maxwellian
+                                  (UGKS_REF_* layout above), the same array for
+                                  every block of the solve; unused by *_fp64 */
 } ugks_fused_block;
 
 typedef struct ugks_solve_state {
@@ -312,11 +337,18 @@ typedef struct ugks_solve_state {
   int32_t active;              /* 0: skipped by every fused kernel          */
   int32_t nblocks;             /* blocks of this solve                      */
   int32_t first_block;         /* index of its first block in the table     */
-  int32_t pad_;
+  int32_t stopped;             /* set by ugks_stop_check: 0 running, UGKS_STOP_* */
   double residual[4];          /* written by ugks_residual: mean over blocks
                                   of sqrt(ni nj sum (dprim)^2) / sum |prim|
                                   (ugks_block.py:1319-1327, ugks_sim.py:463-468) */
+  double stop_residual;        /* stop rule: density residual below this (0: none) */
+  int32_t stop_steps;          /* stop rule: this many completed steps (0: none)   */
+  int32_t pad2_;
 } ugks_solve_state;
+
+#define UGKS_STOP_CONVERGED 1
+#define UGKS_STOP_STEPS 2
+#define UGKS_STOP_ERROR 3
 
 #define UGKS_MAX_FACE_SEGMENTS 16
 
@@ -338,7 +370,18 @@ typedef struct ugks_fused_sizes {
   int32_t seg_method[UGKS_MAX_FACE_SEGMENTS];
   int32_t seg_max_nv[UGKS_MAX_FACE_SEGMENTS];
   int32_t seg_max_axes[UGKS_MAX_FACE_SEGMENTS];
+  /* launch shape per face-pass segment (0 by velocity count; 1..4 force one
+     of the compiled shapes, ugks_fused.cu FaceShape) and of the cell pass
+     (0 default; 2 or 3 CTAs of 8 warps per SM); ugks_fused_layout sets 0, a
+     caller (the autotuner) may change them before stepping.  The shape
+     changes the order of the per-face sums, not the arithmetic: results agree
+     to round-off across shapes and are reproducible for a fixed shape. */
+  int32_t seg_variant[UGKS_MAX_FACE_SEGMENTS];
+  int32_t cell_variant;
+  int32_t pad_;
 } ugks_fused_sizes;
+
+#define UGKS_FACE_VARIANTS 5
 
 /* Fills face_begin/cell_begin/ghost_begin of the host copy `blocks` and the
    sizes.  The blocks of one solve must be contiguous and in the order of
@@ -357,7 +400,8 @@ int ugks_init_mixed(const ugks_fused_block *blocks_dev, int nblocks, const ugks_
 
 /* Restart with saved distributions (UGKSBlock.initFunctions with a restart
    file that holds f, ugks_block.py:274-300, 347-349, then ugks_sim.py:85-92):
-   f, macro and Q are the caller's (loaded into the block arrays beforehand);
+   f, macro and Q are the caller's (loaded into the block arrays beforehand;
+   for *_mixed, f as its deviation from the reference Maxwellian);
    wall_prop from the wall values, the fused path's per-cell moments and next
    heat flux from f, ghosts filled, dt := CFL / max frequency of the loaded
    macro.  `time` and `steps` of each solve record are left as the caller set
@@ -389,6 +433,25 @@ int ugks_step_profiled(int mixed, const ugks_fused_block *blocks_dev, int nblock
    ugks_sim.py:463-468 does) into ugks_solve_state.residual. */
 int ugks_residual(const ugks_fused_block *blocks_dev, int nblocks, ugks_solve_state *solves_dev,
                   int nsolves, UGKS_STREAM);
+
+/* The stop rule of ugks_solve_state for every active solve, after
+   ugks_residual of the same step: a solve with a non-zero status, a density
+   residual below stop_residual or stop_steps completed steps gets stopped =
+   UGKS_STOP_ERROR / _CONVERGED / _STEPS and active = 0, so that later fused
+   launches skip it (the run loop's exits, ugks_sim.py:587-645, decided on the
+   device). */
+int ugks_stop_check(ugks_solve_state *solves_dev, int nsolves, UGKS_STREAM);
+
+/* nsteps times: ugks_step_fp64 (mixed = 0) or ugks_step_mixed (mixed = 1),
+   ugks_residual and ugks_stop_check -- a serving tick, with no host
+   synchronisation, suitable for capture in one CUDA graph. */
+int ugks_serve_steps(int mixed, const ugks_fused_block *blocks_dev, int nblocks, const ugks_fused_sizes *sizes,
+                     ugks_solve_state *solves_dev, int nsolves, int nsteps, UGKS_STREAM);
+
+/* Sets the kernel attributes the fused step needs (dynamic shared memory
+   above 48 KB) on the current device; the first ugks_step_* call on a device
+   does the same.  Call it before capturing steps in a CUDA graph. */
+int ugks_prepare(int mixed);
 
 /* ------------------------------------------------------------------------
  * 3. Time-step frequency without device allocation.  No counterpart in the

@@ -47,7 +47,7 @@ class FusedBlock(C.Structure):
         ("macro", vp), ("Q", vp), ("prim_old", vp),
         ("area", vp), ("centre", vp), ("mid_side", vp), ("normal", vp), ("side_length", vp),
         ("xy", vp), ("wall_prop", vp), ("wall_cover", vp), ("wall_fluxes", vp), ("wall_dist", vp),
-        ("cell_mom", vp), ("Q_next", vp), ("face_geo", vp),
+        ("cell_mom", vp), ("Q_next", vp), ("face_geo", vp), ("ref", vp),
     ]
 
 
@@ -57,9 +57,14 @@ class SolveState(C.Structure):
         ("dt", f64), ("time", f64), ("CFL", f64), ("delta_dt", f64), ("max_dt", f64),
         ("max_freq", C.c_uint64),
         ("retry", i32), ("status", i32), ("steps", i32), ("retries", i32), ("active", i32),
-        ("nblocks", i32), ("first_block", i32), ("pad_", i32),
-        ("residual", f64 * 4),
+        ("nblocks", i32), ("first_block", i32), ("stopped", i32),
+        ("residual", f64 * 4), ("stop_residual", f64), ("stop_steps", i32), ("pad2_", i32),
     ]
+
+
+# ugks_solve_state.stopped (UGKS_STOP_*)
+STOP_CONVERGED, STOP_STEPS, STOP_ERROR = 1, 2, 3
+STOP_REASONS = {STOP_CONVERGED: "converged", STOP_STEPS: "max_steps", STOP_ERROR: "error"}
 
 
 class FusedSizes(C.Structure):
@@ -67,7 +72,11 @@ class FusedSizes(C.Structure):
     _fields_ = [("n_faces", i32), ("n_cells", i32), ("n_ghost", i32), ("max_nv", i32),
                 ("face_begin", i32 * 4), ("face_count", i32 * 4), ("max_axes", i32),
                 ("n_segments", i32), ("seg_begin", i32 * 16), ("seg_count", i32 * 16),
-                ("seg_method", i32 * 16), ("seg_max_nv", i32 * 16), ("seg_max_axes", i32 * 16)]
+                ("seg_method", i32 * 16), ("seg_max_nv", i32 * 16), ("seg_max_axes", i32 * 16),
+                ("seg_variant", i32 * 16), ("cell_variant", i32), ("pad_", i32)]
+
+
+FACE_VARIANTS = 5   # UGKS_FACE_VARIANTS: 0 automatic, 1..4 forced shapes
 
 
 # argument kinds of the drop-in kernels in reference order (p pointer, i int,
@@ -87,6 +96,9 @@ KERNEL_SIGNATURES = {
     "xyExchange": "pipiiiiiiii", "xyExtrapolate": "pi", "cellGeom": "pppppp", "getInternal": "ppp",
 }
 _CT = {"p": vp, "i": C.c_int, "d": f64}
+
+# layout of the mixed path's reference Maxwellian (UGKS_REF_*, include/ugks_b200.h)
+REF_LAMBDA, REF_P0, REF_KB0, REF_MOM, REF_TAB = 0, 1, 2, 4, 32
 
 # ugks_getDT_noalloc limits and error codes (include/ugks_b200.h)
 NOALLOC_MAX_CELLS = 1 << 20
@@ -129,6 +141,12 @@ def lib():
     L.ugks_step_launches.argtypes = [C.POINTER(FusedSizes), C.c_int]
     L.ugks_residual.restype = C.c_int
     L.ugks_residual.argtypes = [vp, C.c_int, vp, C.c_int, vp]
+    L.ugks_stop_check.restype = C.c_int
+    L.ugks_stop_check.argtypes = [vp, C.c_int, vp]
+    L.ugks_serve_steps.restype = C.c_int
+    L.ugks_serve_steps.argtypes = [C.c_int, vp, C.c_int, C.POINTER(FusedSizes), vp, C.c_int, C.c_int, vp]
+    L.ugks_prepare.restype = C.c_int
+    L.ugks_prepare.argtypes = [C.c_int]
     L.ugks_getDT_noalloc.restype = C.c_int
     L.ugks_getDT_noalloc.argtypes = [C.POINTER(BlockDesc), vp, vp, vp, f64, vp, vp]
     L.ugks_version.restype = C.c_char_p

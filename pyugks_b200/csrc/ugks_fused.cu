@@ -44,13 +44,13 @@ constexpr int FT = 128;  // threads per face / cell / ghost CTA
 #define FACE_MIN_BLOCKS 6
 #endif
 #ifndef FACE_MIN_BLOCKS_F32
-#define FACE_MIN_BLOCKS_F32 7
+#define FACE_MIN_BLOCKS_F32 5
 #endif
 #ifndef FACE_MIN_BLOCKS_WIDE
 #define FACE_MIN_BLOCKS_WIDE 2
 #endif
 #ifndef FACE_MIN_BLOCKS_WIDE_F32
-#define FACE_MIN_BLOCKS_WIDE_F32 3
+#define FACE_MIN_BLOCKS_WIDE_F32 2
 #endif
 #ifndef FACE_WIDE_THREADS
 #define FACE_WIDE_THREADS 384
@@ -60,23 +60,44 @@ constexpr int FT = 128;  // threads per face / cell / ghost CTA
 #endif
 // per storage type: the narrow and wide register budgets and the largest
 // velocity grid of the narrow one (that many face CTAs fit in shared memory:
-// FP64 6 x (32 B x 1100 + 3 KB), FP32 7 x (24 B x 1200 + 3 KB) <= 228 KB)
+// FP64 6 x (32 B x 1100 + 3 KB), mixed 5 x (24 B x 1800 + 3 KB) <= 228 KB;
+// the mixed kernels' packed-pair arithmetic needs 96 registers to run
+// without spilling in its velocity loops)
 template <typename T> struct FaceBudget;
 template <> struct FaceBudget<double> {
   static constexpr int narrow = FACE_MIN_BLOCKS, wide = FACE_MIN_BLOCKS_WIDE, narrow_max_nv = 1100,
                        wide_threads = FACE_WIDE_THREADS;
 };
 template <> struct FaceBudget<float> {
-  static constexpr int narrow = FACE_MIN_BLOCKS_F32, wide = FACE_MIN_BLOCKS_WIDE_F32, narrow_max_nv = 1200,
+  static constexpr int narrow = FACE_MIN_BLOCKS_F32, wide = FACE_MIN_BLOCKS_WIDE_F32, narrow_max_nv = 1800,
                        wide_threads = FACE_WIDE_THREADS_F32;
 };
+// Launch shapes a face-pass segment can run with (ugks_fused_sizes.seg_variant;
+// the tuner in pyugks_b200/tuner.py picks them by timing): variant 0 chooses
+// by velocity count (narrow up to FaceBudget::narrow_max_nv, wide above),
+// 1..4 force (threads per face CTA, CTAs per SM of the register budget):
+//   FP64  1 = 128 x 6 (narrow), 2 = 128 x 5, 3 = 256 x 3, 4 = 384 x 2 (wide)
+//   mixed 1 = 128 x 5 (narrow), 2 = 128 x 4, 3 = 256 x 3, 4 = 256 x 2 (wide)
+template <typename T, int V> struct FaceShape;
+template <> struct FaceShape<double, 1> { static constexpr int nt = 128, minb = 6; };
+template <> struct FaceShape<double, 2> { static constexpr int nt = 128, minb = 5; };
+template <> struct FaceShape<double, 3> { static constexpr int nt = 256, minb = 3; };
+template <> struct FaceShape<double, 4> { static constexpr int nt = 384, minb = 2; };
+template <> struct FaceShape<float, 1> { static constexpr int nt = 128, minb = 5; };
+template <> struct FaceShape<float, 2> { static constexpr int nt = 128, minb = 4; };
+template <> struct FaceShape<float, 3> { static constexpr int nt = 256, minb = 3; };
+template <> struct FaceShape<float, 4> { static constexpr int nt = 256, minb = 2; };
+static_assert(FaceShape<double, 1>::minb == FACE_MIN_BLOCKS && FaceShape<double, 4>::nt == FACE_WIDE_THREADS &&
+                  FaceShape<float, 1>::minb == FACE_MIN_BLOCKS_F32 && FaceShape<float, 4>::minb == FACE_MIN_BLOCKS_WIDE_F32,
+              "variants 1 and 4 are the narrow and wide default shapes");
+
 // CTAs of 8 cell warps per SM: FP64 at 128 registers (at 80 the update loop
 // spills and the pass is 12% slower), FP32 storage at 80 (6% faster than 128)
 #ifndef CELL_MIN_BLOCKS
 #define CELL_MIN_BLOCKS 2
 #endif
 #ifndef CELL_MIN_BLOCKS_F32
-#define CELL_MIN_BLOCKS_F32 3
+#define CELL_MIN_BLOCKS_F32 2
 #endif
 // ...and the depth of the per-warp ring of asynchronous copies that stream
 // the f and flux rows of the cell update into shared memory
@@ -444,400 +465,29 @@ __device__ __forceinline__ void block_sum_to0(double (&x)[N], double *scratch) {
   }
 }
 
-// one face work item (all threads of the CTA take part)
-template <typename T, int FM, int NT>
-__device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B, int nb,
-                                          ugks_solve_state *__restrict__ solves, const int w,
-                                          int retry_pass) {
-  extern __shared__ double dyn[];
-  __shared__ FaceShared<NT> sh;
-  using St = Store<T>;
-
-  const int bi = find_block<0>(B, nb, w);
-  const ugks_fused_block &blk = B[bi];
+// The wall procedure of one wall face (all threads of the CTA take part):
+// accommodatingWallDist (clUGKS.c:774-906) or adsorbingWall_P1 (clAdsorb.c:253-482)
+// followed by the re-emission stage (adsorbingWallD_P2 / S_P2 / CL_P2,
+// clAdsorb.c:488-975), then wallFlux (clUGKS.c:910-1011) and
+// wallMassEnergyFluxes (1019-1147).  fw holds the reconstructed face
+// distribution (h, b) per velocity in FP64 and is rewritten in place; rin is
+// shared scratch of Nv (h, b) pairs (double2, or float2 in the mixed path) for
+// the reflected incoming distribution; store_flux(v, h, b) writes the
+// face-flux row of velocity v.
+template <int NT, typename RIN, typename StoreFlux>
+__device__ __forceinline__ void wall_face(const ugks_fused_block &blk, ugks_solve_state &sol, FaceShared<NT> &sh,
+                                          double *fw, RIN *rin, const int wall, const int dir, const long gi,
+                                          const long gj, const long mi, const long mj, const V2 n, const double len,
+                                          const double dt, StoreFlux store_flux) {
+  using R = double;
   const ugks_block_desc &d = blk.d;
-  ugks_solve_state &sol = solves[blk.solve];
-  if (!sol.active) return;
-  if (retry_pass && !sol.retry) return;
-  if (d.flux_method != FM) return;
-  const double dt = sol.dt;
-
-  // work item -> (i, j, direction): S and W faces of one corner (i, j) are
-  // adjacent work items so that both directions read f while it is in L2
-  int lf = w - blk.face_begin;
-  const int dir = lf & 1;
-  lf >>= 1;
-  const int mi = lf / (d.nj + 1), mj = lf % (d.nj + 1);
-  if (dir == SOUTH ? (mi >= d.ni) : (mj >= d.nj)) return;
-
-  const int Nv = d.Nv, G = d.ghost;
-  const long gi = mi + G, gj = mj + G;
-  int wall = -1;
-  if (dir == SOUTH) {
-    if (mj == 0 && is_wall(blk.bc_type[GSOUTH])) wall = GSOUTH;
-    else if (mj == d.nj && is_wall(blk.bc_type[GNORTH])) wall = GNORTH;
-  } else {
-    if (mi == 0 && is_wall(blk.bc_type[GWEST])) wall = GWEST;
-    else if (mi == d.ni && is_wall(blk.bc_type[GEAST])) wall = GEAST;
-  }
-
-  // per velocity: (h, b) at the face and their slopes, kept for the later
-  // sweeps, in the storage precision; the FP32 path also keeps the face-frame
-  // velocity of every node
-  constexpr bool F32 = std::is_same<T, float>::value;
-  using R = T;
-  using R2 = typename St::vec;
-  R2 *fhb = reinterpret_cast<R2 *>(dyn), *sgb = fhb + Nv;
-  float2 *uvf = reinterpret_cast<float2 *>(sgb + Nv);
-  const V2 n = ld2(blk.normal, faceidx(d, gi, gj, dir));
-  const V2 mid = ld2(blk.mid_side, faceidx(d, gi, gj, dir));
-  // velocity tables and the face-frame velocity (interfaceVelocity,
-  // clFunctions.c:191-209), with the table pointers held in registers
+  const int Nv = d.Nv;
   const double2 *__restrict__ qd = reinterpret_cast<const double2 *>(d.quad);
   const double *__restrict__ wt = d.weight;
   auto fvel = [&](int vv) {
     const double2 e = qd[vv];
     return v2(e.x * n.x + e.y * n.y, e.x * (-n.y) + e.y * n.x);
   };
-  // stencil geometry for both upwind directions (iFace, clUGKS.c:148-176):
-  // index 1 for u > 0 (upwind cell before the face), 0 otherwise
-  // (FP64: precomputed by face_geometry; FP32: computed here, which measured
-  // faster than waiting for the loads)
-  double g6[6];
-  if constexpr (std::is_same<T, float>::value) {
-    stencil_geometry(blk, gi, gj, dir, mid, g6);
-  } else {
-    const double *fg = blk.face_geo + 6 * faceidx(d, gi, gj, dir);
-#pragma unroll
-    for (int k = 0; k < 6; ++k) g6[k] = fg[k];
-  }
-  const double dist0 = g6[0], idist0 = g6[1], il0 = g6[2], dist1 = g6[3], idist1 = g6[4], il1 = g6[5];
-  const int step = dir == SOUTH ? Nv : d.Nj * Nv;
-  const size_t base = fidx(d, gi, gj, 0);
-  constexpr int MID = FM == 1 ? 2 : 1;
-  using Vec = typename St::vec;
-  const Vec *fcell = reinterpret_cast<const Vec *>(blk.f) + base;  // cell (gi, gj), velocity 0
-  const Vec *up1 = fcell - (MID + 1) * step, *up0 = fcell + MID * step;
-
-  // ---- sweep 1: reconstruction (+ interior faces: the face moments W of
-  // getFaceCons; the 1/2 of the energy moment is applied after the sum)
-  double m[4] = {0.0, 0.0, 0.0, 0.0};
-  if constexpr (F32) {
-    const float fl0 = (float)il0, fl1 = (float)il1, fd0 = (float)dist0, fd1 = (float)dist1;
-    const float fi0 = (float)idist0, fi1 = (float)idist1;
-    // the stencil of the next velocity is loaded before the current one is
-    // reconstructed (one iteration of software prefetch)
-    constexpr int L = FM == 1 ? 5 : 3;
-    float2 nx[L];
-    V2 nuv = v2(0.0, 0.0);
-    if (threadIdx.x < Nv) {
-      nuv = fvel(threadIdx.x);
-      const bool upn = nuv.x > 0.0;
-      load_stencil<L>((upn ? up1 : up0) + threadIdx.x, upn ? step : -step, nx);
-    }
-#pragma unroll 1
-    for (int v = threadIdx.x; v < Nv; v += NT) {
-      float2 cur[L];
-#pragma unroll
-      for (int k = 0; k < L; ++k) cur[k] = nx[k];
-      const V2 uv = nuv;
-      if (v + NT < Nv) {
-        nuv = fvel(v + NT);
-        const bool upn = nuv.x > 0.0;
-        load_stencil<L>((upn ? up1 : up0) + v + NT, upn ? step : -step, nx);
-      }
-      const bool up = uv.x > 0.0;
-      float ffh, ffb, sx, sy;
-      reconstruct_f<FM>(cur, up ? fl1 : fl0, up ? fd1 : fd0, up ? fi1 : fi0, ffh, ffb, sx, sy);
-      fhb[v] = make_float2(ffh, ffb);
-      sgb[v] = make_float2(sx, sy);
-      uvf[v] = make_float2((float)uv.x, (float)uv.y);
-      if (wall < 0) {
-        const double uu = fma(uv.x, uv.x, uv.y * uv.y), dh = ffh;
-        m[0] += dh;
-        m[1] = fma(uv.x, dh, m[1]);
-        m[2] = fma(uv.y, dh, m[2]);
-        m[3] += fma(uu, dh, (double)ffb);
-      }
-    }
-  } else {
-#pragma unroll 1
-    for (int v = threadIdx.x; v < Nv; v += NT) {
-      const V2 uv = fvel(v);
-      const bool up = uv.x > 0.0;
-      double ffh, ffb, sx, sy;
-      reconstruct<T, FM>((up ? up1 : up0) + v, up ? step : -step, up ? il1 : il0, up ? dist1 : dist0,
-                         up ? idist1 : idist0, ffh, ffb, sx, sy);
-      fhb[v] = make_double2(ffh, ffb);
-      sgb[v] = make_double2(sx, sy);
-      if (wall < 0) {
-        const double uu = fma(uv.x, uv.x, uv.y * uv.y);
-        m[0] += ffh;
-        m[1] = fma(uv.x, ffh, m[1]);
-        m[2] = fma(uv.y, ffh, m[2]);
-        m[3] += fma(uu, ffh, ffb);
-      }
-    }
-  }
-  // the two cells beside an interior face (the inputs of getAL / getAR and
-  // the getPLR slopes, clUGKS.c:424-436), loaded by the last warp, which has
-  // the fewest velocities in sweep 1
-  if (wall < 0 && threadIdx.x >= NT - 32 && threadIdx.x < NT - 30) {
-    const int side = threadIdx.x - (NT - 32);  // 0: left (u > 0 upwind), 1: right
-    const size_t k = side == 0 ? gidx(d, gi - dir, gj - (1 - dir)) : gidx(d, gi, gj);
-    const P4 mc = ld4(blk.cell_mom, k);
-    const V2 uc = to_local(v2(mc.s1, mc.s2), n);
-    const V2 cc = ld2(blk.centre, k);
-    double *o = sh.nbr[side];
-    o[0] = mc.s0;
-    o[1] = uc.x;
-    o[2] = uc.y;
-    o[3] = mc.s3;
-    o[4] = nr_rcp(sqrt((mid.x - cc.x) * (mid.x - cc.x) + (mid.y - cc.y) * (mid.y - cc.y)));
-  }
-  const double len = blk.side_length[faceidx(d, gi, gj, dir)];
-
-  if (wall < 0) {
-    // ---------------- interior face ----------------
-    block_sum<4>(m, sh.scratch);
-    const P4 W = p4(m[0], m[1], m[2], 0.5 * m[3]);
-    Rcp rc;
-    const P4 prim = to_primary_rcp(d, W, rc);  // getPLR (clUGKS.c:421-422), every thread
-    const int un = d.u_num, vn = d.v_num;
-    const bool sep = un > 0 && un * vn == Nv && un + vn <= 512;
-    R *Eu = reinterpret_cast<R *>(F32 ? (void *)(uvf + Nv) : (void *)(sgb + Nv)), *Ev = Eu + (sep ? un : 0);
-    const V2 Ug = to_global(v2(prim.s1, prim.s2), n);  // face mean velocity, global frame
-    // Maxwellian prefactor rho lambda / pi (fM, clFunctions.c:49-58), times the
-    // face length: every per-velocity flux below carries the length
-    const double chl = (prim.s0 * (prim.s3 / d.PI)) * len;
-    double q[2] = {0.0, 0.0};
-    if (threadIdx.x < 32) {
-      // getPLR slopes (clUGKS.c:424-436) and initMacroFlux (446-518), split
-      // over lanes 0 / 1 of warp 0 (one per side, the same instructions)
-      // while lane 0 of warp 1 computes the time weights
-      const double kb = (0.5 * d.K) * rc.lam;
-      double Mv[MTUM], Mxi[3];
-      P4 a;
-      if (threadIdx.x < 2) {
-        const int side = threadIdx.x;
-        const double sg = side == 0 ? 1.0 : -1.0;
-        double Mh[MNUM];
-        half_moments_rcp(d.PI, d.K, prim, rc, sg, Mh, Mv, Mxi);
-        const double *o = sh.nbr[side];
-        // left: (W - W_L) / |mid - c_L|; right: (W_R - W) / |mid - c_R|
-        const double id = sg * o[4];
-        a = micro_slope_rcp(d.K, prim, rc,
-                            p4((W.s0 - o[0]) * id, (W.s1 - o[1]) * id, (W.s2 - o[2]) * id, (W.s3 - o[3]) * id));
-        const P4 t1 = moment_au(a, Mh, Mv, Mxi, 1, 0), t2 = moment_au(a, Mh, Mv, Mxi, 2, 0);
-        double *x = sh.lr[side];
-#pragma unroll
-        for (int k = 0; k < MNUM; ++k) x[k] = Mh[k];
-        x[7] = a.s0; x[8] = a.s1; x[9] = a.s2; x[10] = a.s3;
-        x[11] = t1.s0; x[12] = t1.s1; x[13] = t1.s2; x[14] = t1.s3;
-        x[15] = t2.s0; x[16] = t2.s1; x[17] = t2.s2; x[18] = t2.s3;
-      }
-      pair_wait();
-      double Mt[5];
-#pragma unroll
-      for (int k = 0; k < 5; ++k) Mt[k] = sh.mt[k];
-      double *c = sh.bcast;
-      if (threadIdx.x < 2) {
-        // distFlux coefficients of the upwind slope (derivation at sweep 3)
-        const double xk = Mxi[2] - kb * kb;
-        double *ck = c + 5 * threadIdx.x;
-        ck[0] = Mt[1] * fma(0.5 * a.s3, kb, a.s0);
-        ck[1] = Mt[1] * a.s1;
-        ck[2] = Mt[1] * a.s2;
-        ck[3] = Mt[1] * (0.5 * a.s3);
-        ck[4] = Mt[1] * (0.5 * a.s3 * xk);
-      }
-      if (threadIdx.x == 0) {
-        const double *xl = sh.lr[0], *xr = sh.lr[1];
-        double Mu[MNUM];
-#pragma unroll
-        for (int k = 0; k < MNUM; ++k) Mu[k] = xl[k] + xr[k];
-        const P4 aT = micro_slope_rcp(d.K, prim, rc,
-                                      scale(-prim.s0, add(p4(xl[11], xl[12], xl[13], xl[14]),
-                                                          p4(xr[11], xr[12], xr[13], xr[14]))));
-        const P4 g0 = scale(prim.s0,
-                            add(add(scale(Mt[0], moment_uv(Mu, Mv, Mxi, 1, 0, 0)),
-                                    scale(Mt[1], add(p4(xl[15], xl[16], xl[17], xl[18]),
-                                                     p4(xr[15], xr[16], xr[17], xr[18])))),
-                                scale(Mt[2], moment_au(aT, Mu, Mv, Mxi, 1, 0))));
-        const double xk = Mxi[2] - kb * kb;
-        c[10] = Mt[2] * fma(0.5 * aT.s3, kb, aT.s0) + Mt[0];
-        c[11] = Mt[2] * aT.s1;
-        c[12] = Mt[2] * aT.s2;
-        c[13] = Mt[2] * (0.5 * aT.s3);
-        c[14] = Mt[2] * (0.5 * aT.s3 * xk);
-        c[15] = Mt[0];
-        c[16] = Mt[3] * len;
-        c[17] = Mt[4] * len;
-        c[18] = len * g0.s0; c[19] = len * g0.s1; c[20] = len * g0.s2; c[21] = len * g0.s3;
-      }
-    } else {
-      if (threadIdx.x < 64) {
-        if (threadIdx.x == 32) {
-          double Mt[5];
-          time_weights_rcp(inv_relax_time_rcp(d, prim, rc), dt, Mt);
-#pragma unroll
-          for (int k = 0; k < 5; ++k) sh.mt[k] = Mt[k];
-        }
-        pair_arrive();
-      }
-      // meanwhile: face heat flux (calcFaceQ, clUGKS.c:522-585) and the
-      // axis factors of the face Maxwellian; warp 1, which computed the time
-      // weights, takes the last offsets
-      const int t = (threadIdx.x + NT - 96) % (NT - 32), nt = NT - 32;
-      const double Kinv = 1.0 / d.K;
-      if constexpr (F32) {
-        const float Ux = (float)prim.s1, Uy = (float)prim.s2, Ki = (float)Kinv;
-#pragma unroll 1
-        for (int v = t; v < Nv; v += nt) {
-          const float2 uv = uvf[v], fv = fhb[v];
-          const float cx = uv.x - Ux, cy = uv.y - Uy, c2 = fmaf(cx, cx, cy * cy);
-          const float tq = fmaf(c2, fv.x, fv.y * Ki);
-          q[0] += (double)(0.5f * (cx * tq));
-          q[1] += (double)(0.5f * (cy * tq));
-        }
-      } else {
-        for (int v = t; v < Nv; v += nt) {
-          const V2 uv = fvel(v);
-          const double cx = uv.x - prim.s1, cy = uv.y - prim.s2, c2 = cx * cx + cy * cy;
-          const double2 fv = fhb[v];
-          const double tq = c2 * fv.x + fv.y * Kinv;
-          q[0] += 0.5 * (cx * tq);
-          q[1] += 0.5 * (cy * tq);
-        }
-      }
-      if (sep) {
-        axis_exp(Eu, d.quad, un, vn, 0, Ug.x, prim.s3, t, nt, chl);
-        axis_exp(Ev, d.quad, vn, 1, 1, Ug.y, prim.s3, t, nt);
-      }
-    }
-    block_sum<2>(q, sh.scratch);
-    // ---- sweep 3: macroFlux (587-681) and distFlux (683-772).
-    // With h0 = weight * fM (times the face length), kb = K / (2 lambda),
-    // S = Mt0 s (c . Q) (the Shakhov factor of fS, clFunctions.c:64-77, times
-    // Mt0), P4 = 2 lambda c^2 - 4, the upwind slope a (aL for u > 0, else aR),
-    //   Ph = a0 + a1 u + a2 v + a3 (|u|^2 + kb) / 2, and Th likewise with aT,
-    //   Rh = Mt3 fh - Mt4 u sh,   Rb = Mt3 fb - Mt4 u sb,
-    //   Zh = u (S P4 h0 + Rh),    Zb = u (S (P4 + 2) kb h0 + Rb),
-    //   B  = Mt0 + Mt1 u Ph + Mt2 Th,
-    // distFlux's two components are
-    //   hx = Zh + u h0 B,
-    //   hy = Zb + u h0 (kb B + Mt1 u a3 X / 2 + Mt2 aT3 X / 2),  X = Mxi2 - kb^2,
-    // and macroFlux's discrete part sums (Zh, u Zh, v Zh, (|u|^2 Zh + Zb) / 2).
-    const double *c = sh.bcast;
-    const V2 Q = v2(q[0], q[1]);
-    const double lam = prim.s3, Ux = prim.s1, Uy = prim.s2, lam2 = 2.0 * lam;
-    const double kb = (0.5 * d.K) * rc.lam;
-    const double s0 = 0.8 * (1 - d.Pr) * (lam * lam) * rc.rho;
-    const double Mt0 = c[15], Mt3 = c[16], Mt4 = c[17];
-    const double sx = (Mt0 * s0) * Q.x, sy = (Mt0 * s0) * Q.y;
-    const double T0 = c[10], T1 = c[11], T2 = c[12], T3 = c[13], CT = c[14];
-    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-    void *flux = dir == SOUTH ? blk.flux_S : blk.flux_W;
-    const int qs = sep ? NT / vn : 0, rs = sep ? NT % vn : 0;
-    int iu = sep ? threadIdx.x / vn : 0, jv = sep ? threadIdx.x % vn : 0;
-    if constexpr (F32) {
-      // the same per-velocity flux in FP32; the macro flux sums stay FP64
-      const float fUx = (float)Ux, fUy = (float)Uy, flam = (float)lam, flam2 = (float)lam2, fkb = (float)kb;
-      const float fsx = (float)sx, fsy = (float)sy, fchl = (float)chl;
-      const float fT0 = (float)T0, fT1 = (float)T1, fT2 = (float)T2, fT3 = (float)T3, fCT = (float)CT;
-      const float fMt3 = (float)Mt3, fMt4 = (float)Mt4;
-      float AL[5], AR[5];
-#pragma unroll
-      for (int k = 0; k < 5; ++k) {
-        AL[k] = (float)c[k];
-        AR[k] = (float)c[5 + k];
-      }
-      float2 *fl = reinterpret_cast<float2 *>(flux) + base;
-#pragma unroll 1
-      for (int v = threadIdx.x; v < Nv; v += NT) {
-        const float2 uv = uvf[v];
-        const float u = uv.x, vt = uv.y, uu = fmaf(u, u, vt * vt);
-        const float cx = u - fUx, cy = vt - fUy, c2 = fmaf(cx, cx, cy * cy);
-        float E;
-        if (sep) {
-          E = Eu[iu] * Ev[jv];
-          jv += rs;
-          iu += qs;
-          if (jv >= vn) { jv -= vn; ++iu; }
-        } else {
-          E = fchl * expf(-flam * c2);
-        }
-        const float h0 = (float)wt[v] * E;
-        const float Sp = fmaf(cx, fsx, cy * fsy);
-        const float S4 = Sp * fmaf(flam2, c2, -4.0f), S2 = fmaf(2.0f, Sp, S4);
-        const bool pos = u > 0.0f;
-        const float A0 = pos ? AL[0] : AR[0], A1 = pos ? AL[1] : AR[1], A2 = pos ? AL[2] : AR[2];
-        const float A3 = pos ? AL[3] : AR[3], A4 = pos ? AL[4] : AR[4];
-        const float MP = fmaf(A3, uu, fmaf(A2, vt, fmaf(A1, u, A0)));
-        const float Bk = fmaf(u, MP, fmaf(fT3, uu, fmaf(fT2, vt, fmaf(fT1, u, fT0))));
-        const float2 fd = fhb[v], fs = sgb[v];
-        const float mu = fMt4 * u;
-        const float Rh = fmaf(-mu, fs.x, fMt3 * fd.x), Rb = fmaf(-mu, fs.y, fMt3 * fd.y);
-        const float Zh = u * fmaf(S4, h0, Rh), Zb = u * fmaf(S2, h0 * fkb, Rb);
-        const float uh = u * h0;
-        const float hx = fmaf(uh, Bk, Zh);
-        const float hy = fmaf(uh, fmaf(fkb, Bk, fmaf(A4, u, fCT)), Zb);
-        const double zh = Zh;
-        acc[0] += zh;
-        acc[1] = fma((double)u, zh, acc[1]);
-        acc[2] = fma((double)vt, zh, acc[2]);
-        acc[3] = fma((double)uu, zh, acc[3]);
-        acc[4] += (double)Zb;
-        fl[v] = make_float2(hx, hy);
-      }
-    } else {
-      for (int v = threadIdx.x; v < Nv; v += NT) {
-        const V2 uv = fvel(v);
-        const double u = uv.x, vt = uv.y, uu = fma(u, u, vt * vt);
-        const double cx = u - Ux, cy = vt - Uy, c2 = fma(cx, cx, cy * cy);
-        double E;
-        if (sep) {
-          E = Eu[iu] * Ev[jv];
-          jv += rs;
-          iu += qs;
-          if (jv >= vn) { jv -= vn; ++iu; }
-        } else {
-          E = chl * exp(-lam * c2);
-        }
-        const double h0 = wt[v] * E;
-        const double Sp = fma(cx, sx, cy * sy);
-        const double S4 = Sp * fma(lam2, c2, -4.0), S2 = fma(2.0, Sp, S4);
-        const double *A = c + (u > 0.0 ? 0 : 5);
-        const double MP = fma(A[3], uu, fma(A[2], vt, fma(A[1], u, A[0])));
-        const double Bk = fma(u, MP, fma(T3, uu, fma(T2, vt, fma(T1, u, T0))));
-        const double2 fd = fhb[v], fs = sgb[v];
-        const double mu = Mt4 * u;
-        const double Rh = fma(-mu, fs.x, Mt3 * fd.x), Rb = fma(-mu, fs.y, Mt3 * fd.y);
-        const double Zh = u * fma(S4, h0, Rh), Zb = u * fma(S2, h0 * kb, Rb);
-        const double uh = u * h0;
-        const double hx = fma(uh, Bk, Zh);
-        const double hy = fma(uh, fma(kb, Bk, fma(A[4], u, CT)), Zb);
-        acc[0] += Zh;
-        acc[1] = fma(u, Zh, acc[1]);
-        acc[2] = fma(vt, Zh, acc[2]);
-        acc[3] = fma(uu, Zh, acc[3]);
-        acc[4] += Zb;
-        St::store(flux, base + v, v2(hx, hy));
-      }
-    }
-    block_sum_to0<5>(acc, sh.scratch);
-    if (threadIdx.x == 0) {
-      P4 out = p4(acc[0] + c[18], acc[1] + c[19], acc[2] + c[20], 0.5 * (acc[3] + acc[4]) + c[21]);
-      const V2 g = to_global(v2(out.s1, out.s2), n);
-      out.s1 = g.x;
-      out.s2 = g.y;
-      st4(dir == SOUTH ? blk.flux_macro_S : blk.flux_macro_W, gidx(d, gi, gj), out);
-    }
-    return;
-  }
-
-  // ---------------- wall face ----------------
-  R *fw = reinterpret_cast<R *>(fhb);  // (h, b) per velocity, storage precision
   const int rot = (wall == GNORTH || wall == GEAST) ? -1 : 1;
   const long ci = dir == SOUTH ? mi : mj;
   P4 wl = ld4(blk.wall_prop, ci * 4 + wall);
@@ -945,8 +595,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
       // (ugks_block.py:949-950, 1084): its flux row keeps what iFace wrote
       // there, the face values of (h, b), and its face macro flux is not
       // written this step
-      void *fl = dir == SOUTH ? blk.flux_S : blk.flux_W;
-      for (int v = threadIdx.x; v < Nv; v += NT) St::store(fl, base + v, v2(fw[2 * v], fw[2 * v + 1]));
+      for (int v = threadIdx.x; v < Nv; v += NT) store_flux(v, fw[2 * v], fw[2 * v + 1]);
       return;
     }
     // re-emission of the reflected flux: adsorbingWallD_P2 (clAdsorb.c:821-975,
@@ -958,13 +607,12 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     if (refl > 0.0) {
       // the reflected incoming distribution (wall_dist) of every velocity,
       // staged in the slope buffer, which wall faces do not use
-      R2 *rin = sgb;
       __syncthreads();
       if (kind != UGKS_REFLECT_DIFFUSE)
         for (int v = threadIdx.x; v < Nv; v += NT) {
           const V2 x = ld2(blk.wall_dist, (size_t)ci * Nv + v);
-          rin[v].x = (R)x.x;
-          rin[v].y = (R)x.y;
+          rin[v].x = x.x;
+          rin[v].y = x.y;
         }
       __syncthreads();
       const double an = d.alpha_n[wall], at = d.alpha_t[wall], Tw = 1.0 / wl.s3;
@@ -980,7 +628,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
             for (int va = 0; va < Nv; ++va) {
               const V2 uv_in = fvel(va);
               if (!upwind_flag(uv_in.x, rot) && uv_in.x != 0.0) {
-                const R2 fi = rin[va];
+                const auto fi = rin[va];
                 const V2 c = cercignani_lampis(d.PI, uv_in, uv, v2(fi.x, fi.y), an, at, Tw, wl.s3);
                 out.x += c.x;
                 out.y += c.y;
@@ -989,7 +637,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
             out.x *= wt[v];
             out.y *= wt[v];
           } else {
-            const R2 x = rin[dir == WEST ? d.mirror_EW[v] : d.mirror_NS[v]];
+            const auto x = rin[dir == WEST ? d.mirror_EW[v] : d.mirror_NS[v]];
             out = v2(x.x, x.y);
           }
         }
@@ -1018,7 +666,6 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     }
   }
   // wallFlux (clUGKS.c:910-1011) and wallMassEnergyFluxes (1019-1147)
-  void *flux = dir == SOUTH ? blk.flux_S : blk.flux_W;
   double s[12];
 #pragma unroll
   for (int k = 0; k < 12; ++k) s[k] = 0.0;
@@ -1026,7 +673,7 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     const V2 uv = fvel(v);
     const double wh = fw[2 * v], wb = fw[2 * v + 1];
     const double oh = uv.x * wh * len * dt, ob = uv.x * wb * len * dt;
-    St::store(flux, base + v, v2(oh, ob));
+    store_flux(v, oh, ob);
     const double uu = uv.x * uv.x + uv.y * uv.y;
     s[0] += uv.x * wh;
     s[1] += uv.x * uv.x * wh;
@@ -1046,6 +693,346 @@ __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B
     wf[0] = -rot * s[4]; wf[1] = rot * s[8]; wf[2] = -rot * s[5]; wf[3] = rot * s[9];
     wf[4] = -rot * s[6]; wf[5] = rot * s[10]; wf[6] = -rot * s[7]; wf[7] = rot * s[11];
   }
+}
+
+// Per-face coefficient block of an interior face, called by every thread of
+// the face CTA once W, prim and the neighbour cells (sh.nbr) are in place:
+// getPLR slopes (clUGKS.c:424-436) and initMacroFlux (446-518) split over
+// lanes 0 / 1 of warp 0 (one per side, the same instructions with one sign
+// flipped) while lane 0 of warp 1 computes the time weights and hands them
+// over through named barrier 1; the threads from warp 1 on run
+// meanwhile(t, nt) (item t of nt) in the meantime.  Leaves in sh.bcast:
+//   [0..4] / [5..9] distFlux coefficients of the upwind slope aL / aR,
+//   [10..14] those of the time slope aT ([10] includes Mt0),
+//   [15] Mt0, [16] Mt3 len, [17] Mt4 len,
+//   [18..21] len * g0, the analytic equilibrium part of the macro flux.
+template <int NT, typename Meanwhile>
+__device__ __forceinline__ void face_coefficients(const ugks_block_desc &d, FaceShared<NT> &sh, const P4 W,
+                                                  const P4 prim, const Rcp rc, const double len, const double dt,
+                                                  Meanwhile meanwhile) {
+  if (threadIdx.x < 32) {
+    const double kb = (0.5 * d.K) * rc.lam;
+    double Mv[MTUM], Mxi[3];
+    P4 a;
+    if (threadIdx.x < 2) {
+      const int side = threadIdx.x;
+      const double sg = side == 0 ? 1.0 : -1.0;
+      double Mh[MNUM];
+      half_moments_rcp(d.PI, d.K, prim, rc, sg, Mh, Mv, Mxi);
+      const double *o = sh.nbr[side];
+      // left: (W - W_L) / |mid - c_L|; right: (W_R - W) / |mid - c_R|
+      const double id = sg * o[4];
+      a = micro_slope_rcp(d.K, prim, rc,
+                          p4((W.s0 - o[0]) * id, (W.s1 - o[1]) * id, (W.s2 - o[2]) * id, (W.s3 - o[3]) * id));
+      const P4 t1 = moment_au(a, Mh, Mv, Mxi, 1, 0), t2 = moment_au(a, Mh, Mv, Mxi, 2, 0);
+      double *x = sh.lr[side];
+#pragma unroll
+      for (int k = 0; k < MNUM; ++k) x[k] = Mh[k];
+      x[7] = a.s0; x[8] = a.s1; x[9] = a.s2; x[10] = a.s3;
+      x[11] = t1.s0; x[12] = t1.s1; x[13] = t1.s2; x[14] = t1.s3;
+      x[15] = t2.s0; x[16] = t2.s1; x[17] = t2.s2; x[18] = t2.s3;
+    }
+    pair_wait();
+    double Mt[5];
+#pragma unroll
+    for (int k = 0; k < 5; ++k) Mt[k] = sh.mt[k];
+    double *c = sh.bcast;
+    if (threadIdx.x < 2) {
+      // distFlux coefficients of the upwind slope (derivation at sweep 3)
+      const double xk = Mxi[2] - kb * kb;
+      double *ck = c + 5 * threadIdx.x;
+      ck[0] = Mt[1] * fma(0.5 * a.s3, kb, a.s0);
+      ck[1] = Mt[1] * a.s1;
+      ck[2] = Mt[1] * a.s2;
+      ck[3] = Mt[1] * (0.5 * a.s3);
+      ck[4] = Mt[1] * (0.5 * a.s3 * xk);
+    }
+    if (threadIdx.x == 0) {
+      const double *xl = sh.lr[0], *xr = sh.lr[1];
+      double Mu[MNUM];
+#pragma unroll
+      for (int k = 0; k < MNUM; ++k) Mu[k] = xl[k] + xr[k];
+      const P4 aT = micro_slope_rcp(d.K, prim, rc,
+                                    scale(-prim.s0, add(p4(xl[11], xl[12], xl[13], xl[14]),
+                                                        p4(xr[11], xr[12], xr[13], xr[14]))));
+      const P4 g0 = scale(prim.s0,
+                          add(add(scale(Mt[0], moment_uv(Mu, Mv, Mxi, 1, 0, 0)),
+                                  scale(Mt[1], add(p4(xl[15], xl[16], xl[17], xl[18]),
+                                                   p4(xr[15], xr[16], xr[17], xr[18])))),
+                              scale(Mt[2], moment_au(aT, Mu, Mv, Mxi, 1, 0))));
+      const double xk = Mxi[2] - kb * kb;
+      c[10] = Mt[2] * fma(0.5 * aT.s3, kb, aT.s0) + Mt[0];
+      c[11] = Mt[2] * aT.s1;
+      c[12] = Mt[2] * aT.s2;
+      c[13] = Mt[2] * (0.5 * aT.s3);
+      c[14] = Mt[2] * (0.5 * aT.s3 * xk);
+      c[15] = Mt[0];
+      c[16] = Mt[3] * len;
+      c[17] = Mt[4] * len;
+      c[18] = len * g0.s0; c[19] = len * g0.s1; c[20] = len * g0.s2; c[21] = len * g0.s3;
+    }
+  } else {
+    if (threadIdx.x < 64) {
+      if (threadIdx.x == 32) {
+        double Mt[5];
+        time_weights_rcp(inv_relax_time_rcp(d, prim, rc), dt, Mt);
+#pragma unroll
+        for (int k = 0; k < 5; ++k) sh.mt[k] = Mt[k];
+      }
+      pair_arrive();
+    }
+    // warp 1, which computed the time weights, takes the last items
+    meanwhile((threadIdx.x + NT - 96) % (NT - 32), NT - 32);
+  }
+}
+
+// the two cells beside an interior face (the inputs of getAL / getAR and the
+// getPLR slopes, clUGKS.c:424-436) into sh.nbr, by two lanes of the last warp
+template <int NT>
+__device__ __forceinline__ void face_neighbours(const ugks_fused_block &blk, FaceShared<NT> &sh, const long gi,
+                                                const long gj, const int dir, const V2 n, const V2 mid) {
+  if (threadIdx.x >= NT - 32 && threadIdx.x < NT - 30) {
+    const ugks_block_desc &d = blk.d;
+    const int side = threadIdx.x - (NT - 32);  // 0: left (u > 0 upwind), 1: right
+    const size_t k = side == 0 ? gidx(d, gi - dir, gj - (1 - dir)) : gidx(d, gi, gj);
+    const P4 mc = ld4(blk.cell_mom, k);
+    const V2 uc = to_local(v2(mc.s1, mc.s2), n);
+    const V2 cc = ld2(blk.centre, k);
+    double *o = sh.nbr[side];
+    o[0] = mc.s0;
+    o[1] = uc.x;
+    o[2] = uc.y;
+    o[3] = mc.s3;
+    o[4] = nr_rcp(sqrt((mid.x - cc.x) * (mid.x - cc.x) + (mid.y - cc.y) * (mid.y - cc.y)));
+  }
+}
+
+// face work item -> (block, i, j, direction, wall face); false when the item
+// is skipped (inactive solve, retry pass of a solve without retry, other flux
+// method, or the unused S face of the last column / W face of the last row).
+// S and W faces of one corner (i, j) are adjacent work items so that both
+// directions read f while it is in L2.
+struct FaceWork {
+  int bi, dir, mi, mj, wall;
+  long gi, gj;
+};
+template <int FM>
+__device__ __forceinline__ bool face_work(const ugks_fused_block *__restrict__ B, int nb,
+                                          const ugks_solve_state *__restrict__ solves, const int w, int retry_pass,
+                                          FaceWork &fw) {
+  fw.bi = find_block<0>(B, nb, w);
+  const ugks_fused_block &blk = B[fw.bi];
+  const ugks_block_desc &d = blk.d;
+  const ugks_solve_state &sol = solves[blk.solve];
+  if (!sol.active) return false;
+  if (retry_pass && !sol.retry) return false;
+  if (d.flux_method != FM) return false;
+  int lf = w - blk.face_begin;
+  fw.dir = lf & 1;
+  lf >>= 1;
+  fw.mi = lf / (d.nj + 1);
+  fw.mj = lf % (d.nj + 1);
+  if (fw.dir == SOUTH ? (fw.mi >= d.ni) : (fw.mj >= d.nj)) return false;
+  fw.gi = fw.mi + d.ghost;
+  fw.gj = fw.mj + d.ghost;
+  fw.wall = -1;
+  if (fw.dir == SOUTH) {
+    if (fw.mj == 0 && is_wall(blk.bc_type[GSOUTH])) fw.wall = GSOUTH;
+    else if (fw.mj == d.nj && is_wall(blk.bc_type[GNORTH])) fw.wall = GNORTH;
+  } else {
+    if (fw.mi == 0 && is_wall(blk.bc_type[GWEST])) fw.wall = GWEST;
+    else if (fw.mi == d.ni && is_wall(blk.bc_type[GEAST])) fw.wall = GEAST;
+  }
+  return true;
+}
+
+// one FP64 face work item (all threads of the CTA take part)
+template <int FM, int NT>
+__device__ __forceinline__ void face_item_fp64(const ugks_fused_block *__restrict__ B, int nb,
+                                               ugks_solve_state *__restrict__ solves, const int w, int retry_pass) {
+  extern __shared__ double dyn[];
+  __shared__ FaceShared<NT> sh;
+  using St = Store<double>;
+  FaceWork fwk;
+  if (!face_work<FM>(B, nb, solves, w, retry_pass, fwk)) return;
+  const ugks_fused_block &blk = B[fwk.bi];
+  const ugks_block_desc &d = blk.d;
+  ugks_solve_state &sol = solves[blk.solve];
+  const double dt = sol.dt;
+  const int dir = fwk.dir, mi = fwk.mi, mj = fwk.mj, wall = fwk.wall;
+  const long gi = fwk.gi, gj = fwk.gj;
+  const int Nv = d.Nv;
+
+  // per velocity: (h, b) at the face and their slopes, kept for the later
+  // sweeps in shared memory
+  double2 *fhb = reinterpret_cast<double2 *>(dyn), *sgb = fhb + Nv;
+  const V2 n = ld2(blk.normal, faceidx(d, gi, gj, dir));
+  const V2 mid = ld2(blk.mid_side, faceidx(d, gi, gj, dir));
+  // velocity tables and the face-frame velocity (interfaceVelocity,
+  // clFunctions.c:191-209), with the table pointers held in registers
+  const double2 *__restrict__ qd = reinterpret_cast<const double2 *>(d.quad);
+  const double *__restrict__ wt = d.weight;
+  auto fvel = [&](int vv) {
+    const double2 e = qd[vv];
+    return v2(e.x * n.x + e.y * n.y, e.x * (-n.y) + e.y * n.x);
+  };
+  // stencil geometry for both upwind directions (iFace, clUGKS.c:148-176),
+  // precomputed by face_geometry: index 1 for u > 0 (upwind cell before the
+  // face), 0 otherwise
+  double g6[6];
+  {
+    const double *fg = blk.face_geo + 6 * faceidx(d, gi, gj, dir);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) g6[k] = fg[k];
+  }
+  const double dist0 = g6[0], idist0 = g6[1], il0 = g6[2], dist1 = g6[3], idist1 = g6[4], il1 = g6[5];
+  const int step = dir == SOUTH ? Nv : d.Nj * Nv;
+  const size_t base = fidx(d, gi, gj, 0);
+  constexpr int MID = FM == 1 ? 2 : 1;
+  const double2 *fcell = reinterpret_cast<const double2 *>(blk.f) + base;  // cell (gi, gj), velocity 0
+  const double2 *up1 = fcell - (MID + 1) * step, *up0 = fcell + MID * step;
+
+  // ---- sweep 1: reconstruction (+ interior faces: the face moments W of
+  // getFaceCons; the 1/2 of the energy moment is applied after the sum)
+  double m[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 1
+  for (int v = threadIdx.x; v < Nv; v += NT) {
+    const V2 uv = fvel(v);
+    const bool up = uv.x > 0.0;
+    double ffh, ffb, sx, sy;
+    reconstruct<double, FM>((up ? up1 : up0) + v, up ? step : -step, up ? il1 : il0, up ? dist1 : dist0,
+                            up ? idist1 : idist0, ffh, ffb, sx, sy);
+    fhb[v] = make_double2(ffh, ffb);
+    sgb[v] = make_double2(sx, sy);
+    if (wall < 0) {
+      const double uu = fma(uv.x, uv.x, uv.y * uv.y);
+      m[0] += ffh;
+      m[1] = fma(uv.x, ffh, m[1]);
+      m[2] = fma(uv.y, ffh, m[2]);
+      m[3] += fma(uu, ffh, ffb);
+    }
+  }
+  // loaded by the last warp, which has the fewest velocities in sweep 1
+  if (wall < 0) face_neighbours<NT>(blk, sh, gi, gj, dir, n, mid);
+  const double len = blk.side_length[faceidx(d, gi, gj, dir)];
+
+  if (wall < 0) {
+    // ---------------- interior face ----------------
+    block_sum<4>(m, sh.scratch);
+    const P4 W = p4(m[0], m[1], m[2], 0.5 * m[3]);
+    Rcp rc;
+    const P4 prim = to_primary_rcp(d, W, rc);  // getPLR (clUGKS.c:421-422), every thread
+    const int un = d.u_num, vn = d.v_num;
+    const bool sep = un > 0 && un * vn == Nv && un + vn <= 512;
+    double *Eu = reinterpret_cast<double *>(sgb + Nv), *Ev = Eu + (sep ? un : 0);
+    const V2 Ug = to_global(v2(prim.s1, prim.s2), n);  // face mean velocity, global frame
+    // Maxwellian prefactor rho lambda / pi (fM, clFunctions.c:49-58), times the
+    // face length: every per-velocity flux below carries the length
+    const double chl = (prim.s0 * (prim.s3 / d.PI)) * len;
+    double q[2] = {0.0, 0.0};
+    face_coefficients<NT>(d, sh, W, prim, rc, len, dt, [&](int t, int nt) {
+      // face heat flux (calcFaceQ, clUGKS.c:522-585) and the axis factors of
+      // the face Maxwellian
+      const double Kinv = 1.0 / d.K;
+      for (int v = t; v < Nv; v += nt) {
+        const V2 uv = fvel(v);
+        const double cx = uv.x - prim.s1, cy = uv.y - prim.s2, c2 = cx * cx + cy * cy;
+        const double2 fv = fhb[v];
+        const double tq = c2 * fv.x + fv.y * Kinv;
+        q[0] += 0.5 * (cx * tq);
+        q[1] += 0.5 * (cy * tq);
+      }
+      if (sep) {
+        axis_exp(Eu, d.quad, un, vn, 0, Ug.x, prim.s3, t, nt, chl);
+        axis_exp(Ev, d.quad, vn, 1, 1, Ug.y, prim.s3, t, nt);
+      }
+    });
+    block_sum<2>(q, sh.scratch);
+    // ---- sweep 3: macroFlux (587-681) and distFlux (683-772).
+    // With h0 = weight * fM (times the face length), kb = K / (2 lambda),
+    // S = Mt0 s (c . Q) (the Shakhov factor of fS, clFunctions.c:64-77, times
+    // Mt0), P4 = 2 lambda c^2 - 4, the upwind slope a (aL for u > 0, else aR),
+    //   Ph = a0 + a1 u + a2 v + a3 (|u|^2 + kb) / 2, and Th likewise with aT,
+    //   Rh = Mt3 fh - Mt4 u sh,   Rb = Mt3 fb - Mt4 u sb,
+    //   Zh = u (S P4 h0 + Rh),    Zb = u (S (P4 + 2) kb h0 + Rb),
+    //   B  = Mt0 + Mt1 u Ph + Mt2 Th,
+    // distFlux's two components are
+    //   hx = Zh + u h0 B,
+    //   hy = Zb + u h0 (kb B + Mt1 u a3 X / 2 + Mt2 aT3 X / 2),  X = Mxi2 - kb^2,
+    // and macroFlux's discrete part sums (Zh, u Zh, v Zh, (|u|^2 Zh + Zb) / 2).
+    const double *c = sh.bcast;
+    const V2 Q = v2(q[0], q[1]);
+    const double lam = prim.s3, Ux = prim.s1, Uy = prim.s2, lam2 = 2.0 * lam;
+    const double kb = (0.5 * d.K) * rc.lam;
+    const double s0 = 0.8 * (1 - d.Pr) * (lam * lam) * rc.rho;
+    const double Mt0 = c[15], Mt3 = c[16], Mt4 = c[17];
+    const double sx = (Mt0 * s0) * Q.x, sy = (Mt0 * s0) * Q.y;
+    const double T0 = c[10], T1 = c[11], T2 = c[12], T3 = c[13], CT = c[14];
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    void *flux = dir == SOUTH ? blk.flux_S : blk.flux_W;
+    const int qs = sep ? NT / vn : 0, rs = sep ? NT % vn : 0;
+    int iu = sep ? threadIdx.x / vn : 0, jv = sep ? threadIdx.x % vn : 0;
+    for (int v = threadIdx.x; v < Nv; v += NT) {
+      const V2 uv = fvel(v);
+      const double u = uv.x, vt = uv.y, uu = fma(u, u, vt * vt);
+      const double cx = u - Ux, cy = vt - Uy, c2 = fma(cx, cx, cy * cy);
+      double E;
+      if (sep) {
+        E = Eu[iu] * Ev[jv];
+        jv += rs;
+        iu += qs;
+        if (jv >= vn) { jv -= vn; ++iu; }
+      } else {
+        E = chl * exp(-lam * c2);
+      }
+      const double h0 = wt[v] * E;
+      const double Sp = fma(cx, sx, cy * sy);
+      const double S4 = Sp * fma(lam2, c2, -4.0), S2 = fma(2.0, Sp, S4);
+      const double *A = c + (u > 0.0 ? 0 : 5);
+      const double MP = fma(A[3], uu, fma(A[2], vt, fma(A[1], u, A[0])));
+      const double Bk = fma(u, MP, fma(T3, uu, fma(T2, vt, fma(T1, u, T0))));
+      const double2 fd = fhb[v], fs = sgb[v];
+      const double mu = Mt4 * u;
+      const double Rh = fma(-mu, fs.x, Mt3 * fd.x), Rb = fma(-mu, fs.y, Mt3 * fd.y);
+      const double Zh = u * fma(S4, h0, Rh), Zb = u * fma(S2, h0 * kb, Rb);
+      const double uh = u * h0;
+      const double hx = fma(uh, Bk, Zh);
+      const double hy = fma(uh, fma(kb, Bk, fma(A[4], u, CT)), Zb);
+      acc[0] += Zh;
+      acc[1] = fma(u, Zh, acc[1]);
+      acc[2] = fma(vt, Zh, acc[2]);
+      acc[3] = fma(uu, Zh, acc[3]);
+      acc[4] += Zb;
+      St::store(flux, base + v, v2(hx, hy));
+    }
+    block_sum_to0<5>(acc, sh.scratch);
+    if (threadIdx.x == 0) {
+      P4 out = p4(acc[0] + c[18], acc[1] + c[19], acc[2] + c[20], 0.5 * (acc[3] + acc[4]) + c[21]);
+      const V2 g = to_global(v2(out.s1, out.s2), n);
+      out.s1 = g.x;
+      out.s2 = g.y;
+      st4(dir == SOUTH ? blk.flux_macro_S : blk.flux_macro_W, gidx(d, gi, gj), out);
+    }
+    return;
+  }
+
+  // ---------------- wall face ----------------
+  wall_face<NT>(blk, sol, sh, reinterpret_cast<double *>(fhb), sgb, wall, dir, gi, gj, mi, mj, n, len, dt,
+                [&](int v, double hx, double hy) { St::store(dir == SOUTH ? blk.flux_S : blk.flux_W, base + v,
+                                                               v2(hx, hy)); });
+}
+
+// the mixed path's face work item (ugks_delta.cuh, included further down)
+template <int FM, int NT>
+__device__ __forceinline__ void face_item_delta(const ugks_fused_block *__restrict__ B, int nb,
+                                                ugks_solve_state *__restrict__ solves, const int w, int retry_pass);
+
+// one face work item: FP64 storage, or the mixed path's FP32 deviations
+template <typename T, int FM, int NT>
+__device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B, int nb,
+                                          ugks_solve_state *__restrict__ solves, const int w, int retry_pass) {
+  if constexpr (std::is_same<T, float>::value) face_item_delta<FM, NT>(B, nb, solves, w, retry_pass);
+  else face_item_fp64<FM, NT>(B, nb, solves, w, retry_pass);
 }
 
 // main face pass: one CTA per face work item of the blocks of one flux method
@@ -1101,8 +1088,8 @@ __device__ __forceinline__ void warp_sum(double (&x)[N]) {
   }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(CW * 32, CellBudget<T>::minb) cell_pass(const ugks_fused_block *__restrict__ B, int nb,
+template <typename T, int MINB = CellBudget<T>::minb>
+__global__ void __launch_bounds__(CW * 32, MINB) cell_pass(const ugks_fused_block *__restrict__ B, int nb,
                                                         ugks_solve_state *__restrict__ solves, int n_cells,
                                                         int wstride) {
   extern __shared__ double dyn[];
@@ -1592,15 +1579,30 @@ __global__ void dt_init(ugks_solve_state *solves, int ns) {
   x.retry = 0;
 }
 
+// the mixed-precision (FP32 deviation) kernels
+#include "ugks_delta.cuh"
+
+// the ghost update of every block of the table
+template <typename T>
+void launch_ghosts(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks_solve_state *solves,
+                   cudaStream_t st) {
+  if (!z->n_ghost) return;
+  if (std::is_same<T, float>::value) ghost_pass_delta<<<z->n_ghost, FT, 0, st>>>(B, nb, solves);
+  else ghost_pass<double><<<z->n_ghost, FT, 0, st>>>(B, nb, solves);
+}
+
 template <typename T>
 int init_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks_solve_state *solves,
               int ns, void *stream) {
   cudaStream_t st = S(stream);
   init_walls<<<nb, 128, 0, st>>>(B, nb);
   if (z->n_faces) face_geometry<<<(z->n_faces + 127) / 128, 128, 0, st>>>(B, nb, z->n_faces);
-  if (z->n_cells) init_cells<T><<<z->n_cells, FT, 0, st>>>(B, nb, solves);
+  if (z->n_cells) {
+    if (std::is_same<T, float>::value) setup_cells_delta<true><<<z->n_cells, FT, 0, st>>>(B, nb, solves);
+    else init_cells<double><<<z->n_cells, FT, 0, st>>>(B, nb, solves);
+  }
   dt_init<<<(ns + 127) / 128, 128, 0, st>>>(solves, ns);
-  if (z->n_ghost) ghost_pass<T><<<z->n_ghost, FT, 0, st>>>(B, nb, solves);
+  launch_ghosts<T>(B, nb, z, solves, st);
   return launch_status();
 }
 
@@ -1610,9 +1612,12 @@ int restart_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, u
   cudaStream_t st = S(stream);
   init_walls<<<nb, 128, 0, st>>>(B, nb);
   if (z->n_faces) face_geometry<<<(z->n_faces + 127) / 128, 128, 0, st>>>(B, nb, z->n_faces);
-  if (z->n_cells) restart_cells<T><<<z->n_cells, FT, 0, st>>>(B, nb, solves);
+  if (z->n_cells) {
+    if (std::is_same<T, float>::value) setup_cells_delta<false><<<z->n_cells, FT, 0, st>>>(B, nb, solves);
+    else restart_cells<double><<<z->n_cells, FT, 0, st>>>(B, nb, solves);
+  }
   dt_init<<<(ns + 127) / 128, 128, 0, st>>>(solves, ns);
-  if (z->n_ghost) ghost_pass<T><<<z->n_ghost, FT, 0, st>>>(B, nb, solves);
+  launch_ghosts<T>(B, nb, z, solves, st);
   return launch_status();
 }
 
@@ -1626,6 +1631,21 @@ cudaError_t set_face_attributes() {
     e = cudaFuncSetAttribute(face_pass<T, FM, MINB, NT>, cudaFuncAttributePreferredSharedMemoryCarveout,
                              cudaSharedmemCarveoutMaxShared);
   return e;
+}
+
+template <typename T, int V>
+cudaError_t set_face_shape() {
+  constexpr int NT = FaceShape<T, V>::nt, MINB = FaceShape<T, V>::minb;
+  cudaError_t e = set_face_attributes<T, 0, MINB, NT>();
+  if (e == cudaSuccess) e = set_face_attributes<T, 1, MINB, NT>();
+  if (e == cudaSuccess) e = set_face_attributes<T, 3, MINB, NT>();
+  return e;
+}
+template <typename T, int MINB>
+cudaError_t set_cell_attributes() {
+  if (std::is_same<T, float>::value)
+    return cudaFuncSetAttribute(cell_pass_delta<MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  return cudaFuncSetAttribute(cell_pass<double, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
 }
 
 // Kernel attributes (the dynamic shared memory above 48 KB that the face and
@@ -1642,14 +1662,9 @@ cudaError_t set_step_attributes() {
   if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> guard(lock);
   if (done[dev]) return cudaSuccess;
-  cudaError_t r[7] = {
-      set_face_attributes<T, 0, FaceBudget<T>::narrow, FT>(),
-      set_face_attributes<T, 1, FaceBudget<T>::narrow, FT>(),
-      set_face_attributes<T, 3, FaceBudget<T>::narrow, FT>(),
-      set_face_attributes<T, 0, FaceBudget<T>::wide, FaceBudget<T>::wide_threads>(),
-      set_face_attributes<T, 1, FaceBudget<T>::wide, FaceBudget<T>::wide_threads>(),
-      set_face_attributes<T, 3, FaceBudget<T>::wide, FaceBudget<T>::wide_threads>(),
-      cudaFuncSetAttribute(cell_pass<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024)};
+  cudaError_t r[6] = {
+      set_face_shape<T, 1>(), set_face_shape<T, 2>(), set_face_shape<T, 3>(), set_face_shape<T, 4>(),
+      set_cell_attributes<T, 2>(), set_cell_attributes<T, 3>()};
   for (cudaError_t x : r)
     if (x != cudaSuccess) return x;
   done[dev] = true;
@@ -1660,8 +1675,8 @@ cudaError_t set_step_attributes() {
 // (FP32: also the face-frame velocity per node, as float2)
 template <typename T>
 inline size_t face_smem(int max_nv, int max_axes) {
-  const size_t per_v = std::is_same<T, float>::value ? 3 * sizeof(float2) : 4 * sizeof(double);
-  return per_v * (size_t)max_nv + sizeof(T) * (size_t)max_axes;
+  if (std::is_same<T, float>::value) return delta_face_smem(max_nv, max_axes);
+  return 4 * sizeof(double) * (size_t)max_nv + sizeof(double) * (size_t)max_axes;
 }
 
 // the main face pass of one segment (one flux method, one register budget)
@@ -1693,8 +1708,10 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
   // face pass: (h, b) and slopes per velocity + the two axis factor tables;
   // cell pass: the axis factor tables of the old and new macro state
   const size_t smem = face_smem<T>(z->max_nv, z->max_axes);
-  const int cstride = 2 * z->max_axes + CELL_COEF;  // doubles of shared memory per cell warp
-  const size_t csmem = (size_t)CW * cstride * sizeof(double) + (size_t)CW * cell_ring_bytes<T>();
+  constexpr bool mixed = std::is_same<T, float>::value;
+  // doubles of shared memory per cell warp
+  const int cstride = mixed ? delta_cell_stride(z->max_axes) : 2 * z->max_axes + CELL_COEF;
+  const size_t csmem = (size_t)CW * cstride * sizeof(double) + (mixed ? 0 : (size_t)CW * cell_ring_bytes<T>());
   const cudaError_t attr = set_step_attributes<T>();
   if (attr != cudaSuccess) return -(int)attr;
   if (smem > 200 * 1024 || csmem > 200 * 1024) return -(int)cudaErrorInvalidValue;
@@ -1706,10 +1723,15 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
   for (int k = 0; k < z->n_segments && k < UGKS_MAX_FACE_SEGMENTS; ++k) {
     if (z->seg_count[k] <= 0) continue;
     const size_t sm = face_smem<T>(z->seg_max_nv[k], z->seg_max_axes[k]);
-    if (z->seg_max_nv[k] <= FaceBudget<T>::narrow_max_nv)
-      launch_segment<T, FaceBudget<T>::narrow, FT>(B, nb, solves, z->seg_method[k], z->seg_begin[k], z->seg_count[k], sm, st);
-    else
-      launch_segment<T, FaceBudget<T>::wide, FaceBudget<T>::wide_threads>(B, nb, solves, z->seg_method[k], z->seg_begin[k], z->seg_count[k], sm, st);
+    int v = z->seg_variant[k];
+    if (v <= 0 || v > 4) v = z->seg_max_nv[k] <= FaceBudget<T>::narrow_max_nv ? 1 : 4;
+    const int m = z->seg_method[k], b0 = z->seg_begin[k], n = z->seg_count[k];
+    switch (v) {
+      case 1: launch_segment<T, FaceShape<T, 1>::minb, FaceShape<T, 1>::nt>(B, nb, solves, m, b0, n, sm, st); break;
+      case 2: launch_segment<T, FaceShape<T, 2>::minb, FaceShape<T, 2>::nt>(B, nb, solves, m, b0, n, sm, st); break;
+      case 3: launch_segment<T, FaceShape<T, 3>::minb, FaceShape<T, 3>::nt>(B, nb, solves, m, b0, n, sm, st); break;
+      default: launch_segment<T, FaceShape<T, 4>::minb, FaceShape<T, 4>::nt>(B, nb, solves, m, b0, n, sm, st); break;
+    }
   }
   const bool narrow = z->max_nv <= FaceBudget<T>::narrow_max_nv;
   mark(1);
@@ -1720,11 +1742,22 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
   mark(3);
   dt_check<<<sg, 128, 0, st>>>(solves, ns, 1);
   mark(4);
-  if (z->n_cells) cell_pass<T><<<(z->n_cells + CW - 1) / CW, CW * 32, csmem, st>>>(B, nb, solves, z->n_cells, cstride);
+  if (z->n_cells) {
+    // cell_variant: 0 the default register budget, 2 or 3 CTAs of 8 warps per SM
+    const unsigned cg = (unsigned)((z->n_cells + CW - 1) / CW);
+    const int cv = z->cell_variant == 2 || z->cell_variant == 3 ? z->cell_variant : CellBudget<T>::minb;
+    if (mixed) {
+      if (cv == 3) cell_pass_delta<3><<<cg, CW * 32, csmem, st>>>(B, nb, solves, z->n_cells, cstride);
+      else cell_pass_delta<2><<<cg, CW * 32, csmem, st>>>(B, nb, solves, z->n_cells, cstride);
+    } else {
+      if (cv == 3) cell_pass<double, 3><<<cg, CW * 32, csmem, st>>>(B, nb, solves, z->n_cells, cstride);
+      else cell_pass<double, 2><<<cg, CW * 32, csmem, st>>>(B, nb, solves, z->n_cells, cstride);
+    }
+  }
   mark(5);
   dt_update<<<sg, 128, 0, st>>>(solves, ns);
   mark(6);
-  if (z->n_ghost) ghost_pass<T><<<z->n_ghost, FT, 0, st>>>(B, nb, solves);
+  launch_ghosts<T>(B, nb, z, solves, st);
   mark(7);
   return launch_status();
 }
@@ -1734,7 +1767,7 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
 __global__ void residual_kernel(const ugks_fused_block *B, int nb, ugks_solve_state *solves, int ns) {
   __shared__ double scratch[8 * (FT / 32)];
   const int s = blockIdx.x;
-  if (s >= ns) return;
+  if (s >= ns || !solves[s].active) return;  // a stopped solve keeps its last residual
   double r[4] = {0.0, 0.0, 0.0, 0.0};
   int n = 0;
   for (int b = 0; b < nb; ++b) {
@@ -1762,6 +1795,22 @@ __global__ void residual_kernel(const ugks_fused_block *B, int nb, ugks_solve_st
   }
   if (threadIdx.x == 0)
     for (int k = 0; k < 4; ++k) solves[s].residual[k] = n ? r[k] / n : 0.0;
+}
+
+// the stop rule of every active solve (ugks_stop_check)
+__global__ void stop_check(ugks_solve_state *solves, int ns) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= ns) return;
+  ugks_solve_state &x = solves[s];
+  if (!x.active) return;
+  int why = 0;
+  if (x.status != 0) why = UGKS_STOP_ERROR;
+  else if (x.stop_residual > 0.0 && x.residual[0] < x.stop_residual) why = UGKS_STOP_CONVERGED;
+  else if (x.stop_steps > 0 && x.steps >= x.stop_steps) why = UGKS_STOP_STEPS;
+  if (why) {
+    x.stopped = why;
+    x.active = 0;
+  }
 }
 
 }  // namespace
@@ -1799,6 +1848,29 @@ int ugks_residual(const ugks_fused_block *blocks_dev, int nblocks, ugks_solve_st
   if (nsolves <= 0) return 0;
   residual_kernel<<<nsolves, FT, 0, S(stream)>>>(blocks_dev, nblocks, solves_dev, nsolves);
   return launch_status();
+}
+
+int ugks_stop_check(ugks_solve_state *solves_dev, int nsolves, void *stream) {
+  if (nsolves <= 0) return 0;
+  stop_check<<<(nsolves + 127) / 128, 128, 0, S(stream)>>>(solves_dev, nsolves);
+  return launch_status();
+}
+
+int ugks_serve_steps(int mixed, const ugks_fused_block *blocks_dev, int nblocks, const ugks_fused_sizes *sizes,
+                     ugks_solve_state *solves_dev, int nsolves, int nsteps, void *stream) {
+  for (int k = 0; k < nsteps; ++k) {
+    int rc = mixed ? step_impl<float>(blocks_dev, nblocks, sizes, solves_dev, nsolves, stream)
+                   : step_impl<double>(blocks_dev, nblocks, sizes, solves_dev, nsolves, stream);
+    if (rc == 0) rc = ugks_residual(blocks_dev, nblocks, solves_dev, nsolves, stream);
+    if (rc == 0) rc = ugks_stop_check(solves_dev, nsolves, stream);
+    if (rc != 0) return rc;
+  }
+  return 0;
+}
+
+int ugks_prepare(int mixed) {
+  const cudaError_t e = mixed ? set_step_attributes<float>() : set_step_attributes<double>();
+  return e == cudaSuccess ? 0 : -(int)e;
 }
 
 int ugks_fused_layout(ugks_fused_block *blocks, int nblocks, ugks_fused_sizes *z) {
@@ -1878,6 +1950,8 @@ int ugks_fused_layout(ugks_fused_block *blocks, int nblocks, ugks_fused_sizes *z
     z->face_begin[m] = (int32_t)fb[m];
     z->face_count[m] = (int32_t)fc[m];
   }
+  for (int k = 0; k < UGKS_MAX_FACE_SEGMENTS; ++k) z->seg_variant[k] = 0;
+  z->cell_variant = 0;
   return 0;
 }
 

@@ -1034,7 +1034,7 @@ __global__ void __launch_bounds__(VT) k_adsorbingWallD_P2(ugks_block_desc d, siz
 
 extern "C" {
 
-const char *ugks_version(void) { return "ugks_b200 0.1 (sm_100a)"; }
+const char *ugks_version(void) { return "ugks_b200 0.2 (sm_100a)"; }
 
 int ugks_abi_sizes(int64_t *out, int n) {
   const int64_t v[7] = {(int64_t)sizeof(ugks_block_desc), (int64_t)sizeof(ugks_fused_block),

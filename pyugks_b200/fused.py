@@ -11,8 +11,9 @@ advances them with the fused entry points of libugks_b200.so:
 * ``ugks_residual``: the reference residual on demand.
 
 ``precision="fp64"`` stores f and the face fluxes as double (the plain
-method); ``"mixed"`` stores them as float, with moments, the conserved update,
-the relaxation and dt in FP64.
+method); ``"mixed"`` stores them as FP32 deviations from a reference
+Maxwellian of each solve, in velocity pairs along u (``to_pairs``), with moments, the
+conserved update, the relaxation and dt in FP64.
 """
 from __future__ import annotations
 
@@ -32,16 +33,96 @@ def _torch():
     return torch
 
 
+# ---------------------------------------------------------------------------
+# mixed precision: deviations from a reference Maxwellian in velocity pairs
+# ---------------------------------------------------------------------------
+def reference_state(case):
+    """(rho0, T0) of a solve's reference Maxwellian: the mean fill density, and
+    the wall temperature the gas relaxes to (mean over its diffuse and
+    adsorbing faces; the fill temperature when it has none)."""
+    rho, cells, tw = 0.0, 0, []
+    for b in case["blocks"]:
+        n = b["ni"] * b["nj"]
+        rho += float(np.mean(np.broadcast_to(np.asarray(b["fill"].get("D", 1.0), dtype=np.float64),
+                                             (b["ni"], b["nj"])))) * n
+        cells += n
+        tw += [bc["T"] for bc in b["bc"] if bc["type"] in (D.DIFFUSE, D.ADSORBING)]
+    T0 = float(np.mean(tw)) if tw else float(np.mean([np.mean(b["fill"].get("T", 1.0)) for b in case["blocks"]]))
+    return rho / cells, T0
+
+
+def reference_table(const, rho0, T0):
+    """The UGKS_REF_* array of include/ugks_b200.h for a reference Maxwellian
+    at rest with density rho0 and temperature T0 on this velocity grid."""
+    vg = const.vgrid
+    lam0 = 1.0 / T0
+    P0 = rho0 * lam0 / const.PI
+    kb0 = 0.5 * const.K / lam0
+    q = vg.quad
+    mh = vg.weight * P0 * np.exp(-lam0 * (q[:, 0] * q[:, 0] + q[:, 1] * q[:, 1]))
+    x, y = q[:, 0], q[:, 1]
+    mom = [np.sum(mh), np.sum(x * mh), np.sum(y * mh), np.sum(x * x * mh), np.sum(x * y * mh),
+           np.sum(y * y * mh), np.sum(x * x * x * mh), np.sum(x * x * y * mh), np.sum(x * y * y * mh),
+           np.sum(y * y * y * mh), np.sum(kb0 * mh), np.sum(x * kb0 * mh), np.sum(y * kb0 * mh)]
+    u = q[::vg.v_num, 0]
+    v = q[:vg.v_num, 1]
+    Au = vg.wu * np.sqrt(P0) * np.exp(-lam0 * u * u)
+    Av = vg.wv * np.sqrt(P0) * np.exp(-lam0 * v * v)
+    out = np.zeros(_lib.REF_TAB + vg.Nv + vg.u_num + vg.v_num)
+    out[_lib.REF_LAMBDA], out[_lib.REF_P0], out[_lib.REF_KB0] = lam0, P0, kb0
+    out[_lib.REF_MOM:_lib.REF_MOM + len(mom)] = mom
+    out[_lib.REF_TAB:_lib.REF_TAB + vg.Nv] = mh
+    out[_lib.REF_TAB + vg.Nv:_lib.REF_TAB + vg.Nv + vg.u_num] = Au
+    out[_lib.REF_TAB + vg.Nv + vg.u_num:] = Av
+    return out
+
+
+def pair_count(vg) -> int:
+    """Velocity pairs per cell of the mixed storage: ceil(u_num / 2) v_num."""
+    return (vg.u_num + 1) // 2 * vg.v_num
+
+
+def to_pairs(f, ref, vg):
+    """(..., Nv, 2) FP64 distributions -> (..., pair_count, 4) FP32 deviations
+    from the reference Maxwellian: pair a v_num + jv holds velocities
+    (2a, jv) and (2a + 1, jv) as (h, h', b, b'); an odd u_num pads the last
+    pair row's second lane with zeros."""
+    nv, un, vn = vg.Nv, vg.u_num, vg.v_num
+    lead = f.shape[:-2]
+    mh = ref[_lib.REF_TAB:_lib.REF_TAB + nv]
+    d = np.zeros(lead + (un + (un & 1), vn, 2))
+    d[..., :un, :, 0] = (f[..., 0] - mh).reshape(lead + (un, vn))
+    d[..., :un, :, 1] = (f[..., 1] - ref[_lib.REF_KB0] * mh).reshape(lead + (un, vn))
+    d = d.reshape(lead + ((un + 1) // 2, 2, vn, 2))             # (a, lane, jv, component)
+    d = np.moveaxis(d, -3, -1)                                   # (a, jv, component, lane)
+    return np.ascontiguousarray(d.reshape(lead + (pair_count(vg), 4))).astype(np.float32)
+
+
+def from_pairs(p, ref, vg):
+    """Inverse of to_pairs: FP64 (..., Nv, 2) distributions."""
+    nv, un, vn = vg.Nv, vg.u_num, vg.v_num
+    lead = p.shape[:-2]
+    d = np.asarray(p, dtype=np.float64).reshape(lead + ((un + 1) // 2, vn, 2, 2))  # (a, jv, comp, lane)
+    d = np.moveaxis(d, -1, -3).reshape(lead + (un + (un & 1), vn, 2))[..., :un, :, :].reshape(lead + (nv, 2))
+    mh = ref[_lib.REF_TAB:_lib.REF_TAB + nv]
+    out = np.empty(d.shape)
+    out[..., 0] = d[..., 0] + mh
+    out[..., 1] = d[..., 1] + ref[_lib.REF_KB0] * mh
+    return out
+
+
 class _Block:
     pass
 
 
 class FusedSolver:
-    def __init__(self, cases, precision: str = "fp64", device="cuda", stream=None, restart=None):
+    def __init__(self, cases, precision: str = "fp64", device="cuda", stream=None, restart=None, tune=False):
         """restart: {caller's solve index: checkpoint path or the dict of
         checkpoint.read}; those solves resume from the saved state (the
         reference's restart, ugks_sim.py:824-840, ugks_block.py:274-300)
-        instead of starting from their fill condition."""
+        instead of starting from their fill condition.
+        tune: pick the launch shapes with tuner.tune (cached per kind of
+        segment; timed on a scratch copy when not cached)."""
         torch = _torch()
         if precision not in ("fp64", "mixed"):
             raise ValueError(precision)
@@ -75,6 +156,11 @@ class FusedSolver:
             tabs = dict(quad=self._dev(vg.quad), weight=self._dev(vg.weight),
                         mNS=self._dev(vg.mirror_NS, torch.int32), mEW=self._dev(vg.mirror_EW, torch.int32),
                         mD=self._dev(vg.mirror_D, torch.int32))
+            if precision == "mixed":
+                if vg.u_num * vg.v_num != vg.Nv:
+                    raise ValueError("mixed precision needs a tensor velocity grid")
+                tabs["ref_host"] = reference_table(const, *reference_state(case))
+                tabs["ref"] = self._dev(tabs["ref_host"])
             self._keep.append(tabs)
             first = len(self.blocks)
             ids = []
@@ -116,7 +202,7 @@ class FusedSolver:
                 blk.macro.copy_(self._dev(bd["macro"]))
                 blk.Q.copy_(self._dev(bd["Q"]))
                 if bd["f"] is not None:
-                    blk.f.copy_(self._dev(bd["f"], self.sdtype))
+                    blk.f.copy_(self._dev(self._stored_f(blk, np.asarray(bd["f"], dtype=np.float64))))
                     with_f.add(s)
             st[s].time = data["blocks"][0]["time"]
             st[s].steps = int(data["final_step"])
@@ -139,6 +225,10 @@ class FusedSolver:
             self._set_active_internal([True] * self.nsolves)
         self._step_fn = self.lib.ugks_step_fp64 if precision == "fp64" else self.lib.ugks_step_mixed
         self.graph = None
+        self.shapes = None
+        if tune:
+            from . import tuner
+            self.shapes = tuner.tune(self)
 
     # ---------------------------------------------------------------- set-up
     def _dev(self, a, dtype=None):
@@ -158,9 +248,13 @@ class FusedSolver:
         blk.bc = b["bc"]
         dev = self.device
         z = lambda *shape, dt=torch.float64: torch.zeros(shape, dtype=dt, device=dev)
-        blk.f = z(Ni, Nj, Nv, 2, dt=self.sdtype)
-        blk.flux_S = z(Ni, Nj, Nv, 2, dt=self.sdtype)
-        blk.flux_W = z(Ni, Nj, Nv, 2, dt=self.sdtype)
+        # FP64: (h, b) per velocity; mixed: FP32 deviations in velocity pairs
+        shape = (Ni, Nj, Nv, 2) if self.precision == "fp64" else (Ni, Nj, pair_count(const.vgrid), 4)
+        blk.ref = tabs.get("ref_host")
+        blk.vgrid = const.vgrid
+        blk.f = z(*shape, dt=self.sdtype)
+        blk.flux_S = z(*shape, dt=self.sdtype)
+        blk.flux_W = z(*shape, dt=self.sdtype)
         blk.flux_macro_S = z(Ni, Nj, 4)
         blk.flux_macro_W = z(Ni, Nj, 4)
         macro, Q = fill_arrays(b)
@@ -204,6 +298,8 @@ class FusedSolver:
                      "area", "centre", "mid_side", "normal", "side_length", "xy", "wall_prop",
                      "wall_cover", "wall_fluxes", "wall_dist", "cell_mom", "Q_next", "face_geo"):
             setattr(x, name, getattr(blk, name).data_ptr())
+        if "ref" in tabs:
+            x.ref = tabs["ref"].data_ptr()
         blk.struct = x
         return blk
 
@@ -229,7 +325,9 @@ class FusedSolver:
     def capture(self, steps: int):
         """Capture `steps` steps as one CUDA graph; ``replay()`` runs it."""
         torch = _torch()
-        # the first launch sets kernel attributes, which is not capturable
+        # kernel attributes are set before capture (not a stream operation)
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.ugks_prepare(0 if self.precision == "fp64" else 1), "ugks_prepare")
         g = torch.cuda.CUDAGraph()
         s = torch.cuda.Stream(self.device)
         s.wait_stream(torch.cuda.current_stream(self.device))
@@ -257,8 +355,21 @@ class FusedSolver:
         raw = self.solves.cpu().numpy().tobytes()
         arr = (_lib.SolveState * self.nsolves).from_buffer_copy(raw)
         out = [dict(dt=x.dt, time=x.time, max_dt=x.max_dt, status=x.status, steps=x.steps,
-                    retries=x.retries, active=x.active, residual=list(x.residual)) for x in arr]
+                    retries=x.retries, active=x.active, stopped=x.stopped, residual=list(x.residual))
+               for x in arr]
         return [out[self.order[k]] for k in range(self.nsolves)]
+
+    def set_stop_rule(self, solve: int, tol: float = 0.0, max_steps: int = 0):
+        """The device-side stop rule of the caller's solve (ugks_stop_check):
+        stop when the density residual falls below tol or after max_steps
+        steps (0 disables either)."""
+        torch = _torch()
+        torch.cuda.synchronize(self.device)
+        st = (_lib.SolveState * self.nsolves).from_buffer_copy(self.solves.cpu().numpy().tobytes())
+        s = self.order[solve]
+        st[s].stop_residual = float(tol)
+        st[s].stop_steps = int(max_steps)
+        self.solves.copy_(torch.from_numpy(np.frombuffer(bytes(st), dtype=np.uint8).copy()))
 
     def set_active(self, flags):
         """Switch solves on/off for the next steps (device-side flag)."""
@@ -272,6 +383,20 @@ class FusedSolver:
             st[s].active = 1 if a else 0
         self.solves.copy_(torch.from_numpy(np.frombuffer(bytes(st), dtype=np.uint8).copy()))
 
+    def _stored_f(self, b, f):
+        """FP64 (Ni, Nj, Nv, 2) distributions in this solver's storage form."""
+        return f if self.precision == "fp64" else to_pairs(f, b.ref, b.vgrid)
+
+    def full_f(self, b):
+        """Block b's distributions with ghosts as FP64 (Ni, Nj, Nv, 2) numpy."""
+        f = b.f.cpu().numpy()
+        return f if self.precision == "fp64" else from_pairs(f, b.ref, b.vgrid)
+
+    def _full_f_device(self, b):
+        """The same as a CUDA FP64 tensor in the reference layout (for the
+        drop-in diagnostic kernels)."""
+        return b.f if self.precision == "fp64" else self._dev(self.full_f(b))
+
     def save_checkpoint(self, path: str, solve: int = 0, save_f: bool = True):
         """Write one solve's state as a checkpoint (checkpoint.py; the
         reference's saveHDF5 + close_HDF5, ugks_sim.py:1022-1096)."""
@@ -282,8 +407,8 @@ class FusedSolver:
         for k, bi in enumerate(self.solve_blocks[s]):
             b = self.blocks[bi]
             m = b.macro.cpu().numpy()
-            f_full = b.f.cpu().numpy()
-            q = self._heat_flux(b, f_full[b.G:-b.G, b.G:-b.G].astype(np.float64), m)
+            f_full = self.full_f(b)
+            q = self._heat_flux(b, f_full[b.G:-b.G, b.G:-b.G], m)
             blocks.append(checkpoint.block_datasets(
                 k, state["dt"], state["time"], m, checkpoint.external_heat_flux(q, const.K),
                 b.wall_prop.cpu().numpy(), b.wall_cover.cpu().numpy(), b.wall_fluxes.cpu().numpy(),
@@ -300,7 +425,7 @@ class FusedSolver:
         for bi in self.solve_blocks[self.order[solve]]:
             b = self.blocks[bi]
             m = b.macro.cpu().numpy()
-            f = b.f[b.G:-b.G, b.G:-b.G].double().cpu().numpy()
+            f = self.full_f(b)[b.G:-b.G, b.G:-b.G]
             q = self._heat_flux(b, f, m)
             out.append(dict(rho=m[:, :, 0], U=m[:, :, 1], V=m[:, :, 2], T=1.0 / m[:, :, 3],
                             qx=q[:, :, 0], qy=q[:, :, 1]))
@@ -315,9 +440,11 @@ class FusedSolver:
         return np.stack([0.5 * np.sum(cx * t, axis=-1), 0.5 * np.sum(cy * t, axis=-1)], -1)
 
     def interior_f(self, solve: int = 0):
-        return [self.blocks[bi].f[self.blocks[bi].G:-self.blocks[bi].G,
-                                  self.blocks[bi].G:-self.blocks[bi].G].double().cpu().numpy()
-                for bi in self.solve_blocks[self.order[solve]]]
+        out = []
+        for bi in self.solve_blocks[self.order[solve]]:
+            b = self.blocks[bi]
+            out.append(self.full_f(b)[b.G:-b.G, b.G:-b.G])
+        return out
 
     def _program(self, bi):
         from .kernel_program import KernelProgram
@@ -333,7 +460,7 @@ class FusedSolver:
         out = []
         for bi in self.solve_blocks[self.order[solve]]:
             b = self.blocks[bi]
-            out.append(internal_data(self._program(bi), b.f, b.ni, b.nj))
+            out.append(internal_data(self._program(bi), self._full_f_device(b), b.ni, b.nj))
         return out
 
     def interface_distribution(self, solve: int = 0):
@@ -343,8 +470,8 @@ class FusedSolver:
         out = []
         for bi in self.solve_blocks[self.order[solve]]:
             b = self.blocks[bi]
-            out.append(interface_distribution(self._program(bi), b.f, b.centre, b.mid_side, b.normal, b.ni, b.nj,
-                                              b.G))
+            out.append(interface_distribution(self._program(bi), self._full_f_device(b), b.centre, b.mid_side,
+                                              b.normal, b.ni, b.nj, b.G))
         return out
 
     def solve_block_ids(self, solve: int):

@@ -61,6 +61,7 @@ class VelocityGrid:
         v = np.array([q["v_min"] + j * dv for j in jv])
         wu = np.array([newton_weight(i + 1, self.u_num) * du for i in iu])
         wv = np.array([newton_weight(j + 1, self.v_num) * dv for j in jv])
+        self.wu, self.wv = wu, wv      # 1-D weights: weight = wu x wv (before rounding)
         quad = np.empty((self.Nv, 2))
         quad[:, 0] = np.repeat(u, self.v_num)
         quad[:, 1] = np.tile(v, self.u_num)

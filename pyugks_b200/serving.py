@@ -14,10 +14,13 @@ between launches:
 
 ``Server`` runs a request stream against a pool: requests are admitted in
 arrival order while their HBM footprint fits the budget; every tick advances
-the pool by a fixed number of steps; after a tick the reference residual
-(``ugks_block.py:1303-1327``) of every solve is computed on the device and a
-solve leaves when its density residual is below the tolerance or it reached
-its step limit.  Time-to-converged is measured from arrival to retirement.
+the pool by a fixed number of steps, each followed by the reference residual
+(``ugks_block.py:1303-1327``) and the stop rule of every solve on the device,
+so a solve stops at the step its density residual falls below its tolerance
+or it reaches its step limit, and leaves at the end of that tick.
+Time-to-converged is measured from arrival to the end of that tick.
+``serve_one_at_a_time`` is the comparison arm: the same stream, one solve at
+a time, to the same stop rule.
 """
 from __future__ import annotations
 
@@ -59,12 +62,30 @@ class _Solve:
         self.record = None            # latest ugks_solve_state (bytes) while in the pool
 
 
+def _records(raw: bytes, n: int):
+    arr = (_lib.SolveState * n).from_buffer_copy(raw)
+    return [dict(dt=x.dt, time=x.time, steps=x.steps, status=x.status, stopped=x.stopped, active=x.active,
+                 residual=list(x.residual)) for x in arr]
+
+
 class SolvePool:
-    def __init__(self, precision="fp64", device="cuda"):
+    """Admitted solves advanced together, a tick at a time.
+
+    A tick is ``ugks_serve_steps``: per step the fused step, the residual and
+    the stop rule of every solve, decided on the device (ugks_stop_check), so
+    that a solve stops at the step it meets its rule while the others go on.
+    With ``graphs`` the tick is captured once per membership (a CUDA graph of
+    all its launches) and replayed until a solve joins or leaves."""
+
+    def __init__(self, precision="fp64", device="cuda", graphs=True):
         import torch
         self.precision = precision
         self.device = torch.device(device)
         self.lib = _lib.lib()
+        self.mixed = 0 if precision == "fp64" else 1
+        with torch.cuda.device(self.device):
+            _lib.check(self.lib.ugks_prepare(self.mixed), "ugks_prepare")
+        self.graphs = graphs
         self.solves = {}              # id -> _Solve, admission order
         self._next = 0
         self._table = None
@@ -72,12 +93,15 @@ class SolvePool:
         self._sizes = None
         self._order = []
         self._dirty = True
-        self._step_fn = self.lib.ugks_step_fp64 if precision == "fp64" else self.lib.ugks_step_mixed
+        self._graph = None            # (steps per tick, CUDAGraph) of the current membership
 
     # -------------------------------------------------------------- membership
-    def admit(self, case) -> int:
-        """Allocate and initialise a solve; returns its id."""
+    def admit(self, case, tol=0.0, max_steps=0) -> int:
+        """Allocate and initialise a solve with its stop rule (density
+        residual below tol, or max_steps steps; 0 disables either); returns
+        its id."""
         solver = FusedSolver(case, precision=self.precision, device=self.device)
+        solver.set_stop_rule(0, tol, max_steps)
         sid = self._next
         self._next += 1
         s = _Solve(sid, case, solver)
@@ -104,6 +128,7 @@ class SolvePool:
     def _rebuild(self):
         import torch
         self._sync_records()
+        self._graph = None  # its launches name the old table
         # group by limiter (ugks_fused_layout's rule), then by Nv (one face-pass
         # launch per run), then admission order
         order = sorted(self.solves, key=lambda sid: (D.FLUX_METHODS[self.solves[sid].case["flux_method"]],
@@ -140,32 +165,44 @@ class SolvePool:
         self._dirty = False
 
     # -------------------------------------------------------------- stepping
-    def step(self, n=1):
+    def _serve(self, n, stream):
+        _lib.check(self.lib.ugks_serve_steps(self.mixed, self._table.data_ptr(), self._nblocks,
+                                             C.byref(self._sizes), self._states.data_ptr(), len(self._order),
+                                             n, stream), "ugks_serve_steps")
+
+    def tick(self, n=1):
+        """Advance every running solve by up to n steps (asynchronous)."""
         import torch
         if self._dirty:
             self._rebuild()
         if self._table is None:
             return
-        stream = torch.cuda.current_stream(self.device).cuda_stream
-        for _ in range(n):
-            _lib.check(self._step_fn(self._table.data_ptr(), self._nblocks, C.byref(self._sizes),
-                                     self._states.data_ptr(), len(self._order), stream), "ugks_step")
+        if not self.graphs:
+            self._serve(n, torch.cuda.current_stream(self.device).cuda_stream)
+            return
+        if self._graph is None or self._graph[0] != n:
+            g = torch.cuda.CUDAGraph()
+            cap = torch.cuda.Stream(self.device)
+            cap.wait_stream(torch.cuda.current_stream(self.device))
+            with torch.cuda.graph(g, stream=cap):
+                self._serve(n, cap.cuda_stream)
+            torch.cuda.current_stream(self.device).wait_stream(cap)
+            self._graph = (n, g)
+        self._graph[1].replay()
+
+    def step(self, n=1):
+        """Alias of tick (n steps of every running solve)."""
+        self.tick(n)
 
     def states(self, rebuild=True):
-        """{id: solve record dict} with the residual of the last step.  With
-        rebuild=False the solves admitted since the last step are left out
-        (they have not stepped yet)."""
-        import torch
+        """{id: solve record dict} (synchronises).  With rebuild=False the
+        solves admitted since the last tick are left out (they have not
+        stepped yet)."""
         if self._dirty and rebuild:
             self._rebuild()
         if self._table is None:
             return {}
-        _lib.check(self.lib.ugks_residual(self._table.data_ptr(), self._nblocks, self._states.data_ptr(),
-                                          len(self._order), torch.cuda.current_stream(self.device).cuda_stream),
-                   "ugks_residual")
-        arr = (_lib.SolveState * len(self._order)).from_buffer_copy(self._states.cpu().numpy().tobytes())
-        return {sid: dict(dt=x.dt, time=x.time, steps=x.steps, status=x.status, residual=list(x.residual))
-                for sid, x in zip(self._order, arr)}
+        return dict(zip(self._order, _records(self._states.cpu().numpy().tobytes(), len(self._order))))
 
     def fields(self, sid):
         return self.solves[sid].solver.fields(0)
@@ -184,11 +221,18 @@ class Request:
         self.admitted = self.finished = None
         self.steps = 0
         self.reason = None
+        self.units = case_units(case)
+
+
+def case_units(case) -> int:
+    """Cell-velocity points of one step of a solve."""
+    from .configs import workload_size
+    return workload_size(case)
 
 
 class Server:
-    def __init__(self, budget_bytes=150e9, precision="mixed", steps_per_tick=50, device="cuda"):
-        self.pool = SolvePool(precision, device)
+    def __init__(self, budget_bytes=150e9, precision="mixed", steps_per_tick=50, device="cuda", graphs=True):
+        self.pool = SolvePool(precision, device, graphs=graphs)
         self.budget = budget_bytes
         self.precision = precision
         self.steps_per_tick = steps_per_tick
@@ -202,7 +246,10 @@ class Server:
 
         A tick's steps are launched first; requests that arrived meanwhile are
         then set up (allocation, geometry, initialisation) on a side stream
-        while the tick runs, and join the table at the next tick."""
+        while the tick runs, and join the table at the next tick.  A solve
+        stops on the device at the step that meets its rule (residual below
+        its tolerance, its step limit, or an error status) and leaves at the
+        end of that tick."""
         import torch
         dev = self.pool.device
         main = torch.cuda.current_stream(dev)
@@ -230,47 +277,88 @@ class Server:
                     break
                 waiting.pop(0)
                 with torch.cuda.stream(side):
-                    sid = self.pool.admit(r.case)
+                    sid = self.pool.admit(r.case, r.tol, r.max_steps)
                 r.admitted, r.need, r.sid = time.perf_counter() - t0, need, sid
                 self.used += need
                 active[sid] = r
 
-        while i < len(queue) or waiting or active:
-            now = arrivals()
-            if time_limit is not None and now > time_limit:
-                break
-            admit()
+        try:
+            while i < len(queue) or waiting or active:
+                now = arrivals()
+                if time_limit is not None and now > time_limit:
+                    break
+                admit()
+                main.wait_stream(side)
+                if not active:
+                    if i < len(queue):
+                        time.sleep(max(0.0, min(queue[i].arrival - now, 0.05)))
+                    continue
+                self.pool.tick(self.steps_per_tick)
+                arrivals()
+                admit()                                      # overlaps the tick
+                # the host sync here is also what makes retiring safe: every
+                # kernel that reads a retired solve's arrays has finished
+                states = self.pool.states(rebuild=False)
+                main.wait_stream(side)
+                now = time.perf_counter() - t0
+                for sid, st in states.items():
+                    r = active[sid]
+                    self.units += (st["steps"] - r.steps) * r.units
+                    r.steps = st["steps"]
+                    if st["stopped"]:
+                        r.finished, r.reason = now, _lib.STOP_REASONS[st["stopped"]]
+                        self.pool.retire(sid)
+                        self.used -= r.need
+                        del active[sid]
+                        self.done.append(r)
+        finally:
             main.wait_stream(side)
-            if not active:
-                if i < len(queue):
-                    time.sleep(max(0.0, min(queue[i].arrival - now, 0.05)))
-                continue
-            units = self.pool.units_per_step()
-            self.pool.step(self.steps_per_tick)
-            self.units += units * self.steps_per_tick
-            arrivals()
-            admit()                                      # overlaps the tick
-            states = self.pool.states(rebuild=False)     # synchronises
-            main.wait_stream(side)
-            now = time.perf_counter() - t0
-            for sid, st in states.items():
-                r = active[sid]
-                r.steps = st["steps"]
-                reason = None
-                if st["status"] != 0:
-                    reason = "error"
-                elif st["residual"][0] < r.tol:
-                    reason = "converged"
-                elif st["steps"] >= r.max_steps:
-                    reason = "max_steps"
-                if reason:
-                    r.finished, r.reason = now, reason
-                    self.pool.retire(sid)
-                    self.used -= r.need
-                    del active[sid]
-                    self.done.append(r)
         self.wall = time.perf_counter() - t0
         return self.done
+
+
+def serve_one_at_a_time(requests, precision="fp64", steps_per_tick=50, device="cuda"):
+    """The comparison arm: the same requests served first come, first served,
+    one solve at a time on the fused step, each to the same stop rule.  A
+    request's service time is its solve's stepping time on the device (CUDA
+    events; set-up excluded); its completion is max(arrival, previous
+    completion) + service, as for a single server working the queue in
+    order.  Returns a dict with per-request latencies and the aggregate
+    cell-velocity updates per second of service."""
+    import torch
+    dev = torch.device(device)
+    lib = _lib.lib()
+    mixed = 0 if precision == "fp64" else 1
+    with torch.cuda.device(dev):
+        _lib.check(lib.ugks_prepare(mixed), "ugks_prepare")
+    clock, units, busy = 0.0, 0, 0.0
+    lat, reasons, steps = [], [], []
+    stream = torch.cuda.current_stream(dev)
+    for r in sorted(requests, key=lambda q: q.arrival):
+        solver = FusedSolver([r.case], precision=precision, device=dev)
+        solver.set_stop_rule(0, r.tol, r.max_steps)
+        torch.cuda.synchronize(dev)
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        while True:
+            _lib.check(lib.ugks_serve_steps(mixed, solver.table.data_ptr(), solver.nblocks, C.byref(solver.sizes),
+                                            solver.solves.data_ptr(), 1, steps_per_tick, stream.cuda_stream),
+                       "ugks_serve_steps")
+            st = solver.solve_state()[0]  # synchronises
+            if st["stopped"]:
+                break
+        t1.record(stream)
+        torch.cuda.synchronize(dev)
+        service = t0.elapsed_time(t1) / 1e3
+        clock = max(clock, r.arrival) + service
+        busy += service
+        lat.append(clock - r.arrival)
+        reasons.append(_lib.STOP_REASONS[st["stopped"]])
+        steps.append(st["steps"])
+        units += st["steps"] * r.units
+        del solver
+    return dict(latency=lat, reasons=reasons, steps=steps, units=units, service_s=busy,
+                value=units / busy if busy > 0 else 0.0, makespan_s=clock)
 
 
 def request_stream(seed=2, rate=20.0, duration=600.0, max_steps=20000, tol=1e-6):

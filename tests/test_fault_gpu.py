@@ -64,11 +64,11 @@ def test_serving_retires_a_failed_request(cuda):
     reqs = [Request(k, 0.0, configs.cavity(n=8, m=8, vlim=4.0, lid=0.1 + 0.05 * k), 60, 0.0) for k in range(3)]
     server = Server(precision="mixed", steps_per_tick=5)
     pool = server.pool
-    orig_step = pool.step
+    orig_tick = pool.tick
     planted = []
 
-    def step_and_fault(n):
-        orig_step(n)
+    def tick_and_fault(n):
+        orig_tick(n)
         if not planted and len(pool.solves) == 3:
             # request 1's solve: its one block, through a host copy
             sid = sorted(pool.solves)[1]
@@ -76,7 +76,7 @@ def test_serving_retires_a_failed_request(cuda):
             _plant_nan(blk.f, blk.G)
             planted.append(sid)
 
-    pool.step = step_and_fault
+    pool.tick = tick_and_fault
     done = server.run(reqs)
     reasons = {r.id: r.reason for r in done}
     assert reasons == {0: "max_steps", 1: "error", 2: "max_steps"}, reasons

@@ -48,3 +48,61 @@ def test_server_completes_a_small_stream(cuda):
     assert all(r.reason in ("converged", "max_steps") for r in done)
     lat = sorted(r.finished - r.arrival for r in done)
     assert lat[0] > 0 and np.percentile(lat, 99) >= np.percentile(lat, 50)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_graph_ticks_match_eager_ticks(cuda, precision):
+    """A tick replayed from a CUDA graph gives the same bits as the same
+    launches made one by one."""
+    cases = [configs.cavity(n=8, m=8, vlim=4.0, flux_method="WENO5"), configs.channel(nblocks=2, n=8, m=8)]
+    pools = [SolvePool(precision, graphs=g) for g in (True, False)]
+    ids = [[p.admit(c) for c in cases] for p in pools]
+    for p in pools:
+        p.tick(5)
+        p.tick(5)
+    for k in range(len(cases)):
+        for x, y in zip(pools[0].interior_f(ids[0][k]), pools[1].interior_f(ids[1][k])):
+            np.testing.assert_array_equal(x, y)
+
+
+def test_fused_solver_capture_matches_step(cuda):
+    case = configs.cavity_multiblock(nb=2, n=8, m=8)
+    a, b = FusedSolver(case), FusedSolver(case)
+    a.capture(6)
+    a.replay()
+    a.replay()
+    b.step(12)
+    assert a.solve_state()[0]["steps"] == 12
+    for x, y in zip(a.interior_f(), b.interior_f()):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_device_stop_rule(cuda):
+    """A solve stops on the device at the step it meets its rule; the others
+    in the table go on, unperturbed."""
+    pool = SolvePool("fp64")
+    capped = pool.admit(configs.cavity(n=8, m=8, vlim=4.0), max_steps=7)
+    loose = pool.admit(configs.cavity(n=10, m=8, vlim=4.0), tol=1e-1)
+    free = pool.admit(configs.cavity(n=8, m=12, vlim=5.0, flux_method="WENO5"))
+    pool.tick(5)
+    pool.tick(5)
+    st = pool.states()
+    assert st[capped]["steps"] == 7 and st[capped]["stopped"] == 2 and not st[capped]["active"]
+    assert st[loose]["stopped"] == 1 and st[loose]["residual"][0] < 1e-1 and st[loose]["steps"] < 10
+    assert st[free]["steps"] == 10 and st[free]["stopped"] == 0
+    for x, y in zip(pool.interior_f(free), solo(configs.cavity(n=8, m=12, vlim=5.0, flux_method="WENO5"), 10)):
+        np.testing.assert_array_equal(x, y)
+
+
+def test_one_at_a_time_arm_same_stop_rule(cuda):
+    """The comparison arm serves the same requests to the same stop rule: in
+    the same precision each request ends at the same step as in the batch."""
+    from pyugks_b200.serving import serve_one_at_a_time
+    make = lambda: [Request(k, 0.0, configs.cavity(n=8 + 2 * k, m=8, vlim=4.0, lid=0.1 + 0.05 * k),
+                            max_steps=40, tol=2e-3) for k in range(3)]
+    server = Server(precision="mixed", steps_per_tick=10)
+    done = {r.id: r for r in server.run(make())}
+    arm = serve_one_at_a_time(make(), precision="mixed", steps_per_tick=10)
+    assert [done[k].steps for k in range(3)] == arm["steps"]
+    assert [done[k].reason for k in range(3)] == arm["reasons"]
+    assert all(x > 0 for x in arm["latency"]) and arm["value"] > 0
