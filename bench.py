@@ -54,17 +54,18 @@ BYTES_PER_UPDATE = {"fp64": 32, "mixed": 16}  # read + write of (h, b) per cell-
 
 def workload(name: str):
     if name == "multiblock":
-        case = configs.cavity_multiblock(nb=2, n=64, m=32, vlim=5.0, flux_method="WENO5", Kn=0.01)
+        case = configs.cavity_multiblock(nb=2, n=64, m=32, vlim=5.0, flux_method="WENO5", Kn=0.01,
+                                         CFL=configs.WORKLOAD_CFL)
         desc = ("lid-driven cavity 128x128 as 2x2 blocks of 64x64 cells, 33x33 velocities on "
-                "[-5,5]^2 (Nv=1089), WENO5, Kn 0.01, CFL 0.3")
+                "[-5,5]^2 (Nv=1089), WENO5, Kn 0.01, CFL 0.2")
         return [case], desc
     if name == "cavity":
         case = configs.cavity(n=32, m=24, vlim=4.0)
         return [case], "lid-driven cavity 32x32, 25x25 velocities on [-4,4]^2 (Nv=625), vanLeer, Kn 0.075"
     if name == "channel":
-        case = configs.channel(nblocks=4, n=64, m=32, Kn=0.05)
+        case = configs.channel(nblocks=4, n=64, m=32, Kn=0.05, CFL=configs.WORKLOAD_CFL)
         return [case], ("adsorbing channel 256x64 in 4 blocks, 33x33 velocities on [-5,5]^2, WENO5, "
-                        "Kn 0.05, inlet rho 1.2 / outlet rho 1.0")
+                        "Kn 0.05, inlet rho 1.2 / outlet rho 1.0, CFL 0.2")
     if name == "batched":
         cases = configs.batched_cavities(64, seed=1)
         return cases, "64 independent cavities, n in {24..128}, m in {16..48}, seed 1"

@@ -275,6 +275,10 @@ int ugks_adsorbingWallCL_P2(const ugks_block_desc *d, size_t g0, size_t g1, cons
 #define UGKS_REF_KB0 2
 #define UGKS_REF_MOM 4
 #define UGKS_REF_TAB 32
+/* doubles per face of ugks_fused_block.face_rec (the mixed face pass's
+ * per-face record: the deviation's moments, the flux coefficients and the
+ * face state, handed from one launch of the pass to the next) */
+#define UGKS_FACE_REC 48
 typedef struct ugks_fused_block {
   ugks_block_desc d;           /* sizes, constants, tables, wall values    */
   int32_t solve;               /* index of the owning ugks_solve_state     */
@@ -320,6 +324,10 @@ typedef struct ugks_fused_block {
   const double *ref;           /* *_mixed only: the solve's reference Maxwellian
                                   (UGKS_REF_* layout above), the same array for
                                   every block of the solve; unused by *_fp64 */
+  void *aux_S;                 /* *_mixed only: scratch of the face pass, shaped like
+                                  flux_S: the slopes of the SOUTH-face deviations */
+  void *aux_W;                 /* *_mixed only: the same for the WEST faces */
+  double *face_rec;            /* *_mixed only: [Ni][Nj][2] x UGKS_FACE_REC scratch */
 } ugks_fused_block;
 
 typedef struct ugks_solve_state {

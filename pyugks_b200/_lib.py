@@ -48,6 +48,7 @@ class FusedBlock(C.Structure):
         ("area", vp), ("centre", vp), ("mid_side", vp), ("normal", vp), ("side_length", vp),
         ("xy", vp), ("wall_prop", vp), ("wall_cover", vp), ("wall_fluxes", vp), ("wall_dist", vp),
         ("cell_mom", vp), ("Q_next", vp), ("face_geo", vp), ("ref", vp),
+        ("aux_S", vp), ("aux_W", vp), ("face_rec", vp),
     ]
 
 
@@ -99,6 +100,7 @@ _CT = {"p": vp, "i": C.c_int, "d": f64}
 
 # layout of the mixed path's reference Maxwellian (UGKS_REF_*, include/ugks_b200.h)
 REF_LAMBDA, REF_P0, REF_KB0, REF_MOM, REF_TAB = 0, 1, 2, 4, 32
+FACE_REC = 48       # UGKS_FACE_REC
 
 # ugks_getDT_noalloc limits and error codes (include/ugks_b200.h)
 NOALLOC_MAX_CELLS = 1 << 20

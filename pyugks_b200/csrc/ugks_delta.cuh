@@ -175,17 +175,55 @@ __device__ __forceinline__ float2 slope_pair(const float2 (&S)[FM == 1 ? 5 : 3],
 }
 
 // ---------------------------------------------------------------------------
-// face pass
+// face pass, in three launches
 // ---------------------------------------------------------------------------
-// shared memory of a mixed face CTA: per velocity pair the face deviations,
-// slopes and face-frame velocities (3 float4), then per velocity-axis node
-// (a, Au) / (b, Av) and the axis velocities; a wall face reuses the pair
-// arrays as Nv (h, b) FP64 face values plus Nv float2 of scratch
+// The per-face scalar work (face state, heat flux, half-range moments, slopes,
+// time weights: a chain of FP64 transcendentals) would otherwise run on one or
+// two lanes of every face CTA while the rest of the CTA waits.  Here it runs
+// one face per thread:
+//   1. face_item_delta (moments; a CTA per face): the reconstruction of every
+//      velocity pair, stored as the face deviation in the face's flux row and
+//      the slopes in its aux row, and the 13 raw moments of the deviation
+//      into the face record; a wall face runs its whole wall procedure here;
+//   2. face_coef_delta (a thread per face): the face state and every per-face
+//      coefficient of the flux into the face record;
+//   3. face_flux_delta (a CTA per face): the deviation flux of every velocity
+//      pair over the stored face deviations, written over them, and the
+//      macro flux.
+// Interior faces take the dt after the first dt check, which is the dt of
+// the reference's final flux pass (its first pass is overwritten when dt
+// changes); wall faces run the reference's two passes, for the side effects
+// of adsorbing walls.
+
+// layout of a face record (ugks_fused_block.face_rec, UGKS_FACE_REC doubles
+// per face): [0, 13) the raw moments of the face deviation (face frame);
+// [16, 38) the coefficients of face_coefficients (c[0..21]); then
+constexpr int FR_MOM = 0, FR_C = 16, FR_UX = 38, FR_UY = 39, FR_LAM = 40, FR_KB = 41, FR_SX = 42, FR_SY = 43,
+              FR_LNP = 44, FR_UGX = 45, FR_UGY = 46;
+static_assert(FR_UGY < UGKS_FACE_REC, "face record layout");
+
+// shared memory of a moments CTA: the axis velocities, and for a wall face Nv
+// (h, b) FP64 face values plus Nv float2 of scratch
 inline size_t delta_face_smem(int max_nv, int max_axes) {
-  // pairs: at most max_nv / 2 + v_num <= max_nv / 2 + max_axes
-  return 48 * ((size_t)(max_nv + 1) / 2 + (size_t)max_axes) + 12 * (size_t)(max_axes + 2) + 16;
+  return 24 * (size_t)max_nv + 4 * (size_t)(max_axes + 2) + 16;
+}
+// threads of a flux CTA
+constexpr int FLUX_NT = 128;
+// shared memory of a flux CTA: per velocity-axis node (a, len Au) / (b, Av)
+// and the axis velocities
+inline size_t delta_flux_smem(int max_axes) { return 12 * (size_t)(max_axes + 2) + 16; }
+
+// axis velocities of the tensor grid (entry u_num: the padding lane, 0)
+__device__ __forceinline__ void axis_velocities(const ugks_block_desc &d, float *QX, float *QY, int t, int nt) {
+  const int un = d.u_num, vn = d.v_num;
+  for (int k = t; k <= un + vn; k += nt) {
+    if (k < un) QX[k] = (float)d.quad[2 * (size_t)k * vn];
+    else if (k == un) QX[k] = 0.0f;
+    else QY[k - un - 1] = (float)d.quad[2 * (size_t)(k - un - 1) + 1];
+  }
 }
 
+// 1. moments (a CTA per face; in the retry pass, wall faces only)
 template <int FM, int NT>
 __device__ __forceinline__ void face_item_delta(const ugks_fused_block *__restrict__ B, int nb,
                                                 ugks_solve_state *__restrict__ solves, const int w, int retry_pass) {
@@ -193,16 +231,16 @@ __device__ __forceinline__ void face_item_delta(const ugks_fused_block *__restri
   __shared__ FaceShared<NT> sh;
   FaceWork fwk;
   if (!face_work<FM>(B, nb, solves, w, retry_pass, fwk)) return;
+  if (retry_pass && fwk.wall < 0) return;  // interior faces do not depend on dt here
   const ugks_fused_block &blk = B[fwk.bi];
   const ugks_block_desc &d = blk.d;
   ugks_solve_state &sol = solves[blk.solve];
   const double dt = sol.dt;
   const int dir = fwk.dir, mi = fwk.mi, mj = fwk.mj, wall = fwk.wall;
   const long gi = fwk.gi, gj = fwk.gj;
-  const int Nv = d.Nv, NP = npairs(d), un = d.u_num, vn = d.v_num;
+  const int Nv = d.Nv, NP = npairs(d), vn = d.v_num;
   const RefMaxwellian ref = ref_of(blk);
   const V2 n = ld2(blk.normal, faceidx(d, gi, gj, dir));
-  const V2 mid = ld2(blk.mid_side, faceidx(d, gi, gj, dir));
   const double len = blk.side_length[faceidx(d, gi, gj, dir)];
   double g6[6];
   {
@@ -213,6 +251,7 @@ __device__ __forceinline__ void face_item_delta(const ugks_fused_block *__restri
   const float dist0 = (float)g6[0], idist0 = (float)g6[1], il0 = (float)g6[2];
   const float dist1 = (float)g6[3], idist1 = (float)g6[4], il1 = (float)g6[5];
   constexpr int L = FM == 1 ? 5 : 3, MID = FM == 1 ? 2 : 1;
+  float4 *frow = reinterpret_cast<float4 *>(dir == SOUTH ? blk.flux_S : blk.flux_W) + pidx(d, gi, gj, 0);
 
   if (wall >= 0) {
     // ---------------- wall face: the FP64 wall procedure on M + df --------
@@ -236,7 +275,6 @@ __device__ __forceinline__ void face_item_delta(const ugks_fused_block *__restri
       fw[2 * v] = m + (double)fh;
       fw[2 * v + 1] = ref.kb0 * m + (double)fb;
     }
-    float4 *frow = reinterpret_cast<float4 *>(dir == SOUTH ? blk.flux_S : blk.flux_W) + pidx(d, gi, gj, 0);
     const double dl = dt * len;
     wall_face<NT>(blk, sol, sh, fw, rin, wall, dir, gi, gj, mi, mj, n, len, dt, [&](int v, double hx, double hy) {
       const double2 e = qd[v];
@@ -246,34 +284,15 @@ __device__ __forceinline__ void face_item_delta(const ugks_fused_block *__restri
     return;
   }
 
-  // ---------------- interior face ----------------
-  float4 *FHB = reinterpret_cast<float4 *>(dyn), *SGB = FHB + NP, *UVF = SGB + NP;
-  float2 *EAU = reinterpret_cast<float2 *>(UVF + NP), *EAV = EAU + (un + 1);  // (expm1 table, axis factor)
-  float *QX = reinterpret_cast<float *>(EAV + vn), *QY = QX + (un + 1);
-  const float4 *EAU2 = reinterpret_cast<const float4 *>(EAU);  // the two u-nodes of a pair row
+  // ---------------- interior face: reconstruction and moments -------------
+  float *QX = reinterpret_cast<float *>(dyn), *QY = QX + (d.u_num + 1);
   const float2 *QX2 = reinterpret_cast<const float2 *>(QX);
-  // per-solve axis tables (velocity nodes and reference factors); the entry
-  // un is the padding velocity's: 0, so that its reference value is 0
-  for (int k = threadIdx.x; k <= un + vn; k += NT) {
-    if (k < un) {
-      QX[k] = (float)d.quad[2 * (size_t)k * vn];
-      EAU[k].y = (float)(ref.Au[k] * len);  // the face length rides on the u-axis factor
-    } else if (k == un) {
-      QX[k] = 0.0f;
-      EAU[k] = make_float2(0.0f, 0.0f);
-    } else {
-      const int j = k - un - 1;
-      QY[j] = (float)d.quad[2 * (size_t)j + 1];
-      EAV[j].y = (float)ref.Av[j];
-    }
-  }
+  axis_velocities(d, QX, QY, threadIdx.x, NT);
   __syncthreads();
-
-  // ---- sweep 1: reconstruction of the deviations, their raw moments (face
-  // frame; the heat flux follows from them, so no separate sweep)
   const int pstep = (dir == SOUTH ? 1 : d.Nj) * NP;  // pairs between neighbouring cells along the normal
   const float4 *fcell = reinterpret_cast<const float4 *>(blk.f) + pidx(d, gi, gj, 0);
   const float4 *up1 = fcell - (MID + 1) * pstep, *up0 = fcell + MID * pstep;
+  float4 *arow = reinterpret_cast<float4 *>(dir == SOUTH ? blk.aux_S : blk.aux_W) + pidx(d, gi, gj, 0);
   const float2 nx2 = bc2((float)n.x), ny2 = bc2((float)n.y), mny2 = bc2(-(float)n.y);
   float2 mom[RNMOM];
 #pragma unroll
@@ -312,10 +331,9 @@ __device__ __forceinline__ void face_item_delta(const ugks_fused_block *__restri
     const float2 ids = make_float2(ua ? idist1 : idist0, ub ? idist1 : idist0);
     const float2 sh2 = slope_pair<FM>(Sh, il, ids), sb2 = slope_pair<FM>(Sb, il, ids);
     const float2 fh = fma2(sh2, ds, Sh[MID]), fb = fma2(sb2, ds, Sb[MID]);
-    FHB[p] = cat2(fh, fb);
-    SGB[p] = cat2(sh2, sb2);
-    UVF[p] = cat2(U, T);
-    // raw moments of the face deviation
+    frow[p] = cat2(fh, fb);
+    arow[p] = cat2(sh2, sb2);
+    // raw moments of the face deviation (face frame)
     const float2 t1 = mul2(U, fh), t2 = mul2(T, fh), uu = mul2(U, U), tt = mul2(T, T);
     mom[RM00] = add2(mom[RM00], fh);
     mom[RM10] = add2(mom[RM10], t1);
@@ -334,12 +352,47 @@ __device__ __forceinline__ void face_item_delta(const ugks_fused_block *__restri
     ia += qs;
     if (jv >= vn) { jv -= vn; ++ia; }
   }
-  face_neighbours<NT>(blk, sh, gi, gj, dir, n, mid);
+  // the per-thread FP32 sums, added in FP64 across the CTA
+  double mf[RNMOM];
+#pragma unroll
+  for (int k = 0; k < RNMOM; ++k) {
+    mf[k] = (double)mom[k].x + (double)mom[k].y;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) mf[k] += __shfl_xor_sync(0xffffffffu, mf[k], o);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < RNMOM; ++k) sh.scratch[k * (NT / 32) + warp] = mf[k];
+  __syncthreads();
+  if (threadIdx.x < RNMOM) {
+    double t = 0.0;
+    for (int q = 0; q < NT / 32; ++q) t += sh.scratch[threadIdx.x * (NT / 32) + q];
+    blk.face_rec[(size_t)UGKS_FACE_REC * faceidx(d, gi, gj, dir) + FR_MOM + threadIdx.x] = t;
+  }
+}
+
+// 2. coefficients: the per-face block of face_coefficients, one face per
+// thread (the same chain as the lanes of a face CTA run there)
+__global__ void __launch_bounds__(128) face_coef_delta(const ugks_fused_block *__restrict__ B, int nb,
+                                                       ugks_solve_state *__restrict__ solves, int n_faces) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= n_faces) return;
+  FaceWork fwk;
+  if (!face_work<-1>(B, nb, solves, w, 0, fwk) || fwk.wall >= 0) return;
+  const ugks_fused_block &blk = B[fwk.bi];
+  const ugks_block_desc &d = blk.d;
+  const double dt = solves[blk.solve].dt;
+  const int dir = fwk.dir;
+  const long gi = fwk.gi, gj = fwk.gj;
+  const RefMaxwellian ref = ref_of(blk);
+  const size_t fk = faceidx(d, gi, gj, dir);
+  double *rec = blk.face_rec + (size_t)UGKS_FACE_REC * fk;
+  const V2 n = ld2(blk.normal, fk), mid = ld2(blk.mid_side, fk);
+  const double len = blk.side_length[fk];
   double dm[RNMOM];
 #pragma unroll
-  for (int k = 0; k < RNMOM; ++k) dm[k] = (double)mom[k].x + (double)mom[k].y;
-  block_sum<RNMOM>(dm, sh.scratch);
-
+  for (int k = 0; k < RNMOM; ++k) dm[k] = rec[FR_MOM + k];
   // face state: the reference's moments in the face frame plus the deviation's
   const double *R = ref.mom;
   const V2 rU = to_local(v2(R[RM10], R[RM01]), n);
@@ -349,42 +402,140 @@ __device__ __forceinline__ void face_item_delta(const ugks_fused_block *__restri
   const P4 prim = to_primary_rcp(d, W, rc);
   const V2 Ug = to_global(v2(prim.s1, prim.s2), n);
   // face heat flux (calcFaceQ, clUGKS.c:522-585): M's part from its global
-  // moments, rotated into the face frame, and the deviation's from its raw
-  // face-frame moments
+  // moments rotated into the face frame, the deviation's from its raw moments
   V2 Q = to_local(heat_flux_from_moments(R, d.K, Ug), n);
   {
     const V2 qd_ = heat_flux_from_moments(dm, d.K, v2(prim.s1, prim.s2));
     Q.x += qd_.x;
     Q.y += qd_.y;
   }
-  const double lnP = log((prim.s0 * prim.s3) / (ref.P0 * d.PI));  // ln(P / P0), P = rho lambda / pi
-  face_coefficients<NT>(d, sh, W, prim, rc, len, dt, [&](int t, int nt) {
-    // expm1 axis tables of the face Maxwellian against M
-    for (int k = t; k < un + vn; k += nt) {
-      if (k < un) EAU[k].x = (float)axis_expm1(d.quad[2 * (size_t)k * vn], Ug.x, prim.s3, ref.lam0, lnP);
-      else EAV[k - un].x = (float)axis_expm1(d.quad[2 * (size_t)(k - un) + 1], Ug.y, prim.s3, ref.lam0);
-    }
-  });
-  __syncthreads();
-
-  // ---- sweep 3: the deviation flux (the FP64 sweep's terms, see
-  // face_item_fp64, with f = M + df):
-  //   dflux_h = u Mt0 len M r + Zh + u h0 (B - Mt0),
-  //   dflux_b = u Mt0 len M ((kb - kb0) + kb r) + Zb + u h0 (kb (B - Mt0) + Mt1 u a3 X/2 + Mt2 aT3 X/2),
-  //   Zh = u (S P4 h0 + Mt3 len dfh - Mt4 len u sh), Zb likewise,
-  //   h0 = len M (1 + r), r = g / M - 1,
-  // and the discrete macro flux is Mt3 len sum(u M (1, u, v, |u|^2; kb0)) (the
-  // reference's moments) plus the sums of the deviation Z terms
-  const double *c = sh.bcast;
-  const double lam = prim.s3, Ux = prim.s1, Uy = prim.s2;
+  // the two cells beside the face (getAL / getAR inputs, getPLR slopes)
+  double nbr[2][5];
+  for (int side = 0; side < 2; ++side) {
+    const size_t k = side == 0 ? gidx(d, gi - dir, gj - (1 - dir)) : gidx(d, gi, gj);
+    const P4 mc = ld4(blk.cell_mom, k);
+    const V2 uc = to_local(v2(mc.s1, mc.s2), n);
+    const V2 cc = ld2(blk.centre, k);
+    nbr[side][0] = mc.s0;
+    nbr[side][1] = uc.x;
+    nbr[side][2] = uc.y;
+    nbr[side][3] = mc.s3;
+    nbr[side][4] = nr_rcp(sqrt((mid.x - cc.x) * (mid.x - cc.x) + (mid.y - cc.y) * (mid.y - cc.y)));
+  }
+  // getPLR slopes (clUGKS.c:424-436) and initMacroFlux (446-518)
   const double kb = (0.5 * d.K) * rc.lam;
-  const double s0 = 0.8 * (1 - d.Pr) * (lam * lam) * rc.rho;
-  const double Mt0 = c[15], Mt3L = c[16], Mt4L = c[17];
-  const float2 fUx = bc2((float)Ux), fUy = bc2((float)Uy), flam2 = bc2((float)(2.0 * lam));
-  const float2 fsx = bc2((float)((Mt0 * s0) * Q.x)), fsy = bc2((float)((Mt0 * s0) * Q.y));
-  const float2 fkb = bc2((float)kb), fdkb = bc2((float)(kb - ref.kb0));
-  const float2 fMt0 = bc2((float)Mt0);
-  const float2 fMt3L = bc2((float)Mt3L), fnMt4L = bc2((float)(-Mt4L));
+  double Mh[2][MNUM], Mv[MTUM], Mxi[3];
+  P4 a[2], t1[2], t2[2];
+  for (int side = 0; side < 2; ++side) {
+    const double sg = side == 0 ? 1.0 : -1.0;
+    half_moments_rcp(d.PI, d.K, prim, rc, sg, Mh[side], Mv, Mxi);
+    const double id = sg * nbr[side][4];
+    a[side] = micro_slope_rcp(d.K, prim, rc,
+                              p4((W.s0 - nbr[side][0]) * id, (W.s1 - nbr[side][1]) * id,
+                                 (W.s2 - nbr[side][2]) * id, (W.s3 - nbr[side][3]) * id));
+    t1[side] = moment_au(a[side], Mh[side], Mv, Mxi, 1, 0);
+    t2[side] = moment_au(a[side], Mh[side], Mv, Mxi, 2, 0);
+  }
+  double Mt[5];
+  time_weights_rcp(inv_relax_time_rcp(d, prim, rc), dt, Mt);
+  double *c = rec + FR_C;
+  const double xk = Mxi[2] - kb * kb;
+  for (int side = 0; side < 2; ++side) {
+    double *ck = c + 5 * side;
+    ck[0] = Mt[1] * fma(0.5 * a[side].s3, kb, a[side].s0);
+    ck[1] = Mt[1] * a[side].s1;
+    ck[2] = Mt[1] * a[side].s2;
+    ck[3] = Mt[1] * (0.5 * a[side].s3);
+    ck[4] = Mt[1] * (0.5 * a[side].s3 * xk);
+  }
+  double Mu[MNUM];
+#pragma unroll
+  for (int k = 0; k < MNUM; ++k) Mu[k] = Mh[0][k] + Mh[1][k];
+  const P4 aT = micro_slope_rcp(d.K, prim, rc, scale(-prim.s0, add(t1[0], t1[1])));
+  const P4 g0 = scale(prim.s0, add(add(scale(Mt[0], moment_uv(Mu, Mv, Mxi, 1, 0, 0)), scale(Mt[1], add(t2[0], t2[1]))),
+                                   scale(Mt[2], moment_au(aT, Mu, Mv, Mxi, 1, 0))));
+  c[10] = Mt[2] * fma(0.5 * aT.s3, kb, aT.s0) + Mt[0];
+  c[11] = Mt[2] * aT.s1;
+  c[12] = Mt[2] * aT.s2;
+  c[13] = Mt[2] * (0.5 * aT.s3);
+  c[14] = Mt[2] * (0.5 * aT.s3 * xk);
+  c[15] = Mt[0];
+  c[16] = Mt[3] * len;
+  c[17] = Mt[4] * len;
+  c[18] = len * g0.s0; c[19] = len * g0.s1; c[20] = len * g0.s2; c[21] = len * g0.s3;
+  const double s0 = 0.8 * (1 - d.Pr) * (prim.s3 * prim.s3) * rc.rho;
+  rec[FR_UX] = prim.s1;
+  rec[FR_UY] = prim.s2;
+  rec[FR_LAM] = prim.s3;
+  rec[FR_KB] = kb;
+  rec[FR_SX] = (Mt[0] * s0) * Q.x;
+  rec[FR_SY] = (Mt[0] * s0) * Q.y;
+  rec[FR_LNP] = log((prim.s0 * prim.s3) / (ref.P0 * d.PI));  // ln(P / P0), P = rho lambda / pi
+  rec[FR_UGX] = Ug.x;
+  rec[FR_UGY] = Ug.y;
+}
+
+// 3. flux (a CTA per face): the FP64 sweep's terms (see face_item_fp64) with
+// f = M + df:
+//   dflux_h = u Mt0 len M r + Zh + u h0 (B - Mt0),
+//   dflux_b = u Mt0 len M ((kb - kb0) + kb r) + Zb + u h0 (kb (B - Mt0) + Mt1 u a3 X/2 + Mt2 aT3 X/2),
+//   Zh = u (S P4 h0 + Mt3 len dfh - Mt4 len u sh), Zb likewise,
+//   h0 = len M (1 + r), r = g / M - 1,
+// and the discrete macro flux is Mt3 len sum(u M (1, u, v, |u|^2; kb0)) (the
+// reference's moments) plus the sums of the deviation Z terms
+template <int NT>
+__global__ void __launch_bounds__(NT, 5) face_flux_delta(const ugks_fused_block *__restrict__ B, int nb,
+                                                         ugks_solve_state *__restrict__ solves, int first) {
+  extern __shared__ double dyn[];
+  __shared__ double scratch[8 * (NT / 32)];
+  __shared__ double fc[48];
+  FaceWork fwk;
+  if (!face_work<-1>(B, nb, solves, first + (int)blockIdx.x, 0, fwk) || fwk.wall >= 0) return;
+  const ugks_fused_block &blk = B[fwk.bi];
+  const ugks_block_desc &d = blk.d;
+  const int dir = fwk.dir;
+  const long gi = fwk.gi, gj = fwk.gj;
+  const int NP = npairs(d), un = d.u_num, vn = d.v_num;
+  const RefMaxwellian ref = ref_of(blk);
+  const size_t fk = faceidx(d, gi, gj, dir);
+  const double *rec = blk.face_rec + (size_t)UGKS_FACE_REC * fk;
+  const V2 n = ld2(blk.normal, fk);
+  const double len = blk.side_length[fk];
+  float2 *EAU = reinterpret_cast<float2 *>(dyn), *EAV = EAU + (un + 1);  // (expm1 table, axis factor)
+  float *QX = reinterpret_cast<float *>(EAV + vn), *QY = QX + (un + 1);
+  const float4 *EAU2 = reinterpret_cast<const float4 *>(EAU);  // the two u-nodes of a pair row
+  const float2 *QX2 = reinterpret_cast<const float2 *>(QX);
+  if (threadIdx.x < 48) fc[threadIdx.x] = rec[threadIdx.x];
+  __syncthreads();
+  {
+    // expm1 axis tables of the face Maxwellian against M, its axis factors
+    // (the face length on the u axis) and the axis velocities; entry un is
+    // the padding lane's: 0
+    const double lam = fc[FR_LAM], Ugx = fc[FR_UGX], Ugy = fc[FR_UGY], lnP = fc[FR_LNP];
+    for (int k = threadIdx.x; k <= un + vn; k += NT) {
+      if (k < un) {
+        const double x = d.quad[2 * (size_t)k * vn];
+        EAU[k] = make_float2((float)axis_expm1(x, Ugx, lam, ref.lam0, lnP), (float)(ref.Au[k] * len));
+        QX[k] = (float)x;
+      } else if (k == un) {
+        EAU[k] = make_float2(0.0f, 0.0f);
+        QX[k] = 0.0f;
+      } else {
+        const int j = k - un - 1;
+        const double y = d.quad[2 * (size_t)j + 1];
+        EAV[j] = make_float2((float)axis_expm1(y, Ugy, lam, ref.lam0), (float)ref.Av[j]);
+        QY[j] = (float)y;
+      }
+    }
+  }
+  __syncthreads();
+  const double *c = fc + FR_C;
+  const double Mt0 = c[15];
+  const float2 nx2 = bc2((float)n.x), ny2 = bc2((float)n.y), mny2 = bc2(-(float)n.y);
+  const float2 fUx = bc2((float)fc[FR_UX]), fUy = bc2((float)fc[FR_UY]), flam2 = bc2((float)(2.0 * fc[FR_LAM]));
+  const float2 fsx = bc2((float)fc[FR_SX]), fsy = bc2((float)fc[FR_SY]);
+  const float2 fkb = bc2((float)fc[FR_KB]), fdkb = bc2((float)(fc[FR_KB] - ref.kb0));
+  const float2 fMt0 = bc2((float)Mt0), fMt3L = bc2((float)c[16]), fnMt4L = bc2((float)(-c[17]));
   const float2 fT0 = bc2((float)(c[10] - Mt0)), fT1 = bc2((float)c[11]), fT2 = bc2((float)c[12]);
   const float2 fT3 = bc2((float)c[13]), fCT = bc2((float)c[14]);
   // upwind slope coefficients: aR for u <= 0, aR + dA for u > 0
@@ -396,14 +547,16 @@ __device__ __forceinline__ void face_item_delta(const ugks_fused_block *__restri
 #pragma unroll
   for (int k = 0; k < 5; ++k) acc[k] = make_float2(0.0f, 0.0f);
   float4 *frow = reinterpret_cast<float4 *>(dir == SOUTH ? blk.flux_S : blk.flux_W) + pidx(d, gi, gj, 0);
-  ia = threadIdx.x / vn;
-  jv = threadIdx.x % vn;
+  const float4 *arow = reinterpret_cast<const float4 *>(dir == SOUTH ? blk.aux_S : blk.aux_W) + pidx(d, gi, gj, 0);
+  const int qs = NT / vn, rs = NT % vn;
+  int ia = threadIdx.x / vn, jv = threadIdx.x % vn;
 #pragma unroll 1
   for (int p = threadIdx.x; p < NP; p += NT) {
-    const float4 fd = FHB[p], sg = SGB[p], uv = UVF[p];
+    const float4 fd = frow[p], sg = arow[p];
     const float4 eu = EAU2[ia];  // (a, len Au) of u-nodes 2ia and 2ia + 1
     const float2 ev = EAV[jv];   // (b, Av), shared by the pair
-    const float2 U = lo2(uv), T = hi2(uv);
+    const float2 qx = QX2[ia], qy = bc2(QY[jv]);
+    const float2 U = fma2(qx, nx2, mul2(qy, ny2)), T = fma2(qy, nx2, mul2(qx, mny2));
     const float2 r = rel_excess(make_float2(eu.x, eu.z), bc2(ev.x));
     const float2 ml = mul2(make_float2(eu.y, eu.w), bc2(ev.y));  // len M
     const float2 h0 = fma2(ml, r, ml);
@@ -432,14 +585,29 @@ __device__ __forceinline__ void face_item_delta(const ugks_fused_block *__restri
     ia += qs;
     if (jv >= vn) { jv -= vn; ++ia; }
   }
-  double da[5];
+  // the per-thread FP32 sums, added in FP64 across the CTA
+  double af[5];
 #pragma unroll
-  for (int k = 0; k < 5; ++k) da[k] = (double)acc[k].x + (double)acc[k].y;
-  block_sum_to0<5>(da, sh.scratch);
+  for (int k = 0; k < 5; ++k) {
+    af[k] = (double)acc[k].x + (double)acc[k].y;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) af[k] += __shfl_xor_sync(0xffffffffu, af[k], o);
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0)
+#pragma unroll
+    for (int k = 0; k < 5; ++k) scratch[k * (NT / 32) + warp] = af[k];
+  __syncthreads();
   if (threadIdx.x == 0) {
+    double da[5];
+    for (int k = 0; k < 5; ++k) {
+      da[k] = 0.0;
+      for (int q = 0; q < NT / 32; ++q) da[k] += scratch[k * (NT / 32) + q];
+    }
     // M's part of the discrete macro flux: sums of u_n M (1, u_n, u_t, |u|^2)
     // and u_n M_b from the global moments
-    const double nx = n.x, ny = n.y;
+    const double *R = ref.mom;
+    const double nx = n.x, ny = n.y, Mt3L = c[16];
     const double K0 = nx * R[RM10] + ny * R[RM01];
     const double K1 = nx * nx * R[RM20] + 2.0 * nx * ny * R[RM11] + ny * ny * R[RM02];
     const double K2 = -nx * ny * R[RM20] + (nx * nx - ny * ny) * R[RM11] + nx * ny * R[RM02];

@@ -808,8 +808,8 @@ __device__ __forceinline__ void face_neighbours(const ugks_fused_block &blk, Fac
 }
 
 // face work item -> (block, i, j, direction, wall face); false when the item
-// is skipped (inactive solve, retry pass of a solve without retry, other flux
-// method, or the unused S face of the last column / W face of the last row).
+// is skipped (inactive solve, retry pass of a solve without retry, another flux
+// method than FM >= 0, or the unused S face of the last column / W face of the last row).
 // S and W faces of one corner (i, j) are adjacent work items so that both
 // directions read f while it is in L2.
 struct FaceWork {
@@ -826,7 +826,7 @@ __device__ __forceinline__ bool face_work(const ugks_fused_block *__restrict__ B
   const ugks_solve_state &sol = solves[blk.solve];
   if (!sol.active) return false;
   if (retry_pass && !sol.retry) return false;
-  if (d.flux_method != FM) return false;
+  if (FM >= 0 && d.flux_method != FM) return false;  // FM < 0: any flux method
   int lf = w - blk.face_begin;
   fw.dir = lf & 1;
   lf >>= 1;
@@ -1734,11 +1734,21 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
     }
   }
   const bool narrow = z->max_nv <= FaceBudget<T>::narrow_max_nv;
-  mark(1);
+  // mixed: the interior faces' coefficient and flux launches follow the first
+  // dt check (they use its dt), and the events bracket all of the face pass
+  if (!mixed) mark(1);
   dt_check<<<sg, 128, 0, st>>>(solves, ns, 0);
-  mark(2);
+  if (!mixed) mark(2);
   if (narrow) launch_retry<T, FaceBudget<T>::narrow, FT>(B, nb, z, solves, ns, smem, st);
   else launch_retry<T, FaceBudget<T>::wide, FaceBudget<T>::wide_threads>(B, nb, z, solves, ns, smem, st);
+  if (mixed && z->n_faces) {
+    face_coef_delta<<<(unsigned)((z->n_faces + 127) / 128), 128, 0, st>>>(B, nb, solves, z->n_faces);
+    face_flux_delta<FLUX_NT><<<(unsigned)z->n_faces, FLUX_NT, delta_flux_smem(z->max_axes), st>>>(B, nb, solves, 0);
+  }
+  if (mixed) {
+    mark(1);
+    mark(2);
+  }
   mark(3);
   dt_check<<<sg, 128, 0, st>>>(solves, ns, 1);
   mark(4);
@@ -1832,8 +1842,8 @@ int ugks_step_profiled(int mixed, const ugks_fused_block *blocks_dev, int nblock
                : step_impl<double>(blocks_dev, nblocks, sizes, solves_dev, nsolves, stream, events);
 }
 int ugks_step_launches(const ugks_fused_sizes *z, int mixed) {
-  (void)mixed;  // the same kernels run in both precisions
   int n = 0;
+  if (mixed && z->n_faces) n += 2;  // the mixed face pass's coefficient and flux launches
   for (int k = 0; k < z->n_segments && k < UGKS_MAX_FACE_SEGMENTS; ++k) n += z->seg_count[k] > 0 ? 1 : 0;
   for (int m = 0; m < 4; ++m) n += z->face_count[m] > 0 ? 1 : 0;  // retry passes
   n += 2;                                                          // dt checks

@@ -274,6 +274,12 @@ class FusedSolver:
         blk.cell_mom = z(Ni, Nj, 4)
         blk.Q_next = z(ni, nj, 2)
         blk.face_geo = z(Ni, Nj, 2, 6)
+        if self.precision != "fp64":
+            # the mixed face pass's scratch: slopes beside the stored face
+            # deviations, and a record per face between its three launches
+            blk.aux_S = z(*shape, dt=self.sdtype)
+            blk.aux_W = z(*shape, dt=self.sdtype)
+            blk.face_rec = z(Ni, Nj, 2, _lib.FACE_REC)
         x = _lib.FusedBlock()
         d = x.d
         d.ni, d.nj, d.Ni, d.Nj, d.ghost, d.Nv = ni, nj, Ni, Nj, G, Nv
@@ -300,6 +306,8 @@ class FusedSolver:
             setattr(x, name, getattr(blk, name).data_ptr())
         if "ref" in tabs:
             x.ref = tabs["ref"].data_ptr()
+        if self.precision != "fp64":
+            x.aux_S, x.aux_W, x.face_rec = blk.aux_S.data_ptr(), blk.aux_W.data_ptr(), blk.face_rec.data_ptr()
         blk.struct = x
         return blk
 
@@ -313,7 +321,8 @@ class FusedSolver:
         """Kernel launches of one ugks_step_* call (ugks_step_launches): one
         face pass per (limiter, Nv) segment, one retry pass per limiter
         present, two dt checks, the cell pass, the dt update and the ghost
-        pass."""
+        pass; mixed precision adds the face pass's coefficient and flux
+        launches."""
         return self.lib.ugks_step_launches(C.byref(self.sizes), 0 if self.precision == "fp64" else 1)
 
     def step(self, n: int = 1):

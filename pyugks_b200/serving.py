@@ -380,11 +380,11 @@ def request_stream(seed=2, rate=20.0, duration=600.0, max_steps=20000, tol=1e-6)
             Tw = float(rng.uniform(0.8, 1.2))
             scheme = "WENO5" if rng.random() < 0.5 else "vanLeer"
             case = configs.cavity(n=n, m=m, vlim=5.0, flux_method=scheme, Kn=Kn, lid=lid, T_wall=Tw,
-                                  CFL=0.3)
+                                  CFL=configs.WORKLOAD_CFL)
         else:
             k = int(rng.choice([1, 2, 4]))
             m = int(rng.choice([16, 24, 32]))
             Kn = float(10 ** rng.uniform(np.log10(0.01), np.log10(0.5)))
-            case = configs.channel(nblocks=4, n=16 * k, nj=16 * k, m=m, Kn=Kn)
+            case = configs.channel(nblocks=4, n=16 * k, nj=16 * k, m=m, Kn=Kn, CFL=configs.WORKLOAD_CFL)
         out.append(Request(len(out), t, case, max_steps, tol))
     return out

@@ -34,6 +34,9 @@ Cases:
                (configs.open_channel)
   cavity32     the 32x32 cavity, 25x25 velocities on [-4,4]^2, vanLeer, Kn 0.075,
                CFL 0.8, lid 0.15 (fields at steps 1/10/100/1000)
+  multiblock_cfl03_divergence (only when named: about an hour on 8 cores)
+               the benchmarked 2x2-block WENO5 cavity at CFL 0.3 run by the
+               reference until its NaN flag: a trajectory every 25 steps
   cavity32_perturbed
                the same case run by the reference a second time with f
                multiplied by (1 + 1e-14 N(0,1)) after start-up (fields at
@@ -110,6 +113,28 @@ def perturbed_envelope(name, steps, amp=1e-14, seed=0):
     return out
 
 
+def divergence_trajectory(every=25, limit=2000, CFL=0.3):
+    """The benchmarked 2x2-block WENO5 cavity (bench.workload("multiblock"))
+    run by the reference's kernels at the given CFL until a NaN or `limit`
+    steps: per `every` steps dt, max |U|, max T, min rho and min f (over
+    interior cells and velocities), and the step the NaN flag was raised."""
+    from bench import workload
+    case = workload("multiblock")[0][0]
+    case["CFL"] = CFL
+    sim = host.OracleSim(case, "ref", threads=os.cpu_count())
+    rows, nan_step = [], -1
+    for s in range(1, limit + 1):
+        if sim.one_step():
+            nan_step = s
+            break
+        if s % every == 0:
+            fl = sim.fields()
+            rows.append([s, sim.dt, max(float(np.max(np.abs(f["U"]))) for f in fl),
+                         max(float(np.max(f["T"])) for f in fl), min(float(np.min(f["rho"])) for f in fl),
+                         min(float(np.min(b.f[b.G:-b.G, b.G:-b.G, :, 0])) for b in sim.blocks)])
+    return {"rows": np.array(rows), "nan_step": np.array(nan_step), "CFL": np.array(CFL)}
+
+
 def main(names=None):
     for name, (make, steps, with_f) in CASES.items():
         if names and name not in names:
@@ -125,6 +150,10 @@ def main(names=None):
                 data["s%d_%s" % (s, k)] = v
         path = os.path.join(HERE, name + ".npz")
         np.savez_compressed(path, **data)
+        print(path, os.path.getsize(path))
+    if names and "multiblock_cfl03_divergence" in names:
+        path = os.path.join(HERE, "multiblock_cfl03_divergence.npz")
+        np.savez_compressed(path, **divergence_trajectory())
         print(path, os.path.getsize(path))
     if not names or "cavity32_perturbed" in names:
         path = os.path.join(HERE, "cavity32_perturbed.npz")
