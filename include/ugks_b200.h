@@ -290,7 +290,8 @@ typedef struct ugks_fused_block {
   int32_t face_begin;          /* first face work item of this block       */
   int32_t cell_begin;          /* first cell work item                     */
   int32_t ghost_begin;         /* first ghost-cell work item               */
-  int32_t pad_;
+  int32_t wall_begin;          /* first wall-face work item (2 (ni + nj) per block:
+                                  S faces of rows 0 and nj, W faces of columns 0 and ni) */
   void *f;                     /* [Ni][Nj][Nv] x (h, b), double or float    */
   void *flux_S;                /* [Ni][Nj][Nv] x (h, b), SOUTH-face fluxes  */
   void *flux_W;                /* WEST-face fluxes                          */
@@ -386,7 +387,7 @@ typedef struct ugks_fused_sizes {
      to round-off across shapes and are reproducible for a fixed shape. */
   int32_t seg_variant[UGKS_MAX_FACE_SEGMENTS];
   int32_t cell_variant;
-  int32_t pad_;
+  int32_t n_wall;         /* wall-face work items (2 (ni + nj) per block)          */
 } ugks_fused_sizes;
 
 #define UGKS_FACE_VARIANTS 5

@@ -42,7 +42,7 @@ class FusedBlock(C.Structure):
         ("d", BlockDesc), ("solve", i32),
         ("bc_type", i32 * 4), ("bc_block", i32 * 4), ("bc_face", i32 * 4), ("bc_ori", i32 * 4),
         ("bc_flip", i32 * 4),
-        ("face_begin", i32), ("cell_begin", i32), ("ghost_begin", i32), ("pad_", i32),
+        ("face_begin", i32), ("cell_begin", i32), ("ghost_begin", i32), ("wall_begin", i32),
         ("f", vp), ("flux_S", vp), ("flux_W", vp), ("flux_macro_S", vp), ("flux_macro_W", vp),
         ("macro", vp), ("Q", vp), ("prim_old", vp),
         ("area", vp), ("centre", vp), ("mid_side", vp), ("normal", vp), ("side_length", vp),
@@ -74,7 +74,7 @@ class FusedSizes(C.Structure):
                 ("face_begin", i32 * 4), ("face_count", i32 * 4), ("max_axes", i32),
                 ("n_segments", i32), ("seg_begin", i32 * 16), ("seg_count", i32 * 16),
                 ("seg_method", i32 * 16), ("seg_max_nv", i32 * 16), ("seg_max_axes", i32 * 16),
-                ("seg_variant", i32 * 16), ("cell_variant", i32), ("pad_", i32)]
+                ("seg_variant", i32 * 16), ("cell_variant", i32), ("n_wall", i32)]
 
 
 FACE_VARIANTS = 5   # UGKS_FACE_VARIANTS: 0 automatic, 1..4 forced shapes

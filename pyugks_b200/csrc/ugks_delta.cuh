@@ -202,11 +202,10 @@ constexpr int FR_MOM = 0, FR_C = 16, FR_UX = 38, FR_UY = 39, FR_LAM = 40, FR_KB 
               FR_LNP = 44, FR_UGX = 45, FR_UGY = 46;
 static_assert(FR_UGY < UGKS_FACE_REC, "face record layout");
 
-// shared memory of a moments CTA: the axis velocities, and for a wall face Nv
-// (h, b) FP64 face values plus Nv float2 of scratch
-inline size_t delta_face_smem(int max_nv, int max_axes) {
-  return 24 * (size_t)max_nv + 4 * (size_t)(max_axes + 2) + 16;
-}
+// shared memory of a moments CTA (the axis velocities), and of a wall CTA
+// (Nv (h, b) FP64 face values plus Nv float2 of scratch)
+inline size_t delta_face_smem(int max_axes) { return 4 * (size_t)(max_axes + 2) + 16; }
+inline size_t delta_wall_smem(int max_nv) { return 24 * (size_t)max_nv + 16; }
 // threads of a flux CTA
 constexpr int FLUX_NT = 128;
 // shared memory of a flux CTA: per velocity-axis node (a, len Au) / (b, Av)
@@ -223,15 +222,59 @@ __device__ __forceinline__ void axis_velocities(const ugks_block_desc &d, float 
   }
 }
 
-// 1. moments (a CTA per face; in the retry pass, wall faces only)
-template <int FM, int NT>
+// Sums N <= 16 values over the 32 lanes of a warp by halving butterflies: at
+// each exchange a lane keeps half of its values and adds the partner lane's
+// copies of that half, so that P - 1 + (5 - log2 P) exchanges (P = N rounded
+// up to a power of 2) replace the 5 N of one butterfly per value.  On return
+// the 2^S lanes from k << S on (S = spread_shift<N>()) hold the total of
+// value k.
+template <int N>
+__device__ __forceinline__ constexpr int spread_width() {
+  return N <= 1 ? 1 : (N <= 2 ? 2 : (N <= 4 ? 4 : (N <= 8 ? 8 : 16)));
+}
+template <int N>
+__device__ __forceinline__ constexpr int spread_shift() {
+  return N <= 1 ? 5 : (N <= 2 ? 4 : (N <= 4 ? 3 : (N <= 8 ? 2 : 1)));
+}
+template <int C, int O, int P>
+__device__ __forceinline__ void spread_step(double (&v)[P], unsigned lane) {
+  if constexpr (O >= 1) {
+    if constexpr (C > 1) {
+      constexpr int H = C / 2;
+      const bool hi = (lane & O) != 0;
+#pragma unroll
+      for (int k = 0; k < H; ++k) {
+        const double keep = hi ? v[k + H] : v[k], send = hi ? v[k] : v[k + H];
+        v[k] = keep + __shfl_xor_sync(0xffffffffu, send, O);
+      }
+      spread_step<H, O / 2, P>(v, lane);
+    } else {
+      v[0] += __shfl_xor_sync(0xffffffffu, v[0], O);
+      spread_step<1, O / 2, P>(v, lane);
+    }
+  }
+}
+template <int N>
+__device__ __forceinline__ double warp_spread_sum(const double (&x)[N]) {
+  static_assert(N >= 1 && N <= 16, "at most 16 values");
+  constexpr int P = spread_width<N>();
+  double v[P];
+#pragma unroll
+  for (int k = 0; k < P; ++k) v[k] = k < N ? x[k] : 0.0;
+  spread_step<P, 16, P>(v, threadIdx.x & 31);
+  return v[0];
+}
+
+// 1. moments (a CTA per face).  WALLS: a wall face, whose whole procedure
+// runs here (the wall launch, and the retry pass, where interior faces have
+// nothing to redo: the moments do not depend on dt); else an interior face.
+template <int FM, int NT, bool WALLS>
 __device__ __forceinline__ void face_item_delta(const ugks_fused_block *__restrict__ B, int nb,
                                                 ugks_solve_state *__restrict__ solves, const int w, int retry_pass) {
   extern __shared__ double dyn[];
-  __shared__ FaceShared<NT> sh;
   FaceWork fwk;
   if (!face_work<FM>(B, nb, solves, w, retry_pass, fwk)) return;
-  if (retry_pass && fwk.wall < 0) return;  // interior faces do not depend on dt here
+  if (WALLS != (fwk.wall >= 0)) return;
   const ugks_fused_block &blk = B[fwk.bi];
   const ugks_block_desc &d = blk.d;
   ugks_solve_state &sol = solves[blk.solve];
@@ -253,8 +296,9 @@ __device__ __forceinline__ void face_item_delta(const ugks_fused_block *__restri
   constexpr int L = FM == 1 ? 5 : 3, MID = FM == 1 ? 2 : 1;
   float4 *frow = reinterpret_cast<float4 *>(dir == SOUTH ? blk.flux_S : blk.flux_W) + pidx(d, gi, gj, 0);
 
-  if (wall >= 0) {
+  if constexpr (WALLS) {
     // ---------------- wall face: the FP64 wall procedure on M + df --------
+    __shared__ FaceShared<NT> sh;
     double *fw = dyn;                                          // Nv x (h, b)
     float2 *rin = reinterpret_cast<float2 *>(fw + 2 * (size_t)Nv);  // Nv
     const int step = dir == SOUTH ? 1 : d.Nj;                  // cells
@@ -281,8 +325,7 @@ __device__ __forceinline__ void face_item_delta(const ugks_fused_block *__restri
       const double m = dl * (e.x * n.x + e.y * n.y) * ref.mh[v];
       pair_put(frow, v, vn, (float)(hx - m), (float)(hy - ref.kb0 * m));
     });
-    return;
-  }
+  } else {
 
   // ---------------- interior face: reconstruction and moments -------------
   float *QX = reinterpret_cast<float *>(dyn), *QY = QX + (d.u_num + 1);
@@ -294,9 +337,13 @@ __device__ __forceinline__ void face_item_delta(const ugks_fused_block *__restri
   const float4 *up1 = fcell - (MID + 1) * pstep, *up0 = fcell + MID * pstep;
   float4 *arow = reinterpret_cast<float4 *>(dir == SOUTH ? blk.aux_S : blk.aux_W) + pidx(d, gi, gj, 0);
   const float2 nx2 = bc2((float)n.x), ny2 = bc2((float)n.y), mny2 = bc2(-(float)n.y);
-  float2 mom[RNMOM];
+  // raw moments of the face deviation in FP64, products included: the face
+  // heat flux is a small difference of them
+  double mom[RNMOM];
 #pragma unroll
-  for (int k = 0; k < RNMOM; ++k) mom[k] = make_float2(0.0f, 0.0f);
+  for (int k = 0; k < RNMOM; ++k) mom[k] = 0.0;
+  const double *__restrict__ qd = d.quad;
+  const int un = d.u_num;
   // pair p = a v_num + jv: velocities (2a, jv) and (2a + 1, jv)
   const int qs = NT / vn, rs = NT % vn;
   int ia = threadIdx.x / vn, jv = threadIdx.x % vn;
@@ -333,44 +380,80 @@ __device__ __forceinline__ void face_item_delta(const ugks_fused_block *__restri
     const float2 fh = fma2(sh2, ds, Sh[MID]), fb = fma2(sb2, ds, Sb[MID]);
     frow[p] = cat2(fh, fb);
     arow[p] = cat2(sh2, sb2);
-    // raw moments of the face deviation (face frame)
-    const float2 t1 = mul2(U, fh), t2 = mul2(T, fh), uu = mul2(U, U), tt = mul2(T, T);
-    mom[RM00] = add2(mom[RM00], fh);
-    mom[RM10] = add2(mom[RM10], t1);
-    mom[RM01] = add2(mom[RM01], t2);
-    mom[RM20] = fma2(U, t1, mom[RM20]);
-    mom[RM11] = fma2(T, t1, mom[RM11]);
-    mom[RM02] = fma2(T, t2, mom[RM02]);
-    mom[RM30] = fma2(uu, t1, mom[RM30]);
-    mom[RM21] = fma2(uu, t2, mom[RM21]);
-    mom[RM12] = fma2(tt, t1, mom[RM12]);
-    mom[RM03] = fma2(tt, t2, mom[RM03]);
-    mom[RB00] = add2(mom[RB00], fb);
-    mom[RB10] = fma2(U, fb, mom[RB10]);
-    mom[RB01] = fma2(T, fb, mom[RB01]);
+    // raw moments of the face deviation (face frame); the padding velocity of
+    // an odd u_num has df = 0 and reads velocity 0
+    {
+      const double y = qd[2 * (size_t)jv + 1];
+      const int ua = 2 * ia, ub = 2 * ia + 1 < un ? 2 * ia + 1 : 0;
+      const double xs[2] = {qd[2 * (size_t)ua * vn], qd[2 * (size_t)ub * vn]};
+      const double hs[2] = {fh.x, fh.y}, bs[2] = {fb.x, fb.y};
+#pragma unroll
+      for (int e = 0; e < 2; ++e) {
+        const double u = fma(xs[e], n.x, y * n.y), t = fma(y, n.x, -xs[e] * n.y);
+        const double h = hs[e], b = bs[e], t1 = u * h, t2 = t * h, uu = u * u, tt = t * t;
+        mom[RM00] += h;
+        mom[RM10] += t1;
+        mom[RM01] += t2;
+        mom[RM20] = fma(u, t1, mom[RM20]);
+        mom[RM11] = fma(t, t1, mom[RM11]);
+        mom[RM02] = fma(t, t2, mom[RM02]);
+        mom[RM30] = fma(uu, t1, mom[RM30]);
+        mom[RM21] = fma(uu, t2, mom[RM21]);
+        mom[RM12] = fma(tt, t1, mom[RM12]);
+        mom[RM03] = fma(tt, t2, mom[RM03]);
+        mom[RB00] += b;
+        mom[RB10] = fma(u, b, mom[RB10]);
+        mom[RB01] = fma(t, b, mom[RB01]);
+      }
+    }
     jv += rs;
     ia += qs;
     if (jv >= vn) { jv -= vn; ++ia; }
   }
-  // the per-thread FP32 sums, added in FP64 across the CTA
-  double mf[RNMOM];
-#pragma unroll
-  for (int k = 0; k < RNMOM; ++k) {
-    mf[k] = (double)mom[k].x + (double)mom[k].y;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) mf[k] += __shfl_xor_sync(0xffffffffu, mf[k], o);
-  }
+  // added across the CTA
+  __shared__ double red[RNMOM * (NT / 32)];
+  const double tw = warp_spread_sum<RNMOM>(mom);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0)
-#pragma unroll
-    for (int k = 0; k < RNMOM; ++k) sh.scratch[k * (NT / 32) + warp] = mf[k];
+  constexpr int S = spread_shift<RNMOM>();
+  if ((lane & ((1 << S) - 1)) == 0 && (lane >> S) < RNMOM) red[(lane >> S) * (NT / 32) + warp] = tw;
   __syncthreads();
   if (threadIdx.x < RNMOM) {
     double t = 0.0;
-    for (int q = 0; q < NT / 32; ++q) t += sh.scratch[threadIdx.x * (NT / 32) + q];
+    for (int q = 0; q < NT / 32; ++q) t += red[threadIdx.x * (NT / 32) + q];
     blk.face_rec[(size_t)UGKS_FACE_REC * faceidx(d, gi, gj, dir) + FR_MOM + threadIdx.x] = t;
   }
+  }
 }
+
+// wall faces of the main pass: a CTA per wall work item (2 (ni + nj) per
+// block: the S faces of rows 0 and nj, then the W faces of columns 0 and ni),
+// running the wall procedure when that side of the block is a wall
+template <int NT>
+__global__ void __launch_bounds__(NT) wall_pass_delta(const ugks_fused_block *__restrict__ B, int nb,
+                                                      ugks_solve_state *__restrict__ solves) {
+  const int w = (int)blockIdx.x;
+  const ugks_fused_block &blk = B[find_block<3>(B, nb, w)];
+  const ugks_block_desc &d = blk.d;
+  int lw = w - blk.wall_begin, mi, mj, dir;
+  if (lw < 2 * d.ni) {
+    dir = SOUTH;
+    mi = lw % d.ni;
+    mj = lw < d.ni ? 0 : d.nj;
+  } else {
+    lw -= 2 * d.ni;
+    dir = WEST;
+    mj = lw % d.nj;
+    mi = lw < d.nj ? 0 : d.ni;
+  }
+  const int fw = blk.face_begin + ((mi * (d.nj + 1) + mj) << 1) + dir;
+  switch (d.flux_method) {
+    case 0: face_item_delta<0, NT, true>(B, nb, solves, fw, 0); break;
+    case 1: face_item_delta<1, NT, true>(B, nb, solves, fw, 0); break;
+    case 3: face_item_delta<3, NT, true>(B, nb, solves, fw, 0); break;
+    default: break;
+  }
+}
+constexpr int WALL_NT = 128;
 
 // 2. coefficients: the per-face block of face_coefficients, one face per
 // thread (the same chain as the lanes of a face CTA run there)
@@ -588,15 +671,11 @@ __global__ void __launch_bounds__(NT, 5) face_flux_delta(const ugks_fused_block 
   // the per-thread FP32 sums, added in FP64 across the CTA
   double af[5];
 #pragma unroll
-  for (int k = 0; k < 5; ++k) {
-    af[k] = (double)acc[k].x + (double)acc[k].y;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) af[k] += __shfl_xor_sync(0xffffffffu, af[k], o);
-  }
+  for (int k = 0; k < 5; ++k) af[k] = (double)acc[k].x + (double)acc[k].y;
+  const double tw = warp_spread_sum<5>(af);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0)
-#pragma unroll
-    for (int k = 0; k < 5; ++k) scratch[k * (NT / 32) + warp] = af[k];
+  constexpr int S = spread_shift<5>();
+  if ((lane & ((1 << S) - 1)) == 0 && (lane >> S) < 5) scratch[(lane >> S) * (NT / 32) + warp] = tw;
   __syncthreads();
   if (threadIdx.x == 0) {
     double da[5];
@@ -620,6 +699,27 @@ __global__ void __launch_bounds__(NT, 5) face_flux_delta(const ugks_fused_block 
     out.s2 = g.y;
     st4(dir == SOUTH ? blk.flux_macro_S : blk.flux_macro_W, gidx(d, gi, gj), out);
   }
+}
+
+#ifndef UGKS_SR_STORE
+#define UGKS_SR_STORE 0
+#endif
+// integer hash (a 32-bit xorshift-multiply mixer) for stochastic rounding
+__device__ __forceinline__ uint32_t sr_hash(uint32_t x) {
+  x ^= x >> 16;
+  x *= 0x7feb352du;
+  x ^= x >> 15;
+  x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+// x rounded to the float toward zero or the next one away from zero, away
+// with probability (x - toward) / (away - toward), u16 / 65536 uniform
+__device__ __forceinline__ float sr_round(double x, uint32_t u16) {
+  const float z = __double2float_rz(x);
+  const float a = __uint_as_float(__float_as_uint(z) + 1u);
+  const double gap = (double)a - (double)z, rem = x - (double)z;
+  return fabs(rem) > (double)u16 * (1.0 / 65536.0) * fabs(gap) ? a : z;
 }
 
 // ---------------------------------------------------------------------------
@@ -718,20 +818,28 @@ __global__ void __launch_bounds__(CW * 32, MINB) cell_pass_delta(const ugks_fuse
   const double ko = (0.5 * d.K) * nr_rcp(old.s3);
   const double so = 0.8 * (1 - d.Pr) * (old.s3 * old.s3) * nr_rcp(old.s0);
   const float2 fa1 = bc2((float)bc[3]), fa2 = bc2((float)bc[4]), fa3 = bc2((float)a3), fa4 = bc2((float)a4);
+#if UGKS_SR_STORE
+  const double a1d = bc[3];
+  const uint32_t srseed = sr_hash((uint32_t)sol.steps * 0x9e3779b9u + (uint32_t)bi * 0x85ebca6bu);
+#endif
   const float2 fkbn = bc2((float)kn), fkbo = bc2((float)ko);
   const float2 fdkn = bc2((float)(kn - ref.kb0)), fdko = bc2((float)(ko - ref.kb0));
   const float2 fa3kn = bc2((float)(a3 * kn)), fa4ko = bc2((float)(a4 * ko));
   const float2 fso = bc2((float)so), fsn = bc2((float)sn), fQx = bc2((float)Q.x), fQy = bc2((float)Q.y);
   const float2 fUox = bc2((float)old.s1), fUoy = bc2((float)old.s2), fUnx = bc2((float)nU), fUny = bc2((float)nV);
   const float2 flo2 = bc2((float)(2.0 * old.s3)), fln2 = bc2((float)(2.0 * nl));
-  const float2 fKinv = bc2((float)nr_rcp(d.K));
   const size_t base = pidx(d, gi, gj, 0);
   const size_t sj = (size_t)NP, si = (size_t)d.Nj * NP;
   float4 *gf = reinterpret_cast<float4 *>(blk.f);
   const float4 *gS = reinterpret_cast<const float4 *>(blk.flux_S), *gW = reinterpret_cast<const float4 *>(blk.flux_W);
-  float2 mom[6];
+  // moments of df' in FP64, products included: the deviation's heat flux
+  // nearly cancels the reference's (q is a small difference of large
+  // moments), so FP32 sums would dominate its error
+  double mom[6];
 #pragma unroll
-  for (int k = 0; k < 6; ++k) mom[k] = make_float2(0.0f, 0.0f);
+  for (int k = 0; k < 6; ++k) mom[k] = 0.0;
+  const double *__restrict__ qd = d.quad;
+  const double dUx = nU, dUy = nV, Kinv = nr_rcp(d.K);
   // pair p = a v_num + jv: velocities (2a, jv) and (2a + 1, jv)
   const int qs = 32 / vn, rs = 32 % vn;
   int ia = lane / vn, jv = lane % vn;
@@ -759,25 +867,44 @@ __global__ void __launch_bounds__(CW * 32, MINB) cell_pass_delta(const ugks_fuse
                                 mul2(m, fma2(fa4, fma2(fkbo, ro, fdko), mul2(fa3, fma2(fkbn, rn, fdkn))))));
     const float2 flh = add2(sub2(lo2(s0), lo2(s1)), sub2(lo2(w0), lo2(w1)));
     const float2 flb = add2(sub2(hi2(s0), hi2(s1)), sub2(hi2(w0), hi2(w1)));
+#if UGKS_SR_STORE
+    // stochastic rounding of the new deviation: f a1 + increment in FP64,
+    // rounded to a neighbouring float with probability given by its distance
+    const float2 ih = fma2(flh, fa2, eh), ib = fma2(flb, fa2, eb);
+    uint32_t h1 = sr_hash((uint32_t)k * 2654435761u ^ srseed), h2 = sr_hash(h1 ^ 0x68e31da4u);
+    const float2 oh = make_float2(sr_round(fma((double)f.x, a1d, (double)ih.x), h1 & 0xffffu),
+                                  sr_round(fma((double)f.y, a1d, (double)ih.y), h1 >> 16));
+    const float2 ob = make_float2(sr_round(fma((double)f.z, a1d, (double)ib.x), h2 & 0xffffu),
+                                  sr_round(fma((double)f.w, a1d, (double)ib.y), h2 >> 16));
+#else
     const float2 oh = fma2(lo2(f), fa1, fma2(flh, fa2, eh)), ob = fma2(hi2(f), fa1, fma2(flb, fa2, eb));
+#endif
     gf[k] = cat2(oh, ob);
     // moments of df' for the next face pass and calcQ of f^{n+1} with the new
-    // macro (the deviation's part); a NaN anywhere reaches mom[0] or mom[3]
-    const float2 qq = fma2(qx, qx, mul2(qy, qy));
-    mom[0] = add2(mom[0], oh);
-    mom[1] = fma2(qx, oh, mom[1]);
-    mom[2] = fma2(qy, oh, mom[2]);
-    mom[3] = fma2(qq, oh, add2(mom[3], ob));
-    const float2 tq = fma2(n2, oh, mul2(ob, fKinv));
-    mom[4] = fma2(nx, tq, mom[4]);
-    mom[5] = fma2(ny, tq, mom[5]);
+    // macro (the deviation's part); a NaN anywhere reaches mom[0] or mom[3].
+    // The padding velocity of an odd u_num has df' = 0 and reads velocity 0.
+    {
+      const double y = qd[2 * (size_t)jv + 1];
+      const int ua = 2 * ia, ub = 2 * ia + 1 < un ? 2 * ia + 1 : 0;
+      const double xa = qd[2 * (size_t)ua * vn], xb = qd[2 * (size_t)ub * vn];
+      const double ha = oh.x, hb = oh.y, ba = ob.x, bb = ob.y;
+      const double cy = y - dUy, cxa = xa - dUx, cxb = xb - dUx;
+      mom[0] += ha + hb;
+      mom[1] = fma(xa, ha, fma(xb, hb, mom[1]));
+      mom[2] = fma(y, ha + hb, mom[2]);
+      mom[3] += fma(fma(xa, xa, y * y), ha, fma(fma(xb, xb, y * y), hb, ba + bb));
+      const double ta = fma(fma(cxa, cxa, cy * cy), ha, ba * Kinv);
+      const double tb = fma(fma(cxb, cxb, cy * cy), hb, bb * Kinv);
+      mom[4] = fma(cxa, ta, fma(cxb, tb, mom[4]));
+      mom[5] = fma(cy, ta + tb, mom[5]);
+    }
     jv += rs;
     ia += qs;
     if (jv >= vn) { jv -= vn; ++ia; }
   }
   double dm[6];
 #pragma unroll
-  for (int k = 0; k < 6; ++k) dm[k] = (double)mom[k].x + (double)mom[k].y;
+  for (int k = 0; k < 6; ++k) dm[k] = mom[k];
   warp_sum<6>(dm);
   if (lane == 0) {
     if (isnan(dm[0]) || isnan(dm[3])) atomicExch(&sol.status, 1);

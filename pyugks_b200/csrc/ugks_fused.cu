@@ -140,7 +140,8 @@ __device__ __forceinline__ int find_block(const ugks_fused_block *B, int nb, int
   int lo = 0, hi = nb - 1;
   while (lo < hi) {
     int mid = (lo + hi + 1) >> 1;
-    int beg = WHICH == 0 ? B[mid].face_begin : (WHICH == 1 ? B[mid].cell_begin : B[mid].ghost_begin);
+    int beg = WHICH == 0 ? B[mid].face_begin
+                         : (WHICH == 1 ? B[mid].cell_begin : (WHICH == 2 ? B[mid].ghost_begin : B[mid].wall_begin));
     if (beg <= w) lo = mid; else hi = mid - 1;
   }
   return lo;
@@ -1022,17 +1023,19 @@ __device__ __forceinline__ void face_item_fp64(const ugks_fused_block *__restric
                                                                v2(hx, hy)); });
 }
 
-// the mixed path's face work item (ugks_delta.cuh, included further down)
-template <int FM, int NT>
+// the mixed path's face work item (ugks_delta.cuh, included further down):
+// WALLS, the wall faces (main pass: the wall launch; retry pass), else the
+// reconstruction and moments of the interior faces
+template <int FM, int NT, bool WALLS>
 __device__ __forceinline__ void face_item_delta(const ugks_fused_block *__restrict__ B, int nb,
                                                 ugks_solve_state *__restrict__ solves, const int w, int retry_pass);
 
 // one face work item: FP64 storage, or the mixed path's FP32 deviations
-template <typename T, int FM, int NT>
+template <typename T, int FM, int NT, bool RETRY>
 __device__ __forceinline__ void face_item(const ugks_fused_block *__restrict__ B, int nb,
-                                          ugks_solve_state *__restrict__ solves, const int w, int retry_pass) {
-  if constexpr (std::is_same<T, float>::value) face_item_delta<FM, NT>(B, nb, solves, w, retry_pass);
-  else face_item_fp64<FM, NT>(B, nb, solves, w, retry_pass);
+                                          ugks_solve_state *__restrict__ solves, const int w) {
+  if constexpr (std::is_same<T, float>::value) face_item_delta<FM, NT, RETRY>(B, nb, solves, w, RETRY ? 1 : 0);
+  else face_item_fp64<FM, NT>(B, nb, solves, w, RETRY ? 1 : 0);
 }
 
 // main face pass: one CTA per face work item of the blocks of one flux method
@@ -1040,7 +1043,7 @@ template <typename T, int FM, int MINB, int NT>
 __global__ void __launch_bounds__(NT, MINB) face_pass(const ugks_fused_block *__restrict__ B, int nb,
                                                                  ugks_solve_state *__restrict__ solves,
                                                                  int first) {
-  face_item<T, FM, NT>(B, nb, solves, first + (int)blockIdx.x, 0);
+  face_item<T, FM, NT, false>(B, nb, solves, first + (int)blockIdx.x);
 }
 
 // the flux pass redone after a dt change (ugks_sim.py:432-441): RETRY_CTAS
@@ -1058,7 +1061,7 @@ __global__ void __launch_bounds__(NT, MINB) face_retry(const ugks_fused_block *_
   if (b0.d.flux_method != FM) return;
   const int end = bl.face_begin + 2 * (bl.d.ni + 1) * (bl.d.nj + 1);
   for (int w = b0.face_begin + r; w < end; w += RETRY_CTAS) {
-    face_item<T, FM, NT>(B, nb, solves, w, 1);
+    face_item<T, FM, NT, true>(B, nb, solves, w);
     __syncthreads();  // the next item reuses the shared tables
   }
 }
@@ -1627,9 +1630,12 @@ cudaError_t set_face_attributes() {
                                        200 * 1024);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(face_retry<T, FM, MINB, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  // FP64 keeps the face's velocities in shared memory; the mixed moments
+  // pass needs only axis tables and reads its stencils through L1
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(face_pass<T, FM, MINB, NT>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             cudaSharedmemCarveoutMaxShared);
+                             std::is_same<T, float>::value ? (int)cudaSharedmemCarveoutMaxL1
+                                                           : (int)cudaSharedmemCarveoutMaxShared);
   return e;
 }
 
@@ -1640,6 +1646,12 @@ cudaError_t set_face_shape() {
   if (e == cudaSuccess) e = set_face_attributes<T, 1, MINB, NT>();
   if (e == cudaSuccess) e = set_face_attributes<T, 3, MINB, NT>();
   return e;
+}
+template <typename T>
+cudaError_t set_wall_attributes() {
+  if constexpr (std::is_same<T, float>::value)
+    return cudaFuncSetAttribute(wall_pass_delta<WALL_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  return cudaSuccess;
 }
 template <typename T, int MINB>
 cudaError_t set_cell_attributes() {
@@ -1662,20 +1674,21 @@ cudaError_t set_step_attributes() {
   if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> guard(lock);
   if (done[dev]) return cudaSuccess;
-  cudaError_t r[6] = {
+  cudaError_t r[7] = {
       set_face_shape<T, 1>(), set_face_shape<T, 2>(), set_face_shape<T, 3>(), set_face_shape<T, 4>(),
-      set_cell_attributes<T, 2>(), set_cell_attributes<T, 3>()};
+      set_cell_attributes<T, 2>(), set_cell_attributes<T, 3>(), set_wall_attributes<T>()};
   for (cudaError_t x : r)
     if (x != cudaSuccess) return x;
   done[dev] = true;
   return cudaSuccess;
 }
 
-// shared memory of a face CTA: (h, b) and slopes per velocity + axis tables
-// (FP32: also the face-frame velocity per node, as float2)
+// shared memory of a face CTA: FP64, (h, b) and slopes per velocity + axis
+// tables; mixed, the axis velocities of an interior face, or (wall faces of
+// the retry pass) the wall procedure's FP64 face values
 template <typename T>
-inline size_t face_smem(int max_nv, int max_axes) {
-  if (std::is_same<T, float>::value) return delta_face_smem(max_nv, max_axes);
+inline size_t face_smem(int max_nv, int max_axes, bool retry = false) {
+  if (std::is_same<T, float>::value) return retry ? delta_wall_smem(max_nv) : delta_face_smem(max_axes);
   return 4 * sizeof(double) * (size_t)max_nv + sizeof(double) * (size_t)max_axes;
 }
 
@@ -1707,7 +1720,7 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
   cudaStream_t st = S(stream);
   // face pass: (h, b) and slopes per velocity + the two axis factor tables;
   // cell pass: the axis factor tables of the old and new macro state
-  const size_t smem = face_smem<T>(z->max_nv, z->max_axes);
+  const size_t smem = face_smem<T>(z->max_nv, z->max_axes, true);
   constexpr bool mixed = std::is_same<T, float>::value;
   // doubles of shared memory per cell warp
   const int cstride = mixed ? delta_cell_stride(z->max_axes) : 2 * z->max_axes + CELL_COEF;
@@ -1733,6 +1746,8 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
       default: launch_segment<T, FaceShape<T, 4>::minb, FaceShape<T, 4>::nt>(B, nb, solves, m, b0, n, sm, st); break;
     }
   }
+  if (mixed && z->n_wall)
+    wall_pass_delta<WALL_NT><<<(unsigned)z->n_wall, WALL_NT, delta_wall_smem(z->max_nv), st>>>(B, nb, solves);
   const bool narrow = z->max_nv <= FaceBudget<T>::narrow_max_nv;
   // mixed: the interior faces' coefficient and flux launches follow the first
   // dt check (they use its dt), and the events bracket all of the face pass
@@ -1844,6 +1859,7 @@ int ugks_step_profiled(int mixed, const ugks_fused_block *blocks_dev, int nblock
 int ugks_step_launches(const ugks_fused_sizes *z, int mixed) {
   int n = 0;
   if (mixed && z->n_faces) n += 2;  // the mixed face pass's coefficient and flux launches
+  if (mixed && z->n_wall) n += 1;   // and its wall launch
   for (int k = 0; k < z->n_segments && k < UGKS_MAX_FACE_SEGMENTS; ++k) n += z->seg_count[k] > 0 ? 1 : 0;
   for (int m = 0; m < 4; ++m) n += z->face_count[m] > 0 ? 1 : 0;  // retry passes
   n += 2;                                                          // dt checks
@@ -1884,7 +1900,7 @@ int ugks_prepare(int mixed) {
 }
 
 int ugks_fused_layout(ugks_fused_block *blocks, int nblocks, ugks_fused_sizes *z) {
-  int64_t f = 0, c = 0, g = 0;
+  int64_t f = 0, c = 0, g = 0, wl = 0;
   int32_t max_nv = 0, max_axes = 0;
   int64_t fb[4] = {0, 0, 0, 0}, fc[4] = {0, 0, 0, 0};
   struct Run {
@@ -1910,6 +1926,8 @@ int ugks_fused_layout(ugks_fused_block *blocks, int nblocks, ugks_fused_sizes *z
     x.face_begin = (int32_t)f;
     x.cell_begin = (int32_t)c;
     x.ghost_begin = (int32_t)g;
+    x.wall_begin = (int32_t)wl;
+    wl += 2ll * (x.d.ni + x.d.nj);
     const int64_t nf = 2ll * (x.d.ni + 1) * (x.d.nj + 1);
     const int axes_b = (x.d.u_num > 0 && x.d.u_num * x.d.v_num == x.d.Nv && x.d.u_num + x.d.v_num <= 512)
                            ? x.d.u_num + x.d.v_num : 0;
@@ -1925,7 +1943,8 @@ int ugks_fused_layout(ugks_fused_block *blocks, int nblocks, ugks_fused_sizes *z
     const int axes = x.d.u_num + x.d.v_num;
     if (x.d.u_num > 0 && x.d.u_num * x.d.v_num == x.d.Nv && axes <= 512 && axes > max_axes) max_axes = axes;
   }
-  if (f > INT32_MAX || c > INT32_MAX || g > INT32_MAX) return -1;
+  if (f > INT32_MAX || c > INT32_MAX || g > INT32_MAX || wl > INT32_MAX) return -1;
+  z->n_wall = (int32_t)wl;
   z->n_faces = (int32_t)f;
   z->n_cells = (int32_t)c;
   z->n_ghost = (int32_t)g;
