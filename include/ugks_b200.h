@@ -352,7 +352,8 @@ typedef struct ugks_solve_state {
                                   (ugks_block.py:1319-1327, ugks_sim.py:463-468) */
   double stop_residual;        /* stop rule: density residual below this (0: none) */
   int32_t stop_steps;          /* stop rule: this many completed steps (0: none)   */
-  int32_t pad2_;
+  int32_t stop_after;          /* the residual rule applies from this many completed
+                                  steps on (the reference's residual_start, 10) */
 } ugks_solve_state;
 
 #define UGKS_STOP_CONVERGED 1
@@ -445,7 +446,8 @@ int ugks_residual(const ugks_fused_block *blocks_dev, int nblocks, ugks_solve_st
 
 /* The stop rule of ugks_solve_state for every active solve, after
    ugks_residual of the same step: a solve with a non-zero status, a density
-   residual below stop_residual or stop_steps completed steps gets stopped =
+   residual below stop_residual after at least stop_after completed steps, or
+   stop_steps completed steps gets stopped =
    UGKS_STOP_ERROR / _CONVERGED / _STEPS and active = 0, so that later fused
    launches skip it (the run loop's exits, ugks_sim.py:587-645, decided on the
    device). */

@@ -59,7 +59,7 @@ class SolveState(C.Structure):
         ("max_freq", C.c_uint64),
         ("retry", i32), ("status", i32), ("steps", i32), ("retries", i32), ("active", i32),
         ("nblocks", i32), ("first_block", i32), ("stopped", i32),
-        ("residual", f64 * 4), ("stop_residual", f64), ("stop_steps", i32), ("pad2_", i32),
+        ("residual", f64 * 4), ("stop_residual", f64), ("stop_steps", i32), ("stop_after", i32),
     ]
 
 

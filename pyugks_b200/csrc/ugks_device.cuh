@@ -395,6 +395,86 @@ __device__ __forceinline__ void block_sum(double (&x)[N], double *scratch) {
   }
 }
 
+// Sums N <= 16 values over the 32 lanes of a warp by halving butterflies: at
+// each exchange a lane keeps half of its values and adds the partner lane's
+// copies of that half, so that P - 1 + (5 - log2 P) exchanges (P = N rounded
+// up to a power of 2) replace the 5 N of one butterfly per value.  On return
+// the 2^S lanes from k << S on (S = spread_shift<N>()) hold the total of
+// value k.
+template <int N>
+__device__ __forceinline__ constexpr int spread_width() {
+  return N <= 1 ? 1 : (N <= 2 ? 2 : (N <= 4 ? 4 : (N <= 8 ? 8 : 16)));
+}
+template <int N>
+__device__ __forceinline__ constexpr int spread_shift() {
+  return N <= 1 ? 5 : (N <= 2 ? 4 : (N <= 4 ? 3 : (N <= 8 ? 2 : 1)));
+}
+template <int C, int O, int P>
+__device__ __forceinline__ void spread_step(double (&v)[P], unsigned lane) {
+  if constexpr (O >= 1) {
+    if constexpr (C > 1) {
+      constexpr int H = C / 2;
+      const bool hi = (lane & O) != 0;
+#pragma unroll
+      for (int k = 0; k < H; ++k) {
+        const double keep = hi ? v[k + H] : v[k], send = hi ? v[k] : v[k + H];
+        v[k] = keep + __shfl_xor_sync(0xffffffffu, send, O);
+      }
+      spread_step<H, O / 2, P>(v, lane);
+    } else {
+      v[0] += __shfl_xor_sync(0xffffffffu, v[0], O);
+      spread_step<1, O / 2, P>(v, lane);
+    }
+  }
+}
+template <int N>
+__device__ __forceinline__ double warp_spread_sum(const double (&x)[N]) {
+  static_assert(N >= 1 && N <= 16, "at most 16 values");
+  constexpr int P = spread_width<N>();
+  double v[P];
+#pragma unroll
+  for (int k = 0; k < P; ++k) v[k] = k < N ? x[k] : 0.0;
+  spread_step<P, 16, P>(v, threadIdx.x & 31);
+  return v[0];
+}
+
+// block_sum with halving butterflies inside each warp: the same totals in
+// another order of summation, in 2 (P - 1) + 2 (5 - log2 P) shuffles per warp
+// instead of 10 N
+template <int N>
+__device__ __forceinline__ void block_sum_spread(double (&x)[N], double *scratch) {
+  const double t = warp_spread_sum<N>(x);
+  constexpr int S = spread_shift<N>();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();  // scratch may still be read by a previous call
+  if ((lane & ((1 << S) - 1)) == 0 && (lane >> S) < N) scratch[(lane >> S) * nw + warp] = t;
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    double s = 0.0;
+    for (int w = 0; w < nw; ++w) s += scratch[k * nw + w];
+    x[k] = s;
+  }
+}
+// the same, with the totals only on thread 0
+template <int N>
+__device__ __forceinline__ void block_sum_spread_to0(double (&x)[N], double *scratch) {
+  const double t = warp_spread_sum<N>(x);
+  constexpr int S = spread_shift<N>();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if ((lane & ((1 << S) - 1)) == 0 && (lane >> S) < N) scratch[(lane >> S) * nw + warp] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+      double s = 0.0;
+      for (int w = 0; w < nw; ++w) s += scratch[k * nw + w];
+      x[k] = s;
+    }
+  }
+}
+
 // (h, b) pairs stored as double2 or float2
 template <typename T> struct Store;
 template <> struct Store<double> {

@@ -87,6 +87,15 @@ template <> struct FaceShape<float, 1> { static constexpr int nt = 128, minb = 5
 template <> struct FaceShape<float, 2> { static constexpr int nt = 128, minb = 4; };
 template <> struct FaceShape<float, 3> { static constexpr int nt = 256, minb = 3; };
 template <> struct FaceShape<float, 4> { static constexpr int nt = 256, minb = 2; };
+// launch shapes of the mixed moments sweep (a face per warp): warps per CTA x
+// CTAs per SM
+template <int V> struct MomentsShape;
+template <> struct MomentsShape<1> { static constexpr int wpc = 4, minb = 5; };
+template <> struct MomentsShape<2> { static constexpr int wpc = 4, minb = 4; };
+template <> struct MomentsShape<3> { static constexpr int wpc = 8, minb = 3; };
+template <> struct MomentsShape<4> { static constexpr int wpc = 4, minb = 6; };
+// and of the mixed flux sweep
+constexpr int FLUX_WPC = 4, FLUX_MINB = 5;
 static_assert(FaceShape<double, 1>::minb == FACE_MIN_BLOCKS && FaceShape<double, 4>::nt == FACE_WIDE_THREADS &&
                   FaceShape<float, 1>::minb == FACE_MIN_BLOCKS_F32 && FaceShape<float, 4>::minb == FACE_MIN_BLOCKS_WIDE_F32,
               "variants 1 and 4 are the narrow and wide default shapes");
@@ -919,7 +928,7 @@ __device__ __forceinline__ void face_item_fp64(const ugks_fused_block *__restric
 
   if (wall < 0) {
     // ---------------- interior face ----------------
-    block_sum<4>(m, sh.scratch);
+    block_sum_spread<4>(m, sh.scratch);
     const P4 W = p4(m[0], m[1], m[2], 0.5 * m[3]);
     Rcp rc;
     const P4 prim = to_primary_rcp(d, W, rc);  // getPLR (clUGKS.c:421-422), every thread
@@ -948,7 +957,7 @@ __device__ __forceinline__ void face_item_fp64(const ugks_fused_block *__restric
         axis_exp(Ev, d.quad, vn, 1, 1, Ug.y, prim.s3, t, nt);
       }
     });
-    block_sum<2>(q, sh.scratch);
+    block_sum_spread<2>(q, sh.scratch);
     // ---- sweep 3: macroFlux (587-681) and distFlux (683-772).
     // With h0 = weight * fM (times the face length), kb = K / (2 lambda),
     // S = Mt0 s (c . Q) (the Shakhov factor of fS, clFunctions.c:64-77, times
@@ -1006,7 +1015,7 @@ __device__ __forceinline__ void face_item_fp64(const ugks_fused_block *__restric
       acc[4] += Zb;
       St::store(flux, base + v, v2(hx, hy));
     }
-    block_sum_to0<5>(acc, sh.scratch);
+    block_sum_spread_to0<5>(acc, sh.scratch);
     if (threadIdx.x == 0) {
       P4 out = p4(acc[0] + c[18], acc[1] + c[19], acc[2] + c[20], 0.5 * (acc[3] + acc[4]) + c[21]);
       const V2 g = to_global(v2(out.s1, out.s2), n);
@@ -1630,27 +1639,40 @@ cudaError_t set_face_attributes() {
                                        200 * 1024);
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(face_retry<T, FM, MINB, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-  // FP64 keeps the face's velocities in shared memory; the mixed moments
-  // pass needs only axis tables and reads its stencils through L1
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(face_pass<T, FM, MINB, NT>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             std::is_same<T, float>::value ? (int)cudaSharedmemCarveoutMaxL1
-                                                           : (int)cudaSharedmemCarveoutMaxShared);
+                             cudaSharedmemCarveoutMaxShared);
   return e;
 }
 
 template <typename T, int V>
 cudaError_t set_face_shape() {
   constexpr int NT = FaceShape<T, V>::nt, MINB = FaceShape<T, V>::minb;
-  cudaError_t e = set_face_attributes<T, 0, MINB, NT>();
-  if (e == cudaSuccess) e = set_face_attributes<T, 1, MINB, NT>();
-  if (e == cudaSuccess) e = set_face_attributes<T, 3, MINB, NT>();
-  return e;
+  if constexpr (std::is_same<T, float>::value) {
+    return cudaSuccess;  // mixed: no face_pass (set_wall_attributes covers its retry pass)
+  } else {
+    cudaError_t e = set_face_attributes<T, 0, MINB, NT>();
+    if (e == cudaSuccess) e = set_face_attributes<T, 1, MINB, NT>();
+    if (e == cudaSuccess) e = set_face_attributes<T, 3, MINB, NT>();
+    return e;
+  }
 }
 template <typename T>
 cudaError_t set_wall_attributes() {
-  if constexpr (std::is_same<T, float>::value)
-    return cudaFuncSetAttribute(wall_pass_delta<WALL_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+  if constexpr (std::is_same<T, float>::value) {
+    // the wall launch and the retry pass's wall faces (both budgets)
+    cudaError_t e =
+        cudaFuncSetAttribute(wall_pass_delta<WALL_NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    constexpr int NN = FT, NW = FaceBudget<float>::wide_threads;
+    constexpr int MN = FaceBudget<float>::narrow, MW = FaceBudget<float>::wide;
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(face_retry<float, 0, MN, NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(face_retry<float, 1, MN, NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(face_retry<float, 3, MN, NN>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(face_retry<float, 0, MW, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(face_retry<float, 1, MW, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(face_retry<float, 3, MW, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    return e;
+  }
   return cudaSuccess;
 }
 template <typename T, int MINB>
@@ -1684,11 +1706,11 @@ cudaError_t set_step_attributes() {
 }
 
 // shared memory of a face CTA: FP64, (h, b) and slopes per velocity + axis
-// tables; mixed, the axis velocities of an interior face, or (wall faces of
-// the retry pass) the wall procedure's FP64 face values
+// tables; mixed, the wall procedure's FP64 face values (retry pass; the
+// mixed main pass sizes its warp sweeps itself)
 template <typename T>
 inline size_t face_smem(int max_nv, int max_axes, bool retry = false) {
-  if (std::is_same<T, float>::value) return retry ? delta_wall_smem(max_nv) : delta_face_smem(max_axes);
+  if (std::is_same<T, float>::value) return retry ? delta_wall_smem(max_nv) : 0;
   return 4 * sizeof(double) * (size_t)max_nv + sizeof(double) * (size_t)max_axes;
 }
 
@@ -1714,6 +1736,30 @@ void launch_retry(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, 
   if (z->face_count[3]) face_retry<T, 3, MINB, NT><<<rg, NT, smem, st>>>(B, nb, solves, ns);
 }
 
+// the mixed moments sweep of one segment, in launch shape v (ugks_fused_sizes.seg_variant)
+template <int WPC, int MINB>
+void launch_moments_shape(const ugks_fused_block *B, int nb, ugks_solve_state *solves, int method, int first,
+                          int count, int axes, cudaStream_t st) {
+  const int ws = delta_moments_stride(axes);
+  const unsigned g = (unsigned)((count + WPC - 1) / WPC);
+  const size_t sm = (size_t)WPC * ws * sizeof(double);
+  switch (method) {
+    case 0: face_moments_warp<0, WPC, MINB><<<g, WPC * 32, sm, st>>>(B, nb, solves, first, count, ws); break;
+    case 1: face_moments_warp<1, WPC, MINB><<<g, WPC * 32, sm, st>>>(B, nb, solves, first, count, ws); break;
+    case 3: face_moments_warp<3, WPC, MINB><<<g, WPC * 32, sm, st>>>(B, nb, solves, first, count, ws); break;
+    default: break;
+  }
+}
+inline void launch_moments(int v, const ugks_fused_block *B, int nb, ugks_solve_state *solves, int method,
+                           int first, int count, int axes, cudaStream_t st) {
+  switch (v) {
+    case 2: launch_moments_shape<MomentsShape<2>::wpc, MomentsShape<2>::minb>(B, nb, solves, method, first, count, axes, st); break;
+    case 3: launch_moments_shape<MomentsShape<3>::wpc, MomentsShape<3>::minb>(B, nb, solves, method, first, count, axes, st); break;
+    case 4: launch_moments_shape<MomentsShape<4>::wpc, MomentsShape<4>::minb>(B, nb, solves, method, first, count, axes, st); break;
+    default: launch_moments_shape<MomentsShape<1>::wpc, MomentsShape<1>::minb>(B, nb, solves, method, first, count, axes, st); break;
+  }
+}
+
 template <typename T>
 int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks_solve_state *solves,
               int ns, void *stream, void *const *events = nullptr) {
@@ -1737,13 +1783,18 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
     if (z->seg_count[k] <= 0) continue;
     const size_t sm = face_smem<T>(z->seg_max_nv[k], z->seg_max_axes[k]);
     int v = z->seg_variant[k];
-    if (v <= 0 || v > 4) v = z->seg_max_nv[k] <= FaceBudget<T>::narrow_max_nv ? 1 : 4;
     const int m = z->seg_method[k], b0 = z->seg_begin[k], n = z->seg_count[k];
-    switch (v) {
-      case 1: launch_segment<T, FaceShape<T, 1>::minb, FaceShape<T, 1>::nt>(B, nb, solves, m, b0, n, sm, st); break;
-      case 2: launch_segment<T, FaceShape<T, 2>::minb, FaceShape<T, 2>::nt>(B, nb, solves, m, b0, n, sm, st); break;
-      case 3: launch_segment<T, FaceShape<T, 3>::minb, FaceShape<T, 3>::nt>(B, nb, solves, m, b0, n, sm, st); break;
-      default: launch_segment<T, FaceShape<T, 4>::minb, FaceShape<T, 4>::nt>(B, nb, solves, m, b0, n, sm, st); break;
+    if constexpr (mixed) {
+      if (v <= 0 || v > 4) v = 1;
+      launch_moments(v, B, nb, solves, m, b0, n, z->seg_max_axes[k], st);
+    } else {
+      if (v <= 0 || v > 4) v = z->seg_max_nv[k] <= FaceBudget<T>::narrow_max_nv ? 1 : 4;
+      switch (v) {
+        case 1: launch_segment<T, FaceShape<T, 1>::minb, FaceShape<T, 1>::nt>(B, nb, solves, m, b0, n, sm, st); break;
+        case 2: launch_segment<T, FaceShape<T, 2>::minb, FaceShape<T, 2>::nt>(B, nb, solves, m, b0, n, sm, st); break;
+        case 3: launch_segment<T, FaceShape<T, 3>::minb, FaceShape<T, 3>::nt>(B, nb, solves, m, b0, n, sm, st); break;
+        default: launch_segment<T, FaceShape<T, 4>::minb, FaceShape<T, 4>::nt>(B, nb, solves, m, b0, n, sm, st); break;
+      }
     }
   }
   if (mixed && z->n_wall)
@@ -1758,7 +1809,9 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
   else launch_retry<T, FaceBudget<T>::wide, FaceBudget<T>::wide_threads>(B, nb, z, solves, ns, smem, st);
   if (mixed && z->n_faces) {
     face_coef_delta<<<(unsigned)((z->n_faces + 127) / 128), 128, 0, st>>>(B, nb, solves, z->n_faces);
-    face_flux_delta<FLUX_NT><<<(unsigned)z->n_faces, FLUX_NT, delta_flux_smem(z->max_axes), st>>>(B, nb, solves, 0);
+    const int fs = delta_flux_stride(z->max_axes);
+    face_flux_warp<FLUX_WPC, FLUX_MINB><<<(unsigned)((z->n_faces + FLUX_WPC - 1) / FLUX_WPC), FLUX_WPC * 32,
+                                          (size_t)FLUX_WPC * fs * sizeof(double), st>>>(B, nb, solves, z->n_faces, fs);
   }
   if (mixed) {
     mark(1);
@@ -1830,7 +1883,8 @@ __global__ void stop_check(ugks_solve_state *solves, int ns) {
   if (!x.active) return;
   int why = 0;
   if (x.status != 0) why = UGKS_STOP_ERROR;
-  else if (x.stop_residual > 0.0 && x.residual[0] < x.stop_residual) why = UGKS_STOP_CONVERGED;
+  else if (x.stop_residual > 0.0 && x.steps >= x.stop_after && x.residual[0] < x.stop_residual)
+    why = UGKS_STOP_CONVERGED;
   else if (x.stop_steps > 0 && x.steps >= x.stop_steps) why = UGKS_STOP_STEPS;
   if (why) {
     x.stopped = why;

@@ -368,16 +368,19 @@ class FusedSolver:
                for x in arr]
         return [out[self.order[k]] for k in range(self.nsolves)]
 
-    def set_stop_rule(self, solve: int, tol: float = 0.0, max_steps: int = 0):
+    def set_stop_rule(self, solve: int, tol: float = 0.0, max_steps: int = 0, start: int = 10):
         """The device-side stop rule of the caller's solve (ugks_stop_check):
-        stop when the density residual falls below tol or after max_steps
-        steps (0 disables either)."""
+        stop when the density residual falls below tol once at least `start`
+        steps are done (the reference's residual_start: a solve that starts
+        from rest changes its density by round-off in its first steps), or
+        after max_steps steps (0 disables either)."""
         torch = _torch()
         torch.cuda.synchronize(self.device)
         st = (_lib.SolveState * self.nsolves).from_buffer_copy(self.solves.cpu().numpy().tobytes())
         s = self.order[solve]
         st[s].stop_residual = float(tol)
         st[s].stop_steps = int(max_steps)
+        st[s].stop_after = int(start)
         self.solves.copy_(torch.from_numpy(np.frombuffer(bytes(st), dtype=np.uint8).copy()))
 
     def set_active(self, flags):

@@ -96,12 +96,12 @@ class SolvePool:
         self._graph = None            # (steps per tick, CUDAGraph) of the current membership
 
     # -------------------------------------------------------------- membership
-    def admit(self, case, tol=0.0, max_steps=0) -> int:
+    def admit(self, case, tol=0.0, max_steps=0, start=10) -> int:
         """Allocate and initialise a solve with its stop rule (density
-        residual below tol, or max_steps steps; 0 disables either); returns
-        its id."""
+        residual below tol from `start` steps on, or max_steps steps; 0
+        disables either); returns its id."""
         solver = FusedSolver(case, precision=self.precision, device=self.device)
-        solver.set_stop_rule(0, tol, max_steps)
+        solver.set_stop_rule(0, tol, max_steps, start)
         sid = self._next
         self._next += 1
         s = _Solve(sid, case, solver)

@@ -35,8 +35,11 @@ STEPS = 3
 def _oracle(case, backend):
     if backend == "ref":
         c = ugks_setup.Constants(case)
-        if not all(programs.reference_available(c, b, k) for k, b in enumerate(case["blocks"])):
-            pytest.skip("compiled reference for this case not available")
+        # the reference's kernels for these cases are built by
+        # __graft_entry__.build() into oracle/_ref, which ships with the tree:
+        # a missing build is a packaging error, not a reason to skip
+        assert all(programs.reference_available(c, b, k) for k, b in enumerate(case["blocks"])), \
+            "compiled reference for this case not built (run __graft_entry__.build())"
         return host.OracleSim(case, "ref", threads=os.cpu_count())
     return host.OracleSim(case, "port")
 
@@ -62,7 +65,8 @@ def _compare(name, fields, fs, dt, time, ora):
 
 CASES = {
     "config2_bench": (lambda: bench.workload("multiblock")[0][0], "ref"),
-    "config4_langmuir": (lambda: configs.channel(nblocks=4, n=64, m=32, Kn=0.05, k_des=0.0), "ref"),
+    "config4_langmuir": (lambda: configs.channel(nblocks=4, n=64, m=32, Kn=0.05, k_des=0.0,
+                                                 CFL=configs.WORKLOAD_CFL), "ref"),
     "config4_first_order": (lambda: bench.workload("channel")[0][0], "port"),
 }
 

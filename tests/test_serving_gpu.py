@@ -82,13 +82,16 @@ def test_device_stop_rule(cuda):
     in the table go on, unperturbed."""
     pool = SolvePool("fp64")
     capped = pool.admit(configs.cavity(n=8, m=8, vlim=4.0), max_steps=7)
-    loose = pool.admit(configs.cavity(n=10, m=8, vlim=4.0), tol=1e-1)
+    loose = pool.admit(configs.cavity(n=10, m=8, vlim=4.0), tol=1e-1, start=3)
+    early = pool.admit(configs.cavity(n=10, m=8, vlim=4.0), tol=1e3, start=6)
     free = pool.admit(configs.cavity(n=8, m=12, vlim=5.0, flux_method="WENO5"))
     pool.tick(5)
     pool.tick(5)
     st = pool.states()
     assert st[capped]["steps"] == 7 and st[capped]["stopped"] == 2 and not st[capped]["active"]
-    assert st[loose]["stopped"] == 1 and st[loose]["residual"][0] < 1e-1 and st[loose]["steps"] < 10
+    assert st[loose]["stopped"] == 1 and st[loose]["residual"][0] < 1e-1 and 3 <= st[loose]["steps"] < 10
+    # below its tolerance from the first step, but the rule starts at step 6
+    assert st[early]["stopped"] == 1 and st[early]["steps"] == 6
     assert st[free]["steps"] == 10 and st[free]["stopped"] == 0
     for x, y in zip(pool.interior_f(free), solo(configs.cavity(n=8, m=12, vlim=5.0, flux_method="WENO5"), 10)):
         np.testing.assert_array_equal(x, y)
