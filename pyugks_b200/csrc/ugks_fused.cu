@@ -95,18 +95,24 @@ template <> struct MomentsShape<2> { static constexpr int wpc = 4, minb = 4; };
 template <> struct MomentsShape<3> { static constexpr int wpc = 8, minb = 3; };
 template <> struct MomentsShape<4> { static constexpr int wpc = 4, minb = 6; };
 // and of the mixed flux sweep
-constexpr int FLUX_WPC = 4, FLUX_MINB = 5;
+// 7 CTAs (28 warps) per SM at 72 registers: 0.617 -> 0.598 ms of face pass on
+// the 2x2-block cavity, 13.0 -> 12.2 ms on the 64-solve batch, against 5
+#ifndef UGKS_FLUX_MINB
+#define UGKS_FLUX_MINB 7
+#endif
+constexpr int FLUX_WPC = 4, FLUX_MINB = UGKS_FLUX_MINB;
 static_assert(FaceShape<double, 1>::minb == FACE_MIN_BLOCKS && FaceShape<double, 4>::nt == FACE_WIDE_THREADS &&
                   FaceShape<float, 1>::minb == FACE_MIN_BLOCKS_F32 && FaceShape<float, 4>::minb == FACE_MIN_BLOCKS_WIDE_F32,
               "variants 1 and 4 are the narrow and wide default shapes");
 
 // CTAs of 8 cell warps per SM: FP64 at 128 registers (at 80 the update loop
-// spills and the pass is 12% slower), FP32 storage at 80 (6% faster than 128)
+// spills and the pass is 12% slower), mixed at 80 (3 CTAs: 0.215 against
+// 0.222 ms at 120 registers on the 2x2-block cavity)
 #ifndef CELL_MIN_BLOCKS
 #define CELL_MIN_BLOCKS 2
 #endif
 #ifndef CELL_MIN_BLOCKS_F32
-#define CELL_MIN_BLOCKS_F32 2
+#define CELL_MIN_BLOCKS_F32 3
 #endif
 // ...and the depth of the per-warp ring of asynchronous copies that stream
 // the f and flux rows of the cell update into shared memory
@@ -1686,6 +1692,31 @@ cudaError_t set_cell_attributes() {
 // cell passes of large velocity grids need) hold per device: they are set
 // once for each device a step runs on, with that device current.
 constexpr int kMaxDevices = 64;
+
+// The mixed step's wall launch needs only this step's f and writes only wall
+// faces, so it runs on a side stream beside the interior moments sweep: a
+// fork and a join by events, which stream capture turns into graph edges.
+// One side stream per device, created with the device's kernel attributes
+// (before any capture: ugks_prepare); `lock` keeps the record-wait pairs of
+// concurrent host threads from interleaving.
+struct WallStream {
+  cudaStream_t s = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+  std::mutex lock;
+};
+inline WallStream &wall_stream(int dev) {
+  static WallStream ws[kMaxDevices];
+  return ws[dev];
+}
+inline cudaError_t make_wall_stream(int dev) {
+  WallStream &w = wall_stream(dev);
+  if (w.s) return cudaSuccess;
+  cudaError_t e = cudaStreamCreateWithFlags(&w.s, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w.fork, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w.join, cudaEventDisableTiming);
+  return e;
+}
+
 template <typename T>
 cudaError_t set_step_attributes() {
   static std::mutex lock;
@@ -1701,6 +1732,10 @@ cudaError_t set_step_attributes() {
       set_cell_attributes<T, 2>(), set_cell_attributes<T, 3>(), set_wall_attributes<T>()};
   for (cudaError_t x : r)
     if (x != cudaSuccess) return x;
+  if (std::is_same<T, float>::value) {
+    e = make_wall_stream(dev);
+    if (e != cudaSuccess) return e;
+  }
   done[dev] = true;
   return cudaSuccess;
 }
@@ -1779,6 +1814,20 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
     if (events) cudaEventRecord(reinterpret_cast<cudaEvent_t>(events[k]), st);
   };
   mark(0);
+  // mixed: the wall faces on the device's side stream, beside the segments
+  WallStream *ws = nullptr;
+  std::unique_lock<std::mutex> ws_guard;
+  if (mixed && z->n_wall) {
+    int dev = 0;
+    const cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return -(int)e;
+    ws = &wall_stream(dev);
+    ws_guard = std::unique_lock<std::mutex>(ws->lock);
+    cudaEventRecord(ws->fork, st);
+    cudaStreamWaitEvent(ws->s, ws->fork, 0);
+    wall_pass_delta<WALL_NT><<<(unsigned)z->n_wall, WALL_NT, delta_wall_smem(z->max_nv), ws->s>>>(B, nb, solves);
+    cudaEventRecord(ws->join, ws->s);
+  }
   for (int k = 0; k < z->n_segments && k < UGKS_MAX_FACE_SEGMENTS; ++k) {
     if (z->seg_count[k] <= 0) continue;
     const size_t sm = face_smem<T>(z->seg_max_nv[k], z->seg_max_axes[k]);
@@ -1797,8 +1846,10 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
       }
     }
   }
-  if (mixed && z->n_wall)
-    wall_pass_delta<WALL_NT><<<(unsigned)z->n_wall, WALL_NT, delta_wall_smem(z->max_nv), st>>>(B, nb, solves);
+  if (ws) {
+    cudaStreamWaitEvent(st, ws->join, 0);
+    ws_guard.unlock();
+  }
   const bool narrow = z->max_nv <= FaceBudget<T>::narrow_max_nv;
   // mixed: the interior faces' coefficient and flux launches follow the first
   // dt check (they use its dt), and the events bracket all of the face pass
