@@ -340,7 +340,8 @@ typedef struct ugks_solve_state {
   unsigned long long max_freq; /* bits of the running max CFL frequency (atomicMax) */
   int32_t retry;               /* 1 while this step's flux pass is redone   */
   int32_t status;              /* 0 ok, 1 NaN in f, 4 isotherm, 6 bad block
-                                  connection (clError.c codes otherwise) */
+                                  connection (clError.c codes otherwise), 8 a bulk
+                                  copy of the face pass outlived its wait bound */
   int32_t steps;               /* completed steps                           */
   int32_t retries;             /* flux passes redone so far                 */
   int32_t active;              /* 0: skipped by every fused kernel          */

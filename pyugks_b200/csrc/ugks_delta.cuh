@@ -663,6 +663,199 @@ __global__ void __launch_bounds__(WPC * 32, MINB) face_flux_warp(const ugks_fuse
   }
 }
 
+// ---------------------------------------------------------------------------
+// the flux sweep with its rows staged by the bulk-copy engine: a face per
+// warp, its stored face values and slopes copied into shared memory in chunks
+// of FLUX_CHUNK pairs, two chunks in flight (the copy of chunk c + 1 runs
+// while the lanes work on chunk c; the first overlaps the axis tables)
+// ---------------------------------------------------------------------------
+#ifndef UGKS_FLUX_CHUNK
+#define UGKS_FLUX_CHUNK 128
+#endif
+constexpr int FLUX_CHUNK = UGKS_FLUX_CHUNK;
+static_assert(FLUX_CHUNK % 32 == 0, "whole trips of a warp per chunk");
+constexpr uint32_t kCopyWaitPolls = 1u << 24;  // about 0.7 s
+constexpr int STATUS_COPY_TIMEOUT = 8;
+// bytes of shared memory per warp: two barriers, two chunk buffers (values and
+// slopes), the face record and the axis tables
+inline size_t flux_tma_warp_bytes(int max_axes) {
+  return 16 + 2 * 2 * (size_t)FLUX_CHUNK * 16 + 48 * 8 + (((size_t)12 * (max_axes + 2) + 15) & ~(size_t)15);
+}
+
+template <int WPC, int MINB>
+__global__ void __launch_bounds__(WPC * 32, MINB) face_flux_tma(const ugks_fused_block *__restrict__ B, int nb,
+                                                                ugks_solve_state *__restrict__ solves,
+                                                                int n_faces, int wbytes) {
+  extern __shared__ __align__(128) unsigned char dyn_b[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int item = (int)blockIdx.x * WPC + warp;
+  if (item >= n_faces) return;
+  FaceWork fwk;
+  if (!face_work<-1>(B, nb, solves, item, 0, fwk) || fwk.wall >= 0) return;
+  const ugks_fused_block &blk = B[fwk.bi];
+  const ugks_block_desc &d = blk.d;
+  const int dir = fwk.dir;
+  const long gi = fwk.gi, gj = fwk.gj;
+  const int NP = npairs(d), un = d.u_num, vn = d.v_num;
+  const RefMaxwellian ref = ref_of(blk);
+  const size_t fk = faceidx(d, gi, gj, dir);
+  const double *rec = blk.face_rec + (size_t)UGKS_FACE_REC * fk;
+  const V2 n = ld2(blk.normal, fk);
+  const double len = blk.side_length[fk];
+  // this warp's shared memory
+  unsigned char *wm = dyn_b + (size_t)warp * wbytes;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(wm);
+  float4 *buf = reinterpret_cast<float4 *>(wm + 16);  // [2][values | slopes][FLUX_CHUNK]
+  double *fc = reinterpret_cast<double *>(buf + 4 * FLUX_CHUNK);
+  float2 *EAU = reinterpret_cast<float2 *>(fc + 48), *EAV = EAU + (un + 1);  // (expm1 table, axis factor)
+  float *QX = reinterpret_cast<float *>(EAV + vn), *QY = QX + (un + 1);
+  const float4 *EAU2 = reinterpret_cast<const float4 *>(EAU);
+  const float2 *QX2 = reinterpret_cast<const float2 *>(QX);
+  float4 *frow = reinterpret_cast<float4 *>(dir == SOUTH ? blk.flux_S : blk.flux_W) + pidx(d, gi, gj, 0);
+  const float4 *arow = reinterpret_cast<const float4 *>(dir == SOUTH ? blk.aux_S : blk.aux_W) + pidx(d, gi, gj, 0);
+  const int nchunks = (NP + FLUX_CHUNK - 1) / FLUX_CHUNK;
+  auto issue = [&](int c) {  // lane 0: the copies of chunk c into buffer c & 1
+    const int p0 = c * FLUX_CHUNK, m = min(FLUX_CHUNK, NP - p0);
+    const uint32_t bytes = (uint32_t)m * 16u;
+    float4 *dst = buf + (c & 1) * 2 * FLUX_CHUNK;
+    mbar_arrive_expect_tx(&bar[c & 1], 2u * bytes);
+    bulk_g2s(dst, frow + p0, bytes, &bar[c & 1]);
+    bulk_g2s(dst + FLUX_CHUNK, arow + p0, bytes, &bar[c & 1]);
+  };
+  if (lane == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+    issue(0);
+  }
+  fc[lane] = rec[lane];
+  if (lane < 16) fc[32 + lane] = rec[32 + lane];
+  __syncwarp();
+  {
+    // expm1 axis tables of the face Maxwellian against M, its axis factors
+    // (the face length on the u axis) and the axis velocities; entry un is
+    // the padding lane's: 0
+    const double lam = fc[FR_LAM], Ugx = fc[FR_UGX], Ugy = fc[FR_UGY], lnP = fc[FR_LNP];
+    for (int k = lane; k <= un + vn; k += 32) {
+      if (k < un) {
+        const double x = d.quad[2 * (size_t)k * vn];
+        EAU[k] = make_float2((float)axis_expm1(x, Ugx, lam, ref.lam0, lnP), (float)(ref.Au[k] * len));
+        QX[k] = (float)x;
+      } else if (k == un) {
+        EAU[k] = make_float2(0.0f, 0.0f);
+        QX[k] = 0.0f;
+      } else {
+        const int j = k - un - 1;
+        const double y = d.quad[2 * (size_t)j + 1];
+        EAV[j] = make_float2((float)axis_expm1(y, Ugy, lam, ref.lam0), (float)ref.Av[j]);
+        QY[j] = (float)y;
+      }
+    }
+  }
+  __syncwarp();
+  const double *c = fc + FR_C;
+  const double Mt0 = c[15];
+  const float2 nx2 = bc2((float)n.x), ny2 = bc2((float)n.y), mny2 = bc2(-(float)n.y);
+  const float2 fUx = bc2((float)fc[FR_UX]), fUy = bc2((float)fc[FR_UY]), flam2 = bc2((float)(2.0 * fc[FR_LAM]));
+  const float2 fsx = bc2((float)fc[FR_SX]), fsy = bc2((float)fc[FR_SY]);
+  const float2 fkb = bc2((float)fc[FR_KB]), fdkb = bc2((float)(fc[FR_KB] - ref.kb0));
+  const float2 fMt0 = bc2((float)Mt0), fMt3L = bc2((float)c[16]), fnMt4L = bc2((float)(-c[17]));
+  const float2 fT0 = bc2((float)(c[10] - Mt0)), fT1 = bc2((float)c[11]), fT2 = bc2((float)c[12]);
+  const float2 fT3 = bc2((float)c[13]), fCT = bc2((float)c[14]);
+  const float2 AR0 = bc2((float)c[5]), AR1 = bc2((float)c[6]), AR2 = bc2((float)c[7]), AR3 = bc2((float)c[8]);
+  const float2 AR4 = bc2((float)c[9]);
+  const float2 dA0 = bc2((float)(c[0] - c[5])), dA1 = bc2((float)(c[1] - c[6])), dA2 = bc2((float)(c[2] - c[7]));
+  const float2 dA3 = bc2((float)(c[3] - c[8])), dA4 = bc2((float)(c[4] - c[9]));
+  float2 acc[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) acc[k] = make_float2(0.0f, 0.0f);
+  bool ok = true;
+  for (int ch = 0; ch < nchunks; ++ch) {
+    if (lane == 0 && ch + 1 < nchunks) {
+      fence_proxy_async_smem();  // the lanes' reads of that buffer (chunk ch - 1) came first
+      issue(ch + 1);
+    }
+    // every lane observes the completion itself (its acquire of the copied
+    // rows); a lane that ran out of polls stops the whole warp
+    ok = __all_sync(0xffffffffu, mbar_wait(&bar[ch & 1], (uint32_t)((ch >> 1) & 1), kCopyWaitPolls));
+    if (!ok) break;
+    const float4 *bv = buf + (ch & 1) * 2 * FLUX_CHUNK, *bs = bv + FLUX_CHUNK;
+    const int p0 = ch * FLUX_CHUNK, m = min(FLUX_CHUNK, NP - p0);
+    int ia = (p0 + lane) / vn, jv = (p0 + lane) % vn;
+    const int qs = 32 / vn, rs = 32 % vn;
+#pragma unroll 1
+    for (int q = lane; q < m; q += 32) {
+      const float4 fd = bv[q], sg = bs[q];
+      const float4 eu = EAU2[ia];
+      const float2 ev = EAV[jv];
+      const float2 qx = QX2[ia], qy = bc2(QY[jv]);
+      const float2 U = fma2(qx, nx2, mul2(qy, ny2)), T = fma2(qy, nx2, mul2(qx, mny2));
+      const float2 r = rel_excess(make_float2(eu.x, eu.z), bc2(ev.x));
+      const float2 ml = mul2(make_float2(eu.y, eu.w), bc2(ev.y));  // len M
+      const float2 h0 = fma2(ml, r, ml);
+      const float2 uu = fma2(U, U, mul2(T, T));
+      const float2 cx = sub2(U, fUx), cy = sub2(T, fUy), c2 = fma2(cx, cx, mul2(cy, cy));
+      const float2 Sp = fma2(cx, fsx, mul2(cy, fsy));
+      const float2 S4 = mul2(Sp, fma2(flam2, c2, bc2(-4.0f))), S2 = fma2(bc2(2.0f), Sp, S4);
+      const float2 pos = make_float2(U.x > 0.0f ? 1.0f : 0.0f, U.y > 0.0f ? 1.0f : 0.0f);
+      const float2 MPR = fma2(AR3, uu, fma2(AR2, T, fma2(AR1, U, AR0)));
+      const float2 dMP = fma2(dA3, uu, fma2(dA2, T, fma2(dA1, U, dA0)));
+      const float2 MP = fma2(pos, dMP, MPR), A4 = fma2(pos, dA4, AR4);
+      const float2 Bk = fma2(U, MP, fma2(fT3, uu, fma2(fT2, T, fma2(fT1, U, fT0))));  // B - Mt0
+      const float2 mu = mul2(fnMt4L, U);
+      const float2 Rh = fma2(mu, lo2(sg), mul2(fMt3L, lo2(fd))), Rb = fma2(mu, hi2(sg), mul2(fMt3L, hi2(fd)));
+      const float2 Zh = mul2(U, fma2(S4, h0, Rh)), Zb = mul2(U, fma2(mul2(S2, fkb), h0, Rb));
+      const float2 uh = mul2(U, h0), um0 = mul2(mul2(U, ml), fMt0);
+      const float2 hx = fma2(uh, Bk, fma2(um0, r, Zh));
+      const float2 hy = fma2(uh, fma2(fkb, Bk, fma2(A4, U, fCT)), fma2(um0, fma2(fkb, r, fdkb), Zb));
+      acc[0] = add2(acc[0], Zh);
+      acc[1] = fma2(U, Zh, acc[1]);
+      acc[2] = fma2(T, Zh, acc[2]);
+      acc[3] = fma2(uu, Zh, acc[3]);
+      acc[4] = add2(acc[4], Zb);
+      frow[p0 + q] = cat2(hx, hy);
+      jv += rs;
+      ia += qs;
+      if (jv >= vn) { jv -= vn; ++ia; }
+    }
+    __syncwarp();
+  }
+  if (!ok) {
+    // a copy outlived its bound: flag the solve, give the copies in flight
+    // one more bound, and leave the face
+    if (lane == 0) {
+      atomicExch(&solves[blk.solve].status, STATUS_COPY_TIMEOUT);
+      mbar_wait(&bar[0], 0u, kCopyWaitPolls);
+      mbar_wait(&bar[1], 0u, kCopyWaitPolls);
+    }
+    __syncwarp();
+    return;
+  }
+  double af[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) af[k] = (double)acc[k].x + (double)acc[k].y;
+  const double tw = warp_spread_sum<5>(af);
+  constexpr int S = spread_shift<5>();
+  double da[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) da[k] = __shfl_sync(0xffffffffu, tw, k << S);
+  if (lane == 0) {
+    const double *R = ref.mom;
+    const double nx = n.x, ny = n.y, Mt3L = c[16];
+    const double K0 = nx * R[RM10] + ny * R[RM01];
+    const double K1 = nx * nx * R[RM20] + 2.0 * nx * ny * R[RM11] + ny * ny * R[RM02];
+    const double K2 = -nx * ny * R[RM20] + (nx * nx - ny * ny) * R[RM11] + nx * ny * R[RM02];
+    const double K3 = nx * (R[RM30] + R[RM12]) + ny * (R[RM21] + R[RM03]);
+    const double Kb = nx * R[RB10] + ny * R[RB01];
+    P4 out = p4(da[0] + Mt3L * K0 + c[18], da[1] + Mt3L * K1 + c[19], da[2] + Mt3L * K2 + c[20],
+                0.5 * ((da[3] + Mt3L * K3) + (da[4] + Mt3L * Kb)) + c[21]);
+    const V2 g = to_global(v2(out.s1, out.s2), n);
+    out.s1 = g.x;
+    out.s2 = g.y;
+    st4(dir == SOUTH ? blk.flux_macro_S : blk.flux_macro_W, gidx(d, gi, gj), out);
+  }
+}
+
 // The cell pass stores the new deviation with stochastic rounding: round to
 // nearest is biased where a slowly relaxing solve changes df by less than
 // half an FP32 ulp per step (the stored value stays put while the FP64 one

@@ -101,6 +101,16 @@ template <> struct MomentsShape<4> { static constexpr int wpc = 4, minb = 6; };
 #define UGKS_FLUX_MINB 7
 #endif
 constexpr int FLUX_WPC = 4, FLUX_MINB = UGKS_FLUX_MINB;
+// the flux sweep with bulk-copied rows (face_flux_tma) instead of per-lane
+// loads: 0.598 -> 0.529 ms of face pass on the 2x2-block cavity (the sweep
+// itself 252 -> 169 us under ncu, DRAM 42% -> 62% of peak)
+#ifndef UGKS_FLUX_TMA
+#define UGKS_FLUX_TMA 1
+#endif
+#ifndef UGKS_FLUX_TMA_MINB
+#define UGKS_FLUX_TMA_MINB 5
+#endif
+constexpr int FLUX_TMA_MINB = UGKS_FLUX_TMA_MINB;
 static_assert(FaceShape<double, 1>::minb == FACE_MIN_BLOCKS && FaceShape<double, 4>::nt == FACE_WIDE_THREADS &&
                   FaceShape<float, 1>::minb == FACE_MIN_BLOCKS_F32 && FaceShape<float, 4>::minb == FACE_MIN_BLOCKS_WIDE_F32,
               "variants 1 and 4 are the narrow and wide default shapes");
@@ -1681,6 +1691,18 @@ cudaError_t set_wall_attributes() {
   }
   return cudaSuccess;
 }
+template <typename T>
+cudaError_t set_flux_attributes() {
+  if constexpr (std::is_same<T, float>::value) {
+    cudaError_t e = cudaFuncSetAttribute(face_flux_tma<FLUX_WPC, FLUX_TMA_MINB>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(face_flux_tma<FLUX_WPC, FLUX_TMA_MINB>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                               cudaSharedmemCarveoutMaxShared);
+    return e;
+  }
+  return cudaSuccess;
+}
 template <typename T, int MINB>
 cudaError_t set_cell_attributes() {
   if (std::is_same<T, float>::value)
@@ -1727,9 +1749,9 @@ cudaError_t set_step_attributes() {
   if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> guard(lock);
   if (done[dev]) return cudaSuccess;
-  cudaError_t r[7] = {
+  cudaError_t r[8] = {
       set_face_shape<T, 1>(), set_face_shape<T, 2>(), set_face_shape<T, 3>(), set_face_shape<T, 4>(),
-      set_cell_attributes<T, 2>(), set_cell_attributes<T, 3>(), set_wall_attributes<T>()};
+      set_cell_attributes<T, 2>(), set_cell_attributes<T, 3>(), set_wall_attributes<T>(), set_flux_attributes<T>()};
   for (cudaError_t x : r)
     if (x != cudaSuccess) return x;
   if (std::is_same<T, float>::value) {
@@ -1860,9 +1882,15 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
   else launch_retry<T, FaceBudget<T>::wide, FaceBudget<T>::wide_threads>(B, nb, z, solves, ns, smem, st);
   if (mixed && z->n_faces) {
     face_coef_delta<<<(unsigned)((z->n_faces + 127) / 128), 128, 0, st>>>(B, nb, solves, z->n_faces);
-    const int fs = delta_flux_stride(z->max_axes);
-    face_flux_warp<FLUX_WPC, FLUX_MINB><<<(unsigned)((z->n_faces + FLUX_WPC - 1) / FLUX_WPC), FLUX_WPC * 32,
-                                          (size_t)FLUX_WPC * fs * sizeof(double), st>>>(B, nb, solves, z->n_faces, fs);
+    if (UGKS_FLUX_TMA) {
+      const int wb = (int)flux_tma_warp_bytes(z->max_axes);
+      face_flux_tma<FLUX_WPC, FLUX_TMA_MINB><<<(unsigned)((z->n_faces + FLUX_WPC - 1) / FLUX_WPC), FLUX_WPC * 32,
+                                               (size_t)FLUX_WPC * wb, st>>>(B, nb, solves, z->n_faces, wb);
+    } else {
+      const int fs = delta_flux_stride(z->max_axes);
+      face_flux_warp<FLUX_WPC, FLUX_MINB><<<(unsigned)((z->n_faces + FLUX_WPC - 1) / FLUX_WPC), FLUX_WPC * 32,
+                                            (size_t)FLUX_WPC * fs * sizeof(double), st>>>(B, nb, solves, z->n_faces, fs);
+    }
   }
   if (mixed) {
     mark(1);
