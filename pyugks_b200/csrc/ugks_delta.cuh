@@ -674,7 +674,7 @@ __global__ void __launch_bounds__(WPC * 32, MINB) face_flux_warp(const ugks_fuse
 #endif
 constexpr int FLUX_CHUNK = UGKS_FLUX_CHUNK;
 static_assert(FLUX_CHUNK % 32 == 0, "whole trips of a warp per chunk");
-constexpr uint32_t kCopyWaitPolls = 1u << 24;  // about 0.7 s
+constexpr uint32_t kCopyWaitPolls = UGKS_MBAR_TRY_WAIT ? 1u << 20 : 1u << 24;  // about 1 s
 constexpr int STATUS_COPY_TIMEOUT = 8;
 // bytes of shared memory per warp: two barriers, two chunk buffers (values and
 // slopes), the face record and the axis tables

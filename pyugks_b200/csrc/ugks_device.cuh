@@ -500,11 +500,24 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
                : "memory");
 }
 // true once the barrier's phase of the given parity has completed; false
-// after `limit` polls (about 40 ns apart)
+// after `limit` waits.  UGKS_MBAR_TRY_WAIT: each wait is a try_wait that
+// suspends the thread for at most about a microsecond; else a test_wait poll
+// followed by a 32 ns sleep.
+#ifndef UGKS_MBAR_TRY_WAIT
+#define UGKS_MBAR_TRY_WAIT 1
+#endif
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit) {
   const uint32_t a = smem_u32(bar);
   for (uint32_t i = 0; i < limit; ++i) {
     uint32_t done;
+#if UGKS_MBAR_TRY_WAIT
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(parity), "r"(1000u)
+        : "memory");
+    if (done) return true;
+#else
     asm volatile(
         "{\n\t.reg .pred p;\n\tmbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(done)
@@ -512,6 +525,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32
         : "memory");
     if (done) return true;
     __nanosleep(32);
+#endif
   }
   return false;
 }
