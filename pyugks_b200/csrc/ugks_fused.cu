@@ -354,7 +354,21 @@ __device__ __forceinline__ void reconstruct(const typename Store<T>::vec *p, int
 // the weights only enter as ratios, the largest scaled e_k is >= 1/3 and the
 // smallest >= 1e-17, so the weight of the smoothest stencil stays a normal
 // FP32 number (>= 1e-35) while only negligible weights can underflow.
-__device__ __forceinline__ float frcp(float x) { return __fdividef(1.0f, x); }
+// 1 / x by the hardware's approximate reciprocal (rcp.approx.ftz.f32, within
+// about an ulp; denormal results flush to zero): the FP32 limiter and WENO5
+// weights divide only by sums that are at least 1e-16 or normalised to 1
+#ifndef UGKS_FRCP_APPROX
+#define UGKS_FRCP_APPROX 1
+#endif
+__device__ __forceinline__ float frcp(float x) {
+#if UGKS_FRCP_APPROX
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+#else
+  return __fdividef(1.0f, x);
+#endif
+}
 __device__ __forceinline__ float fsign(float a) {
   return a > 0.0f ? 1.0f : (a < 0.0f ? -1.0f : (a == 0.0f ? a : 0.0f));
 }
