@@ -465,6 +465,15 @@ int ugks_serve_steps(int mixed, const ugks_fused_block *blocks_dev, int nblocks,
    does the same.  Call it before capturing steps in a CUDA graph. */
 int ugks_prepare(int mixed);
 
+/* The bounded wait the mixed face pass puts on its bulk copies
+   (cp.async.bulk on an mbarrier), checked on its own: one warp expects 512
+   bytes and copies them from src_dev (device, 16-byte aligned) or, with
+   src_dev NULL, never does, then waits at most `polls` times (each at most
+   about a microsecond).  *status_dev (device int) becomes 0 when the copy
+   completed and matched, 8 (the solve status of a copy that outlived its
+   bound) when the wait ran out, -1 on a mismatch. */
+int ugks_check_copy_wait(const void *src_dev, unsigned polls, int *status_dev, UGKS_STREAM);
+
 /* ------------------------------------------------------------------------
  * 3. Time-step frequency without device allocation.  No counterpart in the
  *    reference.  For callers that cannot allocate device memory (a host

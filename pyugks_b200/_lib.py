@@ -149,6 +149,8 @@ def lib():
     L.ugks_serve_steps.argtypes = [C.c_int, vp, C.c_int, C.POINTER(FusedSizes), vp, C.c_int, C.c_int, vp]
     L.ugks_prepare.restype = C.c_int
     L.ugks_prepare.argtypes = [C.c_int]
+    L.ugks_check_copy_wait.restype = C.c_int
+    L.ugks_check_copy_wait.argtypes = [vp, C.c_uint, vp, vp]
     L.ugks_getDT_noalloc.restype = C.c_int
     L.ugks_getDT_noalloc.argtypes = [C.POINTER(BlockDesc), vp, vp, vp, f64, vp, vp]
     L.ugks_version.restype = C.c_char_p

@@ -1968,6 +1968,29 @@ __global__ void residual_kernel(const ugks_fused_block *B, int nb, ugks_solve_st
     for (int k = 0; k < 4; ++k) solves[s].residual[k] = n ? r[k] / n : 0.0;
 }
 
+// The bounded wait of the face pass's bulk copies, exercised on its own: a
+// warp arms an mbarrier for 512 bytes and copies them from `src` (global, 16-
+// byte aligned), or, with src null, never does; it then waits at most `polls`
+// times and writes 0 when the copy completed, STATUS_COPY_TIMEOUT when the
+// wait ran out (what the face pass writes into a solve's status)
+__global__ void copy_wait_check(const float4 *src, unsigned polls, int *status) {
+  __shared__ __align__(128) float4 buf[32];
+  __shared__ __align__(8) uint64_t bar;
+  const int lane = threadIdx.x & 31;
+  if (lane == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+    mbar_arrive_expect_tx(&bar, 512u);
+    if (src) bulk_g2s(buf, src, 512u, &bar);
+  }
+  __syncwarp();
+  const bool ok = __all_sync(0xffffffffu, mbar_wait(&bar, 0u, polls));
+  // the copied values read back (a lane's float4 must equal the source's)
+  const bool same = ok && src ? __all_sync(0xffffffffu, buf[lane].x == src[lane].x && buf[lane].w == src[lane].w)
+                              : true;
+  if (lane == 0) *status = !ok ? STATUS_COPY_TIMEOUT : (same ? 0 : -1);
+}
+
 // the stop rule of every active solve (ugks_stop_check)
 __global__ void stop_check(ugks_solve_state *solves, int ns) {
   const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -2039,6 +2062,11 @@ int ugks_serve_steps(int mixed, const ugks_fused_block *blocks_dev, int nblocks,
     if (rc != 0) return rc;
   }
   return 0;
+}
+
+int ugks_check_copy_wait(const void *src_dev, unsigned polls, int *status_dev, void *stream) {
+  copy_wait_check<<<1, 32, 0, S(stream)>>>(reinterpret_cast<const float4 *>(src_dev), polls, status_dev);
+  return launch_status();
 }
 
 int ugks_prepare(int mixed) {

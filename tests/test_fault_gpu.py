@@ -80,3 +80,26 @@ def test_serving_retires_a_failed_request(cuda):
     done = server.run(reqs)
     reasons = {r.id: r.reason for r in done}
     assert reasons == {0: "max_steps", 1: "error", 2: "max_steps"}, reasons
+
+
+def test_bulk_copy_wait_is_bounded(cuda):
+    """The mixed face pass waits on its bulk copies (cp.async.bulk completing
+    on an mbarrier) with a bound: a copy that never comes leaves status 8 and
+    a usable context, a copy that comes is waited for and lands intact.  The
+    wait is made to run out by arming the barrier for bytes nothing sends."""
+    from pyugks_b200 import _lib
+    L = _lib.lib()
+    dev = torch.device("cuda")
+    src = torch.arange(128, dtype=torch.float32, device=dev)  # 512 bytes
+    status = torch.full((1,), 99, dtype=torch.int32, device=dev)
+    stream = torch.cuda.current_stream().cuda_stream
+    _lib.check(L.ugks_check_copy_wait(None, 1000, status.data_ptr(), stream), "ugks_check_copy_wait")
+    torch.cuda.synchronize()
+    assert int(status.item()) == 8
+    _lib.check(L.ugks_check_copy_wait(src.data_ptr(), 1 << 20, status.data_ptr(), stream), "ugks_check_copy_wait")
+    torch.cuda.synchronize()
+    assert int(status.item()) == 0
+    # the context is still usable
+    s = FusedSolver(configs.cavity(n=8, m=8, vlim=4.0), precision="mixed")
+    s.step(2)
+    assert s.solve_state()[0]["status"] == 0
