@@ -317,13 +317,15 @@ class Server:
         return self.done
 
 
-def serve_one_at_a_time(requests, precision="fp64", steps_per_tick=50, device="cuda"):
+def serve_one_at_a_time(requests, precision="fp64", steps_per_tick=50, device="cuda", graphs=True):
     """The comparison arm: the same requests served first come, first served,
-    one solve at a time on the fused step, each to the same stop rule.  A
-    request's service time is its solve's stepping time on the device (CUDA
-    events; set-up excluded); its completion is max(arrival, previous
-    completion) + service, as for a single server working the queue in
-    order.  Returns a dict with per-request latencies and the aggregate
+    one solve at a time on the fused step, each to the same stop rule, with
+    the same tick (steps_per_tick steps, replayed as one CUDA graph when
+    graphs) as the batched server.  A request's service time is its solve's
+    stepping time on the device (CUDA events around its ticks, the graph's
+    capture included; set-up excluded); its completion is max(arrival,
+    previous completion) + service, as for a single server working the queue
+    in order.  Returns a dict with per-request latencies and the aggregate
     cell-velocity updates per second of service."""
     import torch
     dev = torch.device(device)
@@ -335,16 +337,14 @@ def serve_one_at_a_time(requests, precision="fp64", steps_per_tick=50, device="c
     lat, reasons, steps = [], [], []
     stream = torch.cuda.current_stream(dev)
     for r in sorted(requests, key=lambda q: q.arrival):
-        solver = FusedSolver([r.case], precision=precision, device=dev)
-        solver.set_stop_rule(0, r.tol, r.max_steps)
+        pool = SolvePool(precision, dev, graphs=graphs)
+        sid = pool.admit(r.case, r.tol, r.max_steps)
         torch.cuda.synchronize(dev)
         t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         t0.record(stream)
         while True:
-            _lib.check(lib.ugks_serve_steps(mixed, solver.table.data_ptr(), solver.nblocks, C.byref(solver.sizes),
-                                            solver.solves.data_ptr(), 1, steps_per_tick, stream.cuda_stream),
-                       "ugks_serve_steps")
-            st = solver.solve_state()[0]  # synchronises
+            pool.tick(steps_per_tick)
+            st = pool.states(rebuild=False)[sid]  # synchronises
             if st["stopped"]:
                 break
         t1.record(stream)
@@ -356,7 +356,8 @@ def serve_one_at_a_time(requests, precision="fp64", steps_per_tick=50, device="c
         reasons.append(_lib.STOP_REASONS[st["stopped"]])
         steps.append(st["steps"])
         units += st["steps"] * r.units
-        del solver
+        pool.retire(sid)
+        del pool
     return dict(latency=lat, reasons=reasons, steps=steps, units=units, service_s=busy,
                 value=units / busy if busy > 0 else 0.0, makespan_s=clock)
 
