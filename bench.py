@@ -282,6 +282,10 @@ def run_ours(args, rank, world, dist):
         line["cpu_baseline"] = {"value": val, "unit": UNIT, "cores": cores, "kind": kind,
                                 "sample": "%d full steps of the workload (time budget %.0f s) after 1 warm-up"
                                           % (done, budget)}
+    if args.metrics:
+        from pyugks_b200.metrics import MetricsLog
+        with MetricsLog(args.metrics, workload=args.workload, precision=args.precision) as log:
+            log.write("bench", **line)
     print(json.dumps(line), flush=True)
 
 
@@ -370,7 +374,7 @@ def batched_record(steps=10, warmup=3):
     return out
 
 
-def serving_record(arrival_seconds=2.0, max_steps=2000, tol=1e-6, steps_per_tick=50):
+def serving_record(arrival_seconds=2.0, max_steps=2000, tol=1e-6, steps_per_tick=50, metrics=None):
     """A bounded config-5 stream: Poisson arrivals at 20/s (seed 2) over
     arrival_seconds, 70% cavities / 30% adsorbing channels with config 5's
     size and parameter distributions, each run until its density residual is
@@ -380,7 +384,7 @@ def serving_record(arrival_seconds=2.0, max_steps=2000, tol=1e-6, steps_per_tick
     from pyugks_b200.serving import Server, request_stream, serve_one_at_a_time
     reqs = request_stream(seed=2, rate=20.0, duration=arrival_seconds, max_steps=max_steps, tol=tol)
     server = Server(budget_bytes=150e9, precision="mixed", steps_per_tick=steps_per_tick)
-    done = server.run(reqs)
+    done = server.run(reqs, metrics=metrics)
     lat = np.array([r.finished - r.arrival for r in done])
     batched = {"value": server.units / server.wall, "unit": UNIT, "wall_s": server.wall,
                "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
@@ -411,7 +415,11 @@ def run_serving(args):
         print(json.dumps({"impl": "reference", "unavailable":
                           "the reference has no serving loop; its CPU step is timed by the default workload"}))
         return
-    rec = serving_record(args.arrival_seconds, args.max_steps)
+    log = None
+    if args.metrics:
+        from pyugks_b200.metrics import MetricsLog
+        log = MetricsLog(args.metrics, workload="serving", precision="mixed")
+    rec = serving_record(args.arrival_seconds, args.max_steps, metrics=log)
     line = {
         "metric": METRIC, "value": rec["mixed_batched"]["value"], "unit": UNIT, "n_gpus": 1,
         "steps": None, "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -419,6 +427,9 @@ def run_serving(args):
         "config": {"workload": "serving stream: " + rec["stream"], "precision": "mixed"},
         "serving": rec,
     }
+    if log is not None:
+        log.write("bench", **line)
+        log.close()
     print(json.dumps(line), flush=True)
 
 
@@ -435,6 +446,8 @@ def main():
                     help="serving: length of the Poisson arrival window (rate 20/s)")
     ap.add_argument("--max-steps", type=int, default=2000, help="serving: step limit per solve")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--metrics", default=None,
+                    help="append JSON-lines records (the bench line; serving: per tick and per request) here")
     ap.add_argument("--no-north-star", action="store_true",
                     help="skip the batched-mixed and serving sub-records of the default line")
     args = ap.parse_args()

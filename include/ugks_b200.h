@@ -398,7 +398,11 @@ typedef struct ugks_fused_sizes {
    sizes.  The blocks of one solve must be contiguous and in the order of
    their solve index, and the blocks of one flux method contiguous (group the
    solves by flux method).  Returns 0, -1 when a count exceeds INT32_MAX, -2
-   when the ordering rule is broken. */
+   when the ordering rule is broken, -3 when a block fails validation (sizes
+   inconsistent with its ghost layers or its flux method's stencil, a missing
+   array or table, a connection outside the table or to a face of another
+   extent, velocity count or solve): a corrupted table is rejected here,
+   before any kernel could index outside its arrays. */
 int ugks_fused_layout(ugks_fused_block *blocks, int nblocks, ugks_fused_sizes *sizes);
 
 /* Initial state (ugks_block.py:411-429, ugks_sim.py:88-92): f := fEQ(macro,

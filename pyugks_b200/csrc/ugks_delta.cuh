@@ -278,6 +278,7 @@ __global__ void __launch_bounds__(NT) wall_pass_delta(const ugks_fused_block *__
   const int w = (int)blockIdx.x;
   const ugks_fused_block &blk = B[find_block<3>(B, nb, w)];
   const ugks_block_desc &d = blk.d;
+  UGKS_CHECK_ITEM(3, blk, w, solves);
   int lw = w - blk.wall_begin, mi, mj, dir;
   if (lw < 2 * d.ni) {
     dir = SOUTH;
@@ -904,6 +905,7 @@ __global__ void __launch_bounds__(CW * 32, MINB) cell_pass_delta(const ugks_fuse
   const int bi = find_block<1>(B, nb, w);
   const ugks_fused_block &blk = B[bi];
   const ugks_block_desc &d = blk.d;
+  UGKS_CHECK_ITEM(1, blk, w, solves);
   ugks_solve_state &sol = solves[blk.solve];
   if (!sol.active) return;
   const RefMaxwellian ref = ref_of(blk);
@@ -1091,6 +1093,7 @@ __global__ void __launch_bounds__(FT) ghost_pass_delta(const ugks_fused_block *_
   const int bi = find_block<2>(B, nb, w);
   const ugks_fused_block &blk = B[bi];
   const ugks_block_desc &d = blk.d;
+  UGKS_CHECK_ITEM(2, blk, w, solves);
   if (!solves[blk.solve].active) return;
   const RefMaxwellian ref = ref_of(blk);
   const int G = d.ghost, Nv = d.Nv, NP = npairs(d), vn = d.v_num;
@@ -1288,6 +1291,7 @@ __global__ void __launch_bounds__(FT) setup_cells_delta(const ugks_fused_block *
   const int bi = find_block<1>(B, nb, w);
   const ugks_fused_block &blk = B[bi];
   const ugks_block_desc &d = blk.d;
+  UGKS_CHECK_ITEM(1, blk, w, solves);
   ugks_solve_state &sol = solves[blk.solve];
   if (!sol.active) return;
   const RefMaxwellian ref = ref_of(blk);

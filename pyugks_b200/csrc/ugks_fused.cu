@@ -24,8 +24,11 @@
 
 #include <algorithm>
 #include <mutex>
+#include <optional>
 #include <type_traits>
 #include <vector>
+
+#include <nvtx3/nvToolsExt.h>
 
 #include "ugks_device.cuh"
 
@@ -173,6 +176,35 @@ __device__ __forceinline__ int find_block(const ugks_fused_block *B, int nb, int
 }
 
 __device__ __forceinline__ bool is_wall(int bc) { return bc == BC_DIFFUSE || bc == BC_ADSORBING; }
+
+// UGKS_CHECKED builds (python -m pyugks_b200.build --checked): every work
+// item is checked against the block it was found in -- inside the block's
+// range of items, and the block's sizes consistent with its ghost layers and
+// its limiter's stencil -- and an item that fails (a table corrupted on the
+// device after ugks_fused_layout validated it) flags its solve with status 9
+// and is skipped instead of indexing outside the block's arrays.
+#ifndef UGKS_CHECKED
+#define UGKS_CHECKED 0
+#endif
+constexpr int STATUS_INDEX_CHECK = 9;
+template <int WHICH>
+__device__ __forceinline__ bool item_in_block(const ugks_fused_block &b, int w) {
+  const ugks_block_desc &d = b.d;
+  long begin = 0, count = 0;
+  if (WHICH == 0) { begin = b.face_begin; count = 2l * (d.ni + 1) * (d.nj + 1); }
+  if (WHICH == 1) { begin = b.cell_begin; count = (long)d.ni * d.nj; }
+  if (WHICH == 2) { begin = b.ghost_begin; count = 2l * d.ghost * (d.ni + d.nj); }
+  if (WHICH == 3) { begin = b.wall_begin; count = 2l * (d.ni + d.nj); }
+  return w >= begin && w < begin + count && d.ghost >= (d.flux_method == 1 ? 3 : 2) &&
+         d.Ni == d.ni + 2 * d.ghost && d.Nj == d.nj + 2 * d.ghost;
+}
+#define UGKS_CHECK_ITEM(WHICH, blk, w, solves, ...)                                                       \
+  do {                                                                                                     \
+    if (UGKS_CHECKED && !item_in_block<WHICH>((blk), (w))) {                                               \
+      atomicExch(const_cast<int *>(&(solves)[(blk).solve].status), STATUS_INDEX_CHECK);                     \
+      return __VA_ARGS__;                                                                                  \
+    }                                                                                                      \
+  } while (0)
 
 // dt update of updateTimeStep (ugks_sim.py:285-311) with limit = True
 __device__ __forceinline__ double limited_dt(double dt_old, double dt_new, double delta) {
@@ -863,6 +895,7 @@ __device__ __forceinline__ bool face_work(const ugks_fused_block *__restrict__ B
   fw.bi = find_block<0>(B, nb, w);
   const ugks_fused_block &blk = B[fw.bi];
   const ugks_block_desc &d = blk.d;
+  UGKS_CHECK_ITEM(0, blk, w, solves, false);
   const ugks_solve_state &sol = solves[blk.solve];
   if (!sol.active) return false;
   if (retry_pass && !sol.retry) return false;
@@ -1142,6 +1175,7 @@ __global__ void __launch_bounds__(CW * 32, MINB) cell_pass(const ugks_fused_bloc
   const int bi = find_block<1>(B, nb, w);
   const ugks_fused_block &blk = B[bi];
   const ugks_block_desc &d = blk.d;
+  UGKS_CHECK_ITEM(1, blk, w, solves);
   ugks_solve_state &sol = solves[blk.solve];
   if (!sol.active) return;
   const int lc = w - blk.cell_begin;
@@ -1323,6 +1357,7 @@ __global__ void __launch_bounds__(FT) ghost_pass(const ugks_fused_block *__restr
   const int bi = find_block<2>(B, nb, w);
   const ugks_fused_block &blk = B[bi];
   const ugks_block_desc &d = blk.d;
+  UGKS_CHECK_ITEM(2, blk, w, solves);
   if (!solves[blk.solve].active) return;
   const int G = d.ghost, Nv = d.Nv;
   // strips in face order N, E, S, W: N/S have ni*G cells, E/W G*nj
@@ -1508,6 +1543,7 @@ __global__ void __launch_bounds__(FT) init_cells(const ugks_fused_block *__restr
   const int bi = find_block<1>(B, nb, w);
   const ugks_fused_block &blk = B[bi];
   const ugks_block_desc &d = blk.d;
+  UGKS_CHECK_ITEM(1, blk, w, solves);
   ugks_solve_state &sol = solves[blk.solve];
   if (!sol.active) return;
   const int lc = w - blk.cell_begin;
@@ -1566,6 +1602,7 @@ __global__ void __launch_bounds__(FT) restart_cells(const ugks_fused_block *__re
   const int bi = find_block<1>(B, nb, w);
   const ugks_fused_block &blk = B[bi];
   const ugks_block_desc &d = blk.d;
+  UGKS_CHECK_ITEM(1, blk, w, solves);
   ugks_solve_state &sol = solves[blk.solve];
   if (!sol.active) return;
   const int lc = w - blk.cell_begin;
@@ -1831,6 +1868,15 @@ inline void launch_moments(int v, const ugks_fused_block *B, int nb, ugks_solve_
   }
 }
 
+// NVTX range over a phase's launches on the host timeline (a profiler shows
+// them beside the kernels; without one attached a range costs a few ns)
+struct NvtxRange {
+  explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange &) = delete;
+  NvtxRange &operator=(const NvtxRange &) = delete;
+};
+
 template <typename T>
 int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks_solve_state *solves,
               int ns, void *stream, void *const *events = nullptr) {
@@ -1849,6 +1895,10 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
   auto mark = [&](int k) {
     if (events) cudaEventRecord(reinterpret_cast<cudaEvent_t>(events[k]), st);
   };
+  // NVTX: the step, and within it the face, cell and ghost phases
+  NvtxRange step_range(mixed ? "ugks step (mixed)" : "ugks step (fp64)");
+  std::optional<NvtxRange> phase;
+  phase.emplace("ugks face pass");
   mark(0);
   // mixed: the wall faces on the device's side stream, beside the segments
   WallStream *ws = nullptr;
@@ -1911,8 +1961,10 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
     mark(2);
   }
   mark(3);
+  phase.reset();
   dt_check<<<sg, 128, 0, st>>>(solves, ns, 1);
   mark(4);
+  phase.emplace("ugks cell pass");
   if (z->n_cells) {
     // cell_variant: 0 the default register budget, 2 or 3 CTAs of 8 warps per SM
     const unsigned cg = (unsigned)((z->n_cells + CW - 1) / CW);
@@ -1926,8 +1978,10 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
     }
   }
   mark(5);
+  phase.reset();
   dt_update<<<sg, 128, 0, st>>>(solves, ns);
   mark(6);
+  phase.emplace("ugks ghost pass");
   launch_ghosts<T>(B, nb, z, solves, st);
   mark(7);
   return launch_status();
@@ -2074,7 +2128,41 @@ int ugks_prepare(int mixed) {
   return e == cudaSuccess ? 0 : -(int)e;
 }
 
+// A block the fused kernels can index safely: sizes consistent with the
+// ghost layers the flux method's stencil needs, the arrays every pass
+// touches present, block connections inside the table and on a face of the
+// same extent.  (A corrupted entry would otherwise send a kernel outside its
+// arrays: the table is rejected on the host before any launch.)
+static bool block_valid(const ugks_fused_block *blocks, int nblocks, int b) {
+  const ugks_fused_block &x = blocks[b];
+  const ugks_block_desc &d = x.d;
+  const int need = d.flux_method == 1 ? 3 : 2;  // stencil half-width of WENO5 / vanLeer, minmod
+  if (d.ni <= 0 || d.nj <= 0 || d.Nv <= 0 || d.ghost < need) return false;
+  if (d.Ni != d.ni + 2 * d.ghost || d.Nj != d.nj + 2 * d.ghost) return false;
+  if (d.u_num < 0 || d.v_num < 0 || (d.u_num > 0 && (int64_t)d.u_num * d.v_num != d.Nv)) return false;
+  if (!d.quad || !d.weight || !d.mirror_NS || !d.mirror_EW || !d.mirror_D) return false;
+  if (!x.f || !x.flux_S || !x.flux_W || !x.flux_macro_S || !x.flux_macro_W || !x.macro || !x.Q || !x.prim_old ||
+      !x.area || !x.centre || !x.mid_side || !x.normal || !x.side_length || !x.xy || !x.cell_mom || !x.Q_next ||
+      !x.face_geo || !x.wall_prop || !x.wall_cover || !x.wall_fluxes || !x.wall_dist)
+    return false;
+  for (int f = 0; f < 4; ++f) {
+    if (x.bc_type[f] < BC_ADJACENT || x.bc_type[f] > BC_BOUNCE_BACK) return false;
+    if (x.bc_type[f] == BC_ADJACENT || x.bc_type[f] == BC_PERIODIC) {
+      const int o = x.bc_block[f], of = x.bc_face[f];
+      if (o < 0 || o >= nblocks || of < 0 || of > 3) return false;
+      const ugks_block_desc &od = blocks[o].d;
+      const int n_here = (f == GNORTH || f == GSOUTH) ? d.ni : d.nj;
+      const int n_there = (of == GNORTH || of == GSOUTH) ? od.ni : od.nj;
+      if (n_here != n_there || od.Nv != d.Nv || od.ghost != d.ghost || blocks[o].solve != x.solve) return false;
+    }
+  }
+  return true;
+}
+
 int ugks_fused_layout(ugks_fused_block *blocks, int nblocks, ugks_fused_sizes *z) {
+  if (nblocks < 0 || (nblocks > 0 && !blocks) || !z) return -3;
+  for (int b = 0; b < nblocks; ++b)
+    if (!block_valid(blocks, nblocks, b)) return -3;
   int64_t f = 0, c = 0, g = 0, wl = 0;
   int32_t max_nv = 0, max_axes = 0;
   int64_t fb[4] = {0, 0, 0, 0}, fc[4] = {0, 0, 0, 0};

@@ -240,7 +240,7 @@ class Server:
         self.done = []
         self.units = 0
 
-    def run(self, requests, time_limit=None):
+    def run(self, requests, time_limit=None, metrics=None):
         """Serve a list of Request (arrival in seconds from the start).
         Returns the completed requests.
 
@@ -249,7 +249,8 @@ class Server:
         while the tick runs, and join the table at the next tick.  A solve
         stops on the device at the step that meets its rule (residual below
         its tolerance, its step limit, or an error status) and leaves at the
-        end of that tick."""
+        end of that tick.  metrics: a metrics.MetricsLog that gets a record
+        per tick and per completed request."""
         import torch
         dev = self.pool.device
         main = torch.cuda.current_stream(dev)
@@ -311,6 +312,10 @@ class Server:
                         self.used -= r.need
                         del active[sid]
                         self.done.append(r)
+                        if metrics is not None:
+                            metrics.request(r)
+                if metrics is not None:
+                    metrics.tick(now, len(active), len(waiting) + len(queue) - i, self.used, self.budget, self.units)
         finally:
             main.wait_stream(side)
         self.wall = time.perf_counter() - t0

@@ -103,3 +103,38 @@ def test_bulk_copy_wait_is_bounded(cuda):
     s = FusedSolver(configs.cavity(n=8, m=8, vlim=4.0), precision="mixed")
     s.step(2)
     assert s.solve_state()[0]["status"] == 0
+
+
+def test_checked_build_matches_and_passes(cuda):
+    """The UGKS_CHECKED library (every fused work item checked against its
+    block; a failed check would set status 9 and skip the item) runs the same
+    steps to bit-identical results with status 0, in both precisions."""
+    import os
+    import subprocess
+    import sys
+    from pyugks_b200 import build as B
+    if not os.path.exists(B.LIB_CHECKED):
+        pytest.fail("libugks_b200_checked.so not built (python -m pyugks_b200.build --checked)")
+    code = (
+        "import sys, numpy as np; sys.path.insert(0, %r)\n"
+        "from pyugks_b200 import configs\n"
+        "from pyugks_b200.fused import FusedSolver\n"
+        "out = {}\n"
+        "for prec in ('fp64', 'mixed'):\n"
+        "    s = FusedSolver([configs.cavity_multiblock(nb=2, n=8, m=8), configs.channel(nblocks=2, n=8, m=8)],"
+        " precision=prec)\n"
+        "    s.step(6)\n"
+        "    st = s.solve_state()\n"
+        "    out[prec] = [int(x['status']) for x in st] + [float(np.sum([f['rho'].sum() + f['T'].sum() for f in"
+        " s.fields(k)])) for k in range(2)]\n"
+        "print(repr(out))\n") % os.path.dirname(B.HERE)
+    runs = []
+    for lib in (B.LIB, B.LIB_CHECKED):
+        env = dict(os.environ, UGKS_LIB_PATH=lib)
+        r = subprocess.run([sys.executable, "-c", code], env=env, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        runs.append(eval(r.stdout.strip().splitlines()[-1]))
+    plain, checked = runs
+    for prec in ("fp64", "mixed"):
+        assert checked[prec][:2] == [0, 0]
+        assert checked[prec] == plain[prec]
