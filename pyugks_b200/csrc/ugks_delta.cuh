@@ -300,6 +300,27 @@ __global__ void __launch_bounds__(NT) wall_pass_delta(const ugks_fused_block *__
 }
 constexpr int WALL_NT = 128;
 
+// raw moments up to third order (RM* / RB*) of a distribution, from the
+// global frame (x, y) into a face frame u = nx x + ny y, t = nx y - ny x: the
+// moment tensors rotate as the velocities do
+__device__ __forceinline__ void rotate_moments(double (&m)[RNMOM], V2 n) {
+  const double a = n.x, c = n.y, aa = a * a, cc = c * c, ac = a * c;
+  const double m10 = m[RM10], m01 = m[RM01], m20 = m[RM20], m11 = m[RM11], m02 = m[RM02];
+  const double m30 = m[RM30], m21 = m[RM21], m12 = m[RM12], m03 = m[RM03], b10 = m[RB10], b01 = m[RB01];
+  m[RM10] = a * m10 + c * m01;
+  m[RM01] = a * m01 - c * m10;
+  m[RM20] = aa * m20 + 2.0 * ac * m11 + cc * m02;
+  m[RM11] = ac * (m02 - m20) + (aa - cc) * m11;
+  m[RM02] = cc * m20 - 2.0 * ac * m11 + aa * m02;
+  // u^3, u^2 t, u t^2, t^3 expanded in x^3, x^2 y, x y^2, y^3
+  m[RM30] = a * aa * m30 + 3.0 * aa * c * m21 + 3.0 * a * cc * m12 + c * cc * m03;
+  m[RM21] = -aa * c * m30 + a * (aa - 2.0 * cc) * m21 + c * (2.0 * aa - cc) * m12 + a * cc * m03;
+  m[RM12] = a * cc * m30 + c * (cc - 2.0 * aa) * m21 + a * (aa - 2.0 * cc) * m12 + aa * c * m03;
+  m[RM03] = -c * cc * m30 + 3.0 * a * cc * m21 - 3.0 * aa * c * m12 + a * aa * m03;
+  m[RB10] = a * b10 + c * b01;
+  m[RB01] = a * b01 - c * b10;
+}
+
 // 2. coefficients: the per-face block of face_coefficients, one face per
 // thread (the same chain as the lanes of a face CTA run there)
 __global__ void __launch_bounds__(128) face_coef_delta(const ugks_fused_block *__restrict__ B, int nb,
@@ -321,6 +342,7 @@ __global__ void __launch_bounds__(128) face_coef_delta(const ugks_fused_block *_
   double dm[RNMOM];
 #pragma unroll
   for (int k = 0; k < RNMOM; ++k) dm[k] = rec[FR_MOM + k];
+  rotate_moments(dm, n);
   // face state: the reference's moments in the face frame plus the deviation's
   const double *R = ref.mom;
   const V2 rU = to_local(v2(R[RM10], R[RM01]), n);
@@ -449,8 +471,9 @@ __global__ void __launch_bounds__(WPC * 32, MINB) face_moments_warp(const ugks_f
   float4 *frow = reinterpret_cast<float4 *>(dir == SOUTH ? blk.flux_S : blk.flux_W) + pidx(d, gi, gj, 0);
   float4 *arow = reinterpret_cast<float4 *>(dir == SOUTH ? blk.aux_S : blk.aux_W) + pidx(d, gi, gj, 0);
   const float2 nx2 = bc2((float)n.x), ny2 = bc2((float)n.y), mny2 = bc2(-(float)n.y);
-  // raw moments of the face deviation in FP64, products included: the face
-  // heat flux is a small difference of them
+  // raw moments of the face deviation in FP64, products included (the face
+  // heat flux is a small difference of them), in the global frame: the
+  // coefficient pass rotates the sums into the face frame
   double mom[RNMOM];
 #pragma unroll
   for (int k = 0; k < RNMOM; ++k) mom[k] = 0.0;
@@ -492,25 +515,25 @@ __global__ void __launch_bounds__(WPC * 32, MINB) face_moments_warp(const ugks_f
     const float2 fh = fma2(sh2, ds, Sh[MID]), fb = fma2(sb2, ds, Sb[MID]);
     frow[p] = cat2(fh, fb);
     arow[p] = cat2(sh2, sb2);
-    // raw moments (face frame); the padding velocity has df = 0 and x = 0
+    // raw moments (global frame); the padding velocity has df = 0
     const double xs[2] = {xd.x, xd.y}, hs[2] = {fh.x, fh.y}, bs[2] = {fb.x, fb.y};
+    const double yy = yd * yd;
 #pragma unroll
     for (int e = 0; e < 2; ++e) {
-      const double u = fma(xs[e], n.x, yd * n.y), t = fma(yd, n.x, -xs[e] * n.y);
-      const double h = hs[e], b = bs[e], t1 = u * h, t2 = t * h, uu = u * u, tt = t * t;
+      const double x = xs[e], h = hs[e], b = bs[e], xh = x * h, yh = yd * h, xx = x * x;
       mom[RM00] += h;
-      mom[RM10] += t1;
-      mom[RM01] += t2;
-      mom[RM20] = fma(u, t1, mom[RM20]);
-      mom[RM11] = fma(t, t1, mom[RM11]);
-      mom[RM02] = fma(t, t2, mom[RM02]);
-      mom[RM30] = fma(uu, t1, mom[RM30]);
-      mom[RM21] = fma(uu, t2, mom[RM21]);
-      mom[RM12] = fma(tt, t1, mom[RM12]);
-      mom[RM03] = fma(tt, t2, mom[RM03]);
+      mom[RM10] += xh;
+      mom[RM01] += yh;
+      mom[RM20] = fma(x, xh, mom[RM20]);
+      mom[RM11] = fma(yd, xh, mom[RM11]);
+      mom[RM02] = fma(yd, yh, mom[RM02]);
+      mom[RM30] = fma(xx, xh, mom[RM30]);
+      mom[RM21] = fma(xx, yh, mom[RM21]);
+      mom[RM12] = fma(yy, xh, mom[RM12]);
+      mom[RM03] = fma(yy, yh, mom[RM03]);
       mom[RB00] += b;
-      mom[RB10] = fma(u, b, mom[RB10]);
-      mom[RB01] = fma(t, b, mom[RB01]);
+      mom[RB10] = fma(x, b, mom[RB10]);
+      mom[RB01] = fma(yd, b, mom[RB01]);
     }
     jv += rs;
     ia += qs;
@@ -876,13 +899,33 @@ __device__ __forceinline__ uint32_t sr_hash(uint32_t x) {
   x ^= x >> 16;
   return x;
 }
-// x rounded to the float toward zero or the next one away from zero, away
-// with probability (x - toward) / (away - toward), u16 / 65536 uniform
-__device__ __forceinline__ float sr_round(double x, uint32_t u16) {
-  const float z = __double2float_rz(x);
-  const float a = __uint_as_float(__float_as_uint(z) + 1u);
-  const double gap = (double)a - (double)z, rem = x - (double)z;
-  return fabs(rem) > (double)u16 * (1.0 / 65536.0) * fabs(gap) ? a : z;
+// x = f a1 + inc for two velocities as float pairs hi + lo, hi = RN(x),
+// |lo| <= ulp(hi) / 2, in FP32 arithmetic only: a1 = a1h + a1l (two floats,
+// given as -a1h and -a1l), the product's rounding error by FMA (Dekker's
+// product) and the sums' by Knuth's two-sum.  hi + lo is x to within about
+// 2^-24 of lo (2^-48 of f where f a1 and inc cancel), far below what the
+// rounding probability needs.
+__device__ __forceinline__ void sr_parts(float2 f, float2 inc, float2 a1h, float2 na1h, float2 na1l, float2 &hi,
+                                         float2 &lo) {
+  const float2 p = mul2(f, a1h);      // RN(f a1h)
+  const float2 q = fma2(f, na1h, p);  // p - f a1h, exact
+  const float2 cn = fma2(f, na1l, q); // -(f a1h - p + f a1l): x = p + inc - cn
+  const float2 s = add2(p, inc);
+  const float2 bp = sub2(s, p);
+  const float2 e = add2(sub2(p, sub2(s, bp)), sub2(inc, bp));  // s + e = p + inc exactly
+  const float2 r = sub2(e, cn);                                 // x - s
+  hi = add2(s, r);
+  const float2 bq = sub2(hi, s);
+  lo = add2(sub2(s, sub2(hi, bq)), sub2(r, bq));                // hi + lo = s + r exactly
+}
+// hi + lo rounded to hi or to hi's neighbour on lo's side, the neighbour
+// with probability |lo| / (the gap between them), u16 / 65536 uniform.  A
+// zero, infinite or NaN hi comes back unchanged (the comparison is false).
+__device__ __forceinline__ float sr_pick(float hi, float lo, uint32_t u16) {
+  const uint32_t hb = __float_as_uint(hi);
+  const float nb = __uint_as_float(((hb ^ __float_as_uint(lo)) >> 31) ? hb - 1u : hb + 1u);
+  const float u = __uint_as_float(0x3f800000u | (u16 << 7)) - 1.0f;  // u16 / 65536, exact
+  return fabsf(lo) > u * fabsf(nb - hi) ? nb : hi;
 }
 
 // ---------------------------------------------------------------------------
@@ -983,14 +1026,16 @@ __global__ void __launch_bounds__(CW * 32, MINB) cell_pass_delta(const ugks_fuse
   const double so = 0.8 * (1 - d.Pr) * (old.s3 * old.s3) * nr_rcp(old.s0);
   const float2 fa1 = bc2((float)bc[3]), fa2 = bc2((float)bc[4]), fa3 = bc2((float)a3), fa4 = bc2((float)a4);
 #if UGKS_SR_STORE
-  const double a1d = bc[3];
+  const float a1h = (float)bc[3];
+  const float2 fa1h = bc2(a1h), fna1h = bc2(-a1h), fna1l = bc2(-(float)(bc[3] - (double)a1h));
   const uint32_t srseed =
       sr_hash((uint32_t)sol.steps * 0x9e3779b9u + (uint32_t)(bi - sol.first_block) * 0x85ebca6bu);
 #endif
   const float2 fkbn = bc2((float)kn), fkbo = bc2((float)ko);
   const float2 fdkn = bc2((float)(kn - ref.kb0)), fdko = bc2((float)(ko - ref.kb0));
-  const float2 fa3kn = bc2((float)(a3 * kn)), fa4ko = bc2((float)(a4 * ko));
-  const float2 fso = bc2((float)so), fsn = bc2((float)sn), fQx = bc2((float)Q.x), fQy = bc2((float)Q.y);
+  // the Shakhov factors weighted by a4 / a3, times the heat flux
+  const float2 fSoQx = bc2((float)(a4 * so * Q.x)), fSoQy = bc2((float)(a4 * so * Q.y));
+  const float2 fSnQx = bc2((float)(a3 * sn * Q.x)), fSnQy = bc2((float)(a3 * sn * Q.y));
   const float2 fUox = bc2((float)old.s1), fUoy = bc2((float)old.s2), fUnx = bc2((float)nU), fUny = bc2((float)nV);
   const float2 flo2 = bc2((float)(2.0 * old.s3)), fln2 = bc2((float)(2.0 * nl));
   const size_t base = pidx(d, gi, gj, 0);
@@ -1020,27 +1065,28 @@ __global__ void __launch_bounds__(CW * 32, MINB) cell_pass_delta(const ugks_fuse
     const float2 Mo = fma2(m, ro, m), Mn = fma2(m, rn, m);
     const float2 ox = sub2(qx, fUox), oy = sub2(qy, fUoy), o2 = fma2(ox, ox, mul2(oy, oy));
     const float2 nx = sub2(qx, fUnx), ny = sub2(qy, fUny), n2 = fma2(nx, nx, mul2(ny, ny));
-    const float2 So = mul2(fso, fma2(ox, fQx, mul2(oy, fQy))), Sn = mul2(fsn, fma2(nx, fQx, mul2(ny, fQy)));
+    // a4 S and a3 S of the old and new states' Shakhov terms
+    const float2 So = fma2(ox, fSoQx, mul2(oy, fSoQy)), Sn = fma2(nx, fSnQx, mul2(ny, fSnQy));
     const float2 po = fma2(flo2, o2, bc2(-4.0f)), pn = fma2(fln2, n2, bc2(-4.0f));
     // fEQ - M of both states, weighted by a4 / a3 (fEQ, clFunctions.c:79-86)
-    const float2 So_p = mul2(So, po), Sn_p = mul2(Sn, pn);
-    const float2 eh = fma2(mul2(fa4, So_p), Mo,
-                           fma2(mul2(fa3, Sn_p), Mn, mul2(m, fma2(fa4, ro, mul2(fa3, rn)))));
+    const float2 eh = fma2(mul2(So, po), Mo, fma2(mul2(Sn, pn), Mn, mul2(m, fma2(fa4, ro, mul2(fa3, rn)))));
     const float2 So_b = fma2(So, po, add2(So, So)), Sn_b = fma2(Sn, pn, add2(Sn, Sn));  // S (P4 + 2)
-    const float2 eb = fma2(mul2(fa4ko, So_b), Mo,
-                           fma2(mul2(fa3kn, Sn_b), Mn,
+    const float2 eb = fma2(mul2(fkbo, So_b), Mo,
+                           fma2(mul2(fkbn, Sn_b), Mn,
                                 mul2(m, fma2(fa4, fma2(fkbo, ro, fdko), mul2(fa3, fma2(fkbn, rn, fdkn))))));
     const float2 flh = add2(sub2(lo2(s0), lo2(s1)), sub2(lo2(w0), lo2(w1)));
     const float2 flb = add2(sub2(hi2(s0), hi2(s1)), sub2(hi2(w0), hi2(w1)));
 #if UGKS_SR_STORE
-    // stochastic rounding of the new deviation: f a1 + increment in FP64,
-    // rounded to a neighbouring float with probability given by its distance
+    // stochastic rounding of the new deviation: f a1 + increment as a float
+    // pair, rounded to a neighbouring float with probability given by its
+    // distance
     const float2 ih = fma2(flh, fa2, eh), ib = fma2(flb, fa2, eb);
     uint32_t h1 = sr_hash((uint32_t)k * 2654435761u ^ srseed), h2 = sr_hash(h1 ^ 0x68e31da4u);
-    const float2 oh = make_float2(sr_round(fma((double)f.x, a1d, (double)ih.x), h1 & 0xffffu),
-                                  sr_round(fma((double)f.y, a1d, (double)ih.y), h1 >> 16));
-    const float2 ob = make_float2(sr_round(fma((double)f.z, a1d, (double)ib.x), h2 & 0xffffu),
-                                  sr_round(fma((double)f.w, a1d, (double)ib.y), h2 >> 16));
+    float2 hh, hl, bh, bl;
+    sr_parts(lo2(f), ih, fa1h, fna1h, fna1l, hh, hl);
+    sr_parts(hi2(f), ib, fa1h, fna1h, fna1l, bh, bl);
+    const float2 oh = make_float2(sr_pick(hh.x, hl.x, h1 & 0xffffu), sr_pick(hh.y, hl.y, h1 >> 16));
+    const float2 ob = make_float2(sr_pick(bh.x, bl.x, h2 & 0xffffu), sr_pick(bh.y, bl.y, h2 >> 16));
 #else
     const float2 oh = fma2(lo2(f), fa1, fma2(flh, fa2, eh)), ob = fma2(hi2(f), fa1, fma2(flb, fa2, eb));
 #endif
