@@ -431,8 +431,9 @@ __global__ void __launch_bounds__(128) face_coef_delta(const ugks_fused_block *_
 // sums close with one halving butterfly and no CTA barrier, so that a warp's
 // per-face set-up overlaps the other warps' sweeps.
 // ---------------------------------------------------------------------------
-// doubles of shared memory per warp: moments (FP64 axis velocities), flux
-// (the face record, then the axis tables)
+// doubles of shared memory per warp: moments (the axis velocities as floats,
+// in at most max_axes + 2 doubles), flux (the face record, then the axis
+// tables)
 inline int delta_moments_stride(int max_axes) { return ((max_axes + 2) + 1) & ~1; }
 inline int delta_flux_stride(int max_axes) { return 48 + (((12 * (max_axes + 2) + 7) / 8 + 1) & ~1); }
 
@@ -457,12 +458,12 @@ __global__ void __launch_bounds__(WPC * 32, MINB) face_moments_warp(const ugks_f
   const float dist0 = (float)fg[0], idist0 = (float)fg[1], il0 = (float)fg[2];
   const float dist1 = (float)fg[3], idist1 = (float)fg[4], il1 = (float)fg[5];
   constexpr int L = FM == 1 ? 5 : 3, MID = FM == 1 ? 2 : 1;
-  // FP64 axis velocities (entry u_num: the padding lane's, 0)
-  double *QXd = dyn + (size_t)warp * wstride, *QYd = QXd + (un + 1);
+  // axis velocities as floats (entry u_num: the padding lane's, 0)
+  float *QXf = reinterpret_cast<float *>(dyn + (size_t)warp * wstride), *QYf = QXf + (un + 1);
   for (int k = lane; k <= un + vn; k += 32) {
-    if (k < un) QXd[k] = d.quad[2 * (size_t)k * vn];
-    else if (k == un) QXd[k] = 0.0;
-    else QYd[k - un - 1] = d.quad[2 * (size_t)(k - un - 1) + 1];
+    if (k < un) QXf[k] = (float)d.quad[2 * (size_t)k * vn];
+    else if (k == un) QXf[k] = 0.0f;
+    else QYf[k - un - 1] = (float)d.quad[2 * (size_t)(k - un - 1) + 1];
   }
   __syncwarp();
   const int pstep = (dir == SOUTH ? 1 : d.Nj) * NP;  // pairs between neighbouring cells along the normal
@@ -471,20 +472,19 @@ __global__ void __launch_bounds__(WPC * 32, MINB) face_moments_warp(const ugks_f
   float4 *frow = reinterpret_cast<float4 *>(dir == SOUTH ? blk.flux_S : blk.flux_W) + pidx(d, gi, gj, 0);
   float4 *arow = reinterpret_cast<float4 *>(dir == SOUTH ? blk.aux_S : blk.aux_W) + pidx(d, gi, gj, 0);
   const float2 nx2 = bc2((float)n.x), ny2 = bc2((float)n.y), mny2 = bc2(-(float)n.y);
-  // raw moments of the face deviation in FP64, products included (the face
-  // heat flux is a small difference of them), in the global frame: the
-  // coefficient pass rotates the sums into the face frame
-  double mom[RNMOM];
+  // raw moments of the face deviation in the global frame (the coefficient
+  // pass rotates the sums into the face frame): products and each lane's sums
+  // in packed FP32, the two velocities of a pair in the two halves, about 17
+  // terms per half at Nv 1089; the halves and the lanes are combined in FP64
+  float2 acc[RNMOM];
 #pragma unroll
-  for (int k = 0; k < RNMOM; ++k) mom[k] = 0.0;
+  for (int k = 0; k < RNMOM; ++k) acc[k] = make_float2(0.0f, 0.0f);
   // pair p = a v_num + jv: velocities (2a, jv) and (2a + 1, jv)
   const int qs = 32 / vn, rs = 32 % vn;
   int ia = lane / vn, jv = lane % vn;
 #pragma unroll 1
   for (int p = lane; p < NP; p += 32) {
-    const double2 xd = *reinterpret_cast<const double2 *>(QXd + 2 * ia);
-    const double yd = QYd[jv];
-    const float2 qx = make_float2((float)xd.x, (float)xd.y), qy = bc2((float)yd);
+    const float2 qx = *reinterpret_cast<const float2 *>(QXf + 2 * ia), qy = bc2(QYf[jv]);
     const float2 U = fma2(qx, nx2, mul2(qy, ny2));
     const bool ua = U.x > 0.0f, ub = U.y > 0.0f;
     float2 Sh[L], Sb[L];
@@ -516,29 +516,29 @@ __global__ void __launch_bounds__(WPC * 32, MINB) face_moments_warp(const ugks_f
     frow[p] = cat2(fh, fb);
     arow[p] = cat2(sh2, sb2);
     // raw moments (global frame); the padding velocity has df = 0
-    const double xs[2] = {xd.x, xd.y}, hs[2] = {fh.x, fh.y}, bs[2] = {fb.x, fb.y};
-    const double yy = yd * yd;
-#pragma unroll
-    for (int e = 0; e < 2; ++e) {
-      const double x = xs[e], h = hs[e], b = bs[e], xh = x * h, yh = yd * h, xx = x * x;
-      mom[RM00] += h;
-      mom[RM10] += xh;
-      mom[RM01] += yh;
-      mom[RM20] = fma(x, xh, mom[RM20]);
-      mom[RM11] = fma(yd, xh, mom[RM11]);
-      mom[RM02] = fma(yd, yh, mom[RM02]);
-      mom[RM30] = fma(xx, xh, mom[RM30]);
-      mom[RM21] = fma(xx, yh, mom[RM21]);
-      mom[RM12] = fma(yy, xh, mom[RM12]);
-      mom[RM03] = fma(yy, yh, mom[RM03]);
-      mom[RB00] += b;
-      mom[RB10] = fma(x, b, mom[RB10]);
-      mom[RB01] = fma(yd, b, mom[RB01]);
+    {
+      const float2 xh = mul2(qx, fh), yh = mul2(qy, fh), xx = mul2(qx, qx), yy = mul2(qy, qy);
+      acc[RM00] = add2(acc[RM00], fh);
+      acc[RM10] = add2(acc[RM10], xh);
+      acc[RM01] = add2(acc[RM01], yh);
+      acc[RM20] = fma2(qx, xh, acc[RM20]);
+      acc[RM11] = fma2(qy, xh, acc[RM11]);
+      acc[RM02] = fma2(qy, yh, acc[RM02]);
+      acc[RM30] = fma2(xx, xh, acc[RM30]);
+      acc[RM21] = fma2(xx, yh, acc[RM21]);
+      acc[RM12] = fma2(yy, xh, acc[RM12]);
+      acc[RM03] = fma2(yy, yh, acc[RM03]);
+      acc[RB00] = add2(acc[RB00], fb);
+      acc[RB10] = fma2(qx, fb, acc[RB10]);
+      acc[RB01] = fma2(qy, fb, acc[RB01]);
     }
     jv += rs;
     ia += qs;
     if (jv >= vn) { jv -= vn; ++ia; }
   }
+  double mom[RNMOM];
+#pragma unroll
+  for (int k = 0; k < RNMOM; ++k) mom[k] = (double)acc[k].x + (double)acc[k].y;
   const double tw = warp_spread_sum<RNMOM>(mom);
   constexpr int S = spread_shift<RNMOM>();
   if ((lane & ((1 << S) - 1)) == 0 && (lane >> S) < RNMOM)
@@ -1180,6 +1180,29 @@ __global__ void __launch_bounds__(FT) ghost_pass_delta(const ugks_fused_block *_
     vb = va + vn;
   };
   auto gather = [&](const float4 *src, const int32_t *perm) {
+    if (perm == nullptr) {
+      // a plain copy: GHOST_U loads per thread in flight before the first
+      // store (a store may alias a later load, so the compiler keeps them in
+      // program order)
+      for (int p0 = threadIdx.x; p0 < NP; p0 += GHOST_U * FT) {
+        float4 o[GHOST_U];
+#pragma unroll
+        for (int u = 0; u < GHOST_U; ++u)
+          if (p0 + u * FT < NP) o[u] = src[p0 + u * FT];
+#pragma unroll
+        for (int u = 0; u < GHOST_U; ++u) {
+          const int p = p0 + u * FT;
+          if (p < NP) {
+            dst[p] = o[u];
+            int va, vb;
+            lanes(p, va, vb);
+            tally(va, o[u].x, o[u].z);
+            if (vb < Nv) tally(vb, o[u].y, o[u].w);
+          }
+        }
+      }
+      return;
+    }
     for (int p = threadIdx.x; p < NP; p += FT) {
       int va, vb;
       lanes(p, va, vb);
@@ -1250,14 +1273,27 @@ __global__ void __launch_bounds__(FT) ghost_pass_delta(const ugks_fused_block *_
     const float4 *c0 = reinterpret_cast<const float4 *>(blk.f) + pidx(d, ei0, ej0, 0);
     const float4 *c1 = reinterpret_cast<const float4 *>(blk.f) + pidx(d, ei1, ej1, 0);
     const float2 fm = bc2(m);
-    for (int p = threadIdx.x; p < NP; p += FT) {
-      const float4 x0 = c0[p], x1 = c1[p];
-      const float2 h = fma2(fm, sub2(lo2(x1), lo2(x0)), lo2(x1)), bb = fma2(fm, sub2(hi2(x1), hi2(x0)), hi2(x1));
-      dst[p] = cat2(h, bb);
-      int va, vb;
-      lanes(p, va, vb);
-      tally(va, h.x, bb.x);
-      if (vb < Nv) tally(vb, h.y, bb.y);
+    for (int p0 = threadIdx.x; p0 < NP; p0 += GHOST_U * FT) {
+      float4 x0[GHOST_U], x1[GHOST_U];
+#pragma unroll
+      for (int u = 0; u < GHOST_U; ++u)
+        if (p0 + u * FT < NP) {
+          x0[u] = c0[p0 + u * FT];
+          x1[u] = c1[p0 + u * FT];
+        }
+#pragma unroll
+      for (int u = 0; u < GHOST_U; ++u) {
+        const int p = p0 + u * FT;
+        if (p < NP) {
+          const float2 h = fma2(fm, sub2(lo2(x1[u]), lo2(x0[u])), lo2(x1[u]));
+          const float2 bb = fma2(fm, sub2(hi2(x1[u]), hi2(x0[u])), hi2(x1[u]));
+          dst[p] = cat2(h, bb);
+          int va, vb;
+          lanes(p, va, vb);
+          tally(va, h.x, bb.x);
+          if (vb < Nv) tally(vb, h.y, bb.y);
+        }
+      }
     }
   } else if (t == BC_EXTRAPOLATE_OUT || t == BC_REFLECT || t == BC_BOUNCE_BACK) {
     long si, sj;

@@ -37,6 +37,10 @@ using namespace ugks;
 namespace {
 
 constexpr int FT = 128;  // threads per face / cell / ghost CTA
+// velocities (or pairs) per thread whose loads are in flight together in
+// the ghost copies, issued before the first store (a store may alias a later
+// load, so the compiler keeps them in program order)
+constexpr int GHOST_U = 4;
 // face kernels come in two shapes: narrow, FT threads per face at
 // FACE_MIN_BLOCKS CTAs per SM (fits while the per-face shared memory allows
 // that many), and wide, for larger velocity grids, where shared memory allows
@@ -1393,6 +1397,18 @@ __global__ void __launch_bounds__(FT) ghost_pass(const ugks_fused_block *__restr
     mom[2] = fma(e.y, o.x, mom[2]);
     mom[3] += fma(fma(e.x, e.x, e.y * e.y), o.x, o.y);
   };
+  // load(v) for every velocity, put in the same order as a plain loop
+  auto copy = [&](auto load) {
+    for (int v0 = threadIdx.x; v0 < Nv; v0 += GHOST_U * FT) {
+      V2 x[GHOST_U];
+#pragma unroll
+      for (int u = 0; u < GHOST_U; ++u)
+        if (v0 + u * FT < Nv) x[u] = load(v0 + u * FT);
+#pragma unroll
+      for (int u = 0; u < GHOST_U; ++u)
+        if (v0 + u * FT < Nv) put(v0 + u * FT, x[u]);
+    }
+  };
   if (t == BC_ADJACENT || t == BC_PERIODIC) {
     // edgeExchange (clGhostRoutines.c:407-538)
     const ugks_fused_block &ob = B[blk.bc_block[face]];
@@ -1426,7 +1442,8 @@ __global__ void __launch_bounds__(FT) ghost_pass(const ugks_fused_block *__restr
     const size_t src = ((size_t)iB * NJB + jB) * (size_t)Nv;
     const int flip = blk.bc_flip[face];
     const int32_t *perm = flip == FLIP_NS ? d.mirror_NS : (flip == FLIP_D ? d.mirror_D : d.mirror_EW);
-    for (int v = threadIdx.x; v < Nv; v += FT) put(v, St::load(ob.f, src + (flip == NO_FLIP ? v : perm[v])));
+    if (flip == NO_FLIP) copy([&](int v) { return St::load(ob.f, src + v); });
+    else copy([&](int v) { return St::load(ob.f, src + perm[v]); });
   } else if (t == BC_DIFFUSE || t == BC_ADSORBING) {
     // edgeConstGrad (clGhostRoutines.c:967-1048)
     long ei0, ej0, ei1, ej1;
@@ -1438,11 +1455,11 @@ __global__ void __launch_bounds__(FT) ghost_pass(const ugks_fused_block *__restr
       default: ei1 = G; ej1 = gj; ei0 = ei1 + 1; ej0 = ej1; m = (double)(ei1 - gi); break;
     }
     const size_t k0 = fidx(d, ei0, ej0, 0), k1 = fidx(d, ei1, ej1, 0);
-    for (int v = threadIdx.x; v < Nv; v += FT) {
+    copy([&](int v) {
       const V2 f0 = St::load(blk.f, k0 + v), f1 = St::load(blk.f, k1 + v);
-      put(v, v2(__dadd_rn(f1.x, __dmul_rn(m, __dsub_rn(f1.x, f0.x))),
-                __dadd_rn(f1.y, __dmul_rn(m, __dsub_rn(f1.y, f0.y)))));
-    }
+      return v2(__dadd_rn(f1.x, __dmul_rn(m, __dsub_rn(f1.x, f0.x))),
+                __dadd_rn(f1.y, __dmul_rn(m, __dsub_rn(f1.y, f0.y))));
+    });
   } else if (t == BC_EXTRAPOLATE_OUT || t == BC_REFLECT || t == BC_BOUNCE_BACK) {
     long si, sj;
     const int32_t *perm = nullptr;
@@ -1463,7 +1480,8 @@ __global__ void __launch_bounds__(FT) ghost_pass(const ugks_fused_block *__restr
       if (t == BC_BOUNCE_BACK) perm = d.mirror_D;
     }
     const size_t src = fidx(d, si, sj, 0);
-    for (int v = threadIdx.x; v < Nv; v += FT) put(v, St::load(blk.f, src + (perm ? perm[v] : v)));
+    if (perm) copy([&](int v) { return St::load(blk.f, src + perm[v]); });
+    else copy([&](int v) { return St::load(blk.f, src + v); });
   } else if (t == BC_CONSTANT || t == BC_INFLOW || t == BC_OUTFLOW) {
     const long ci = (face == GNORTH || face == GSOUTH) ? a : b;
     const P4 wp = ld4(blk.wall_prop, ci * 4 + face);
