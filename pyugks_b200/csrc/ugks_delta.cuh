@@ -482,6 +482,32 @@ __global__ void __launch_bounds__(WPC * 32, MINB) face_moments_warp(const ugks_f
   // pair p = a v_num + jv: velocities (2a, jv) and (2a + 1, jv)
   const int qs = 32 / vn, rs = 32 % vn;
   int ia = lane / vn, jv = lane % vn;
+  // reconstruction, stored face values and slopes, and moments of pair p
+  // from its stencil rows
+  auto pair_work = [&](int p, const float2 (&Sh)[L], const float2 (&Sb)[L], float2 qx, float2 qy, bool ua, bool ub) {
+    const float2 il = make_float2(ua ? il1 : il0, ub ? il1 : il0);
+    const float2 ds = make_float2(ua ? dist1 : dist0, ub ? dist1 : dist0);
+    const float2 ids = make_float2(ua ? idist1 : idist0, ub ? idist1 : idist0);
+    const float2 sh2 = slope_pair<FM>(Sh, il, ids), sb2 = slope_pair<FM>(Sb, il, ids);
+    const float2 fh = fma2(sh2, ds, Sh[MID]), fb = fma2(sb2, ds, Sb[MID]);
+    frow[p] = cat2(fh, fb);
+    arow[p] = cat2(sh2, sb2);
+    // raw moments (global frame); the padding velocity has df = 0
+    const float2 xh = mul2(qx, fh), yh = mul2(qy, fh), xx = mul2(qx, qx), yy = mul2(qy, qy);
+    acc[RM00] = add2(acc[RM00], fh);
+    acc[RM10] = add2(acc[RM10], xh);
+    acc[RM01] = add2(acc[RM01], yh);
+    acc[RM20] = fma2(qx, xh, acc[RM20]);
+    acc[RM11] = fma2(qy, xh, acc[RM11]);
+    acc[RM02] = fma2(qy, yh, acc[RM02]);
+    acc[RM30] = fma2(xx, xh, acc[RM30]);
+    acc[RM21] = fma2(xx, yh, acc[RM21]);
+    acc[RM12] = fma2(yy, xh, acc[RM12]);
+    acc[RM03] = fma2(yy, yh, acc[RM03]);
+    acc[RB00] = add2(acc[RB00], fb);
+    acc[RB10] = fma2(qx, fb, acc[RB10]);
+    acc[RB01] = fma2(qy, fb, acc[RB01]);
+  };
 #pragma unroll 1
   for (int p = lane; p < NP; p += 32) {
     const float2 qx = *reinterpret_cast<const float2 *>(QXf + 2 * ia), qy = bc2(QYf[jv]);
@@ -508,30 +534,7 @@ __global__ void __launch_bounds__(WPC * 32, MINB) face_moments_warp(const ugks_f
         Sb[s] = make_float2(x.z, y.w);
       }
     }
-    const float2 il = make_float2(ua ? il1 : il0, ub ? il1 : il0);
-    const float2 ds = make_float2(ua ? dist1 : dist0, ub ? dist1 : dist0);
-    const float2 ids = make_float2(ua ? idist1 : idist0, ub ? idist1 : idist0);
-    const float2 sh2 = slope_pair<FM>(Sh, il, ids), sb2 = slope_pair<FM>(Sb, il, ids);
-    const float2 fh = fma2(sh2, ds, Sh[MID]), fb = fma2(sb2, ds, Sb[MID]);
-    frow[p] = cat2(fh, fb);
-    arow[p] = cat2(sh2, sb2);
-    // raw moments (global frame); the padding velocity has df = 0
-    {
-      const float2 xh = mul2(qx, fh), yh = mul2(qy, fh), xx = mul2(qx, qx), yy = mul2(qy, qy);
-      acc[RM00] = add2(acc[RM00], fh);
-      acc[RM10] = add2(acc[RM10], xh);
-      acc[RM01] = add2(acc[RM01], yh);
-      acc[RM20] = fma2(qx, xh, acc[RM20]);
-      acc[RM11] = fma2(qy, xh, acc[RM11]);
-      acc[RM02] = fma2(qy, yh, acc[RM02]);
-      acc[RM30] = fma2(xx, xh, acc[RM30]);
-      acc[RM21] = fma2(xx, yh, acc[RM21]);
-      acc[RM12] = fma2(yy, xh, acc[RM12]);
-      acc[RM03] = fma2(yy, yh, acc[RM03]);
-      acc[RB00] = add2(acc[RB00], fb);
-      acc[RB10] = fma2(qx, fb, acc[RB10]);
-      acc[RB01] = fma2(qy, fb, acc[RB01]);
-    }
+    pair_work(p, Sh, Sb, qx, qy, ua, ub);
     jv += rs;
     ia += qs;
     if (jv >= vn) { jv -= vn; ++ia; }
