@@ -438,7 +438,9 @@ int ugks_step_mixed(const ugks_fused_block *blocks_dev, int nblocks, const ugks_
    stream around the phases: [0] start, [1] after the face pass, [2] after the
    dt check, [3] after the retry face pass, [4] after the second dt check,
    [5] after the cell pass, [6] after the dt update, [7] after the ghost pass.
-   mixed != 0 selects FP32 storage.  Used to time each kernel live. */
+   mixed != 0 selects FP32 storage.  A null entry records nothing (each
+   record costs the stream a few microseconds).  Used to time each kernel
+   live. */
 int ugks_step_profiled(int mixed, const ugks_fused_block *blocks_dev, int nblocks,
                        const ugks_fused_sizes *sizes, ugks_solve_state *solves_dev, int nsolves,
                        void *const *events, UGKS_STREAM);

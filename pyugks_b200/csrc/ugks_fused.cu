@@ -1911,7 +1911,7 @@ int step_impl(const ugks_fused_block *B, int nb, const ugks_fused_sizes *z, ugks
   if (smem > 200 * 1024 || csmem > 200 * 1024) return -(int)cudaErrorInvalidValue;
   const unsigned sg = (unsigned)((ns + 127) / 128);
   auto mark = [&](int k) {
-    if (events) cudaEventRecord(reinterpret_cast<cudaEvent_t>(events[k]), st);
+    if (events && events[k]) cudaEventRecord(reinterpret_cast<cudaEvent_t>(events[k]), st);
   };
   // NVTX: the step, and within it the face, cell and ghost phases
   NvtxRange step_range(mixed ? "ugks step (mixed)" : "ugks step (fp64)");
