@@ -289,8 +289,8 @@ def run_ours(args, rank, world, dist):
         "gpu_launches": solver.launches_per_step() * args.steps,
         "clocks": clocks,
     }
-    if world == 1 and args.workload == "multiblock" and args.precision == "fp64" and not args.no_north_star:
-        # the north-star comparison: batched mixed precision and serving
+    if world == 1 and args.workload == "multiblock" and args.precision == "fp64" and not args.no_comparisons:
+        # the comparison records: batched mixed precision and serving
         # against the plain FP64 method, measured in the same run
         for key, fn in (("batched_mixed", batched_record), ("serving", serving_record)):
             try:
@@ -470,7 +470,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--metrics", default=None,
                     help="append JSON-lines records (the bench line; serving: per tick and per request) here")
-    ap.add_argument("--no-north-star", action="store_true",
+    ap.add_argument("--no-comparisons", action="store_true",
                     help="skip the batched-mixed and serving sub-records of the default line")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
